@@ -1,0 +1,314 @@
+"""Benchmark of the UMAP fit path on B200: SGD edge-updates/s on the 2M-point workload.
+
+Workload (default): n=2,000,000 points, D=64, 50 anisotropic Gaussians (centres ~N(0,8^2 I),
+per-cluster diagonal std ~U[0.5,2], Dirichlet(1) weights), seed 1; exact kNN k=15 (self
+first); init U[-10,10]^2; 500 epochs; min_dist 0.1, spread 1, local_connectivity 1,
+set_op_mix_ratio 1, symmetrize, negative_sample_rate 5.  Synthetic data of that shape.
+
+One step = one complete fit (Umap::learn_manifold -> Optimizer::new -> step_epochs(500) ->
+into_fitted) from kNN + init resident in HBM.  An edge-update is one fired positive edge
+sample in one epoch together with its negative samples; the count per fit is exact (from
+the schedule).  value = edge-updates per fit / fit time.  The SGD kernel's roofline uses
+the algorithmic bytes 4E + F(8 + 16d) + 4dN per epoch (E kept edges, F fired, N negatives,
+d = 2) over the epoch loop's CUDA-event time.
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--n N]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "umap-rs_b200"))
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--n", type=int, default=2_000_000, help="points (default: the 2M workload)")
+    ap.add_argument("--epochs", type=int, default=500)
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--cpu-epochs", type=int, default=4, help="oracle epochs timed for cpu_baseline")
+    ap.add_argument("--cpu-skip", type=int, default=20, help="oracle epochs run untimed first")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--profile", action="store_true",
+                    help="profiling run: build one optimizer, run --profile-epochs epochs, exit")
+    ap.add_argument("--profile-epochs", type=int, default=24)
+    return ap.parse_args()
+
+
+def peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        return {}
+
+
+def traffic_per_epoch():
+    """DRAM bytes per SGD launch from the committed ncu summary (None if absent)."""
+    p = os.path.join(ROOT, "profiles", "sgd_epoch_2m.md")
+    try:
+        for line in open(p):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":", 1)[1].split()[0])
+    except OSError:
+        pass
+    return None
+
+
+class Clocks:
+    """Samples SM clocks and throttle reasons with nvidia-smi during the timed region."""
+    Q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index, self.samples, self.proc = index, [], None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) == 6:
+                self.samples.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[2 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def make_workload(n, seed_note=True):
+    from umap_b200 import workloads as W
+    if n == 2_000_000:
+        X, lab = W.gaussians_2m()
+    else:
+        X, lab = W.gaussian_mixture(n, 64, 50, 8.0, seed=1, anisotropic=True, dirichlet=True)
+    t = time.time()
+    idx, dist, redo = W.knn_exact_clustered_torch(X, lab, 15)
+    knn_s = time.time() - t
+    init = W.uniform_init(n)
+    return idx, dist, init, {"knn_seconds": round(knn_s, 1), "knn_rows_recomputed": redo}
+
+
+def dist_info():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def cpu_baseline(idx, dist, init, epochs_total, n_epochs_timed, skip=20):
+    """Oracle (C++ restatement of the reference's Rayon path) on the host cores: graph built
+    once (untimed), `skip` SGD epochs run untimed (past the first epochs, where few edges
+    fire), then `n_epochs_timed` SGD epochs timed."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    O.build()
+    cores = os.cpu_count() or 1
+    O.set_threads(cores)
+    cfg = O.OracleConfig(n_epochs=epochs_total)
+    t0 = time.time()
+    m = O.learn_manifold(idx, dist, cfg)
+    t_graph = time.time() - t0
+    opt = O.Optimizer(m, init, epochs_total, cfg, seed=1)
+    opt.step_epochs(skip)
+    t1 = time.time()
+    F, N = opt.step_epochs(n_epochs_timed, counts=True)
+    dt = time.time() - t1
+    return {"value": float(F.sum()) / dt, "unit": "edge-updates/s", "cores": cores, "kind": "port",
+            "sample": f"oracle SGD epochs {skip}..{skip + n_epochs_timed} of the {epochs_total}-epoch fit "
+                      f"({int(F.sum())} edge-updates in {dt:.2f} s); graph build {t_graph:.1f} s untimed",
+            "graph_build_s": round(t_graph, 2)}
+
+
+def run_reference(a):
+    rank, world, _ = dist_info()
+    if rank != 0:
+        return
+    idx, dist, init, info = make_workload(a.n)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    vals = []
+    for _ in range(max(1, a.warmup) + a.steps):
+        cb = cpu_baseline(idx, dist, init, a.epochs, a.cpu_epochs, a.cpu_skip)
+        vals.append(cb["value"])
+    v = float(np.median(vals[a.warmup:])) if len(vals) > a.warmup else vals[-1]
+    cb["value"] = v
+    line = {"impl": "reference", "metric": "SGD edge-updates/s", "value": v, "unit": "edge-updates/s",
+            "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"gaussians_{a.n}_d64_k15_{a.epochs}ep"},
+            "cpu_baseline": cb, "e2e": {"value": v, "unit": "edge-updates/s", "h2d_bytes_per_step": 0,
+                                        "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        return run_reference(a)
+    import torch
+    import umap_b200 as ub
+    rank, world, local = dist_info()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as tdist
+        import datetime
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    ub.lib()
+
+    idx, dist, init, winfo = make_workload(a.n)
+    n = a.n
+    cfg = ub.UmapConfig()
+    cfg.optimization.n_epochs = a.epochs
+    d_idx = torch.from_numpy(idx.view(np.int32)).cuda()
+    d_dist = torch.from_numpy(dist).cuda()
+    d_init = torch.from_numpy(init).cuda()
+    torch.cuda.synchronize()
+
+    if a.profile:
+        # Bounded profiling target: one optimizer, a few epochs, few launches before them.
+        m = ub.Umap(cfg).learn_manifold(n, d_idx, d_dist)
+        opt = ub.Optimizer(m, d_init, a.epochs, cfg)
+        opt.step_epochs(a.profile_epochs)
+        torch.cuda.synchronize()
+        print(json.dumps({"profile": True, "epochs": a.profile_epochs, "ms": opt.last_step_ms(),
+                          "edges": opt.n_edges()}), flush=True)
+        return
+
+    def one_fit():
+        m = ub.Umap(cfg).learn_manifold(n, d_idx, d_dist)
+        opt = ub.Optimizer(m, d_init, a.epochs, cfg)
+        opt.step_epochs(a.epochs)
+        sgd_ms = opt.last_step_ms()
+        f = opt.into_fitted(cfg)
+        return f, sgd_ms
+
+    # exact work per fit (independent of timing)
+    m0 = ub.Umap(cfg).learn_manifold(n, d_idx, d_dist)
+    o0 = ub.Optimizer(m0, d_init, a.epochs, cfg)
+    E = o0.n_edges()
+    F_tot, N_tot = o0.schedule_totals(0, a.epochs)
+    del o0
+    dim = 2
+    alg_bytes = 4.0 * E * a.epochs + F_tot * (8 + 16 * dim) + 4.0 * dim * N_tot
+
+    for _ in range(a.warmup):
+        one_fit()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    launches0 = ub.kernel_launches()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sgd_ms = []
+    with Clocks(local) as clk:
+        ev0.record()
+        for _ in range(a.steps):
+            f, ms = one_fit()
+            sgd_ms.append(ms)
+        ev1.record()
+        torch.cuda.synchronize()
+    launches = ub.kernel_launches() - launches0
+    ms_total = ev0.elapsed_time(ev1)
+    if world > 1:
+        t = torch.tensor([ms_total], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms_total = float(t.item())
+    ms_step = ms_total / a.steps
+    value = F_tot * world / (ms_step / 1e3)
+
+    # e2e through the host-pointer C ABI (umap_fit): pinned host inputs, H2D + D2H inside.
+    h_idx = torch.from_numpy(idx.view(np.int32)).pin_memory()
+    h_dist = torch.from_numpy(dist).pin_memory()
+    h_init = torch.from_numpy(init).pin_memory()
+    h_out = torch.empty((n, 2), dtype=torch.float32).pin_memory()
+    import ctypes as C
+    L = ub.lib()
+    ccfg = cfg.to_c()
+    e2e_ms = []
+    for it in range(a.e2e_steps + 1 if a.e2e_steps > 0 else 0):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        out = C.c_void_p()
+        rc = L.umap_fit(C.byref(ccfg), n, C.c_void_p(h_idx.data_ptr()), C.c_void_p(h_dist.data_ptr()), n, 15,
+                        C.c_void_p(h_init.data_ptr()), n, 2, C.byref(out))
+        assert rc == 0, L.umap_last_error()
+        assert L.umap_fitted_embedding(out, C.c_void_p(h_out.data_ptr())) == 0
+        t1 = time.perf_counter()
+        L.umap_fitted_free(out)
+        if it > 0:
+            e2e_ms.append((t1 - t0) * 1e3)
+    e2e_step = float(np.median(e2e_ms)) if e2e_ms else float("nan")
+    h2d = idx.nbytes + dist.nbytes + init.nbytes
+    d2h = n * 2 * 4
+
+    pk = peaks()
+    hbm = pk.get("hbm_gbs")
+    peak_src = "measured" if hbm else "fallback"
+    hbm = hbm or 6650.0
+    sgd_kernel_ms = float(np.median(sgd_ms)) / a.epochs
+    achieved = alg_bytes / a.epochs / (sgd_kernel_ms / 1e3) / 1e9
+    tr = traffic_per_epoch()
+    clocks = clk.summary()
+    line = {
+        "metric": "SGD edge-updates/s", "value": value, "unit": "edge-updates/s", "n_gpus": world,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"gaussians_{n}_d64_k15_{a.epochs}ep", "n_points": n, "k": 15,
+                   "epochs": a.epochs, "n_components": 2, "kept_edges": E, "edge_updates_per_fit": F_tot,
+                   "negatives_per_fit": N_tot, "l2": "inputs exceed L2 (kNN 240 MB + edge slices)",
+                   "parallelism": "replicas" if world > 1 else "single", **winfo},
+        "fit_ms": ms_step,
+        "sgd_ms_per_fit": float(np.median(sgd_ms)),
+        "sgd_edge_updates_per_s": F_tot / (float(np.median(sgd_ms)) / 1e3),
+        "e2e": {"value": F_tot / (e2e_step / 1e3), "unit": "edge-updates/s", "ms_per_step": e2e_step,
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "roofline": {"bound": "hbm", "kernel": "sgd_epoch_kernel<2>", "achieved": achieved,
+                     "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "peak_source": peak_src,
+                     "traffic": tr, "algorithmic_bytes_per_launch": alg_bytes / a.epochs,
+                     "avg_launch_ms": sgd_kernel_ms},
+        "gpu_launches": launches,
+        "clocks": clocks,
+    }
+    if rank == 0 and not a.no_cpu:
+        line["cpu_baseline"] = cpu_baseline(idx, dist, init, a.epochs, a.cpu_epochs, a.cpu_skip)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

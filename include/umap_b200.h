@@ -1,0 +1,205 @@
+/*
+ * umap_b200.h -- C ABI of the B200 (sm_100a) UMAP fit path.
+ *
+ * Each entry point stands in for one item of the Rust API of wilsonzlin/umap-rs 0.4.5
+ * (paths below are relative to that project).  A Rust crate keeps its public API and
+ * implements the bodies by calling these functions (binding sketch in INTEGRATION.md).
+ *
+ * Conventions
+ *  - Every function returns an int status: UMAP_OK (0) or a UMAP_ERR_* code.  Where the
+ *    reference panics, the same condition returns a code and umap_last_error() holds the
+ *    reference's panic message text (e.g. "Cannot step 5 epochs: would exceed
+ *    total_epochs 20 (current: 18)", umap-rs/src/optimizer.rs:298-304).
+ *  - Arrays are row-major and contiguous.  Pointers named host_* are host memory; the
+ *    *_device variants take device pointers on the current CUDA device.
+ *  - Handles are opaque.  A function documented as "consumes" takes ownership (the
+ *    reference moves the value); the caller must not use or free that handle afterwards,
+ *    even when the call fails.
+ *  - One CUDA stream per handle; a handle is not thread-safe (the reference takes
+ *    &mut self).  Distinct handles may be used from distinct threads.
+ *  - No CPU fallback: without a usable CUDA device, compute calls return UMAP_ERR_CUDA.
+ */
+#ifndef UMAP_B200_H
+#define UMAP_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define UMAP_B200_ABI_VERSION 1
+
+enum umap_status {
+  UMAP_OK = 0,
+  UMAP_ERR_INVALID_ARGUMENT = 1, /* reference: validate_parameters / shape panics   */
+  UMAP_ERR_OVERSTEP = 2,         /* reference: Optimizer::step_epochs assert         */
+  UMAP_ERR_CUDA = 3,             /* CUDA runtime error or no device                  */
+  UMAP_ERR_OUT_OF_MEMORY = 4,
+  UMAP_ERR_FORMAT = 5,           /* checkpoint bytes truncated / corrupt / wrong kind */
+  UMAP_ERR_IO = 6,
+  UMAP_ERR_NULL = 7,             /* NULL handle or pointer                           */
+  UMAP_ERR_UNSUPPORTED = 8       /* e.g. MetricType::Generic output metric           */
+};
+
+enum umap_metric_type { /* umap-rs/src/metric.rs:6-12 */
+  UMAP_METRIC_EUCLIDEAN = 0,
+  UMAP_METRIC_GENERIC = 1
+};
+
+/* UmapConfig (umap-rs/src/config.rs:205-235).  Option<T> fields are a has_* flag plus a
+ * value.  Defaults (umap_config_default) are the reference's Default impls:
+ * config.rs:43-52, :117-127, :171-180, :226-235. */
+typedef struct umap_config {
+  uint64_t n_components;            /* 2 */
+  /* ManifoldParams */
+  float min_dist;                   /* 0.1 */
+  float spread;                     /* 1.0 */
+  int32_t has_a; float a;           /* None */
+  int32_t has_b; float b;           /* None */
+  /* GraphParams */
+  uint64_t n_neighbors;             /* 15 */
+  float local_connectivity;         /* 1.0 */
+  float set_op_mix_ratio;           /* 1.0 */
+  int32_t has_disconnection_distance; float disconnection_distance; /* None */
+  int32_t symmetrize;               /* true */
+  /* OptimizationParams */
+  int32_t has_n_epochs; uint64_t n_epochs; /* None */
+  float learning_rate;              /* 1.0 */
+  uint64_t negative_sample_rate;    /* 5 */
+  float repulsion_strength;         /* 1.0 */
+} umap_config;
+
+typedef struct umap_manifold umap_manifold;   /* LearnedManifold, manifold.rs:14-38  */
+typedef struct umap_optimizer umap_optimizer; /* Optimizer, optimizer.rs:27-56       */
+typedef struct umap_fitted umap_fitted;       /* FittedUmap, embedding.rs:438-443    */
+
+/* ---- library ---------------------------------------------------------------------- */
+/* Message of the last failed call on this thread ("" if none). */
+const char* umap_last_error(void);
+int umap_abi_version(void);
+/* Replaces `impl Default for UmapConfig` (config.rs:226-235). */
+int umap_config_default(umap_config* out);
+/* Replaces umap/find_ab_params.rs:9-82 (host code; no GPU needed). */
+int umap_find_ab_params(float spread, float min_dist, float* a_out, float* b_out);
+
+/* ---- Umap::learn_manifold (embedding.rs:149-240) ----------------------------------- */
+/* n_samples = data.shape()[0] (the reference reads nothing else from `data`).
+ * knn_indices u32[knn_rows, knn_cols], knn_dists f32[knn_rows, knn_cols]. */
+int umap_learn_manifold(const umap_config* cfg, uint64_t n_samples,
+                        const uint32_t* host_knn_indices, const float* host_knn_dists,
+                        uint64_t knn_rows, uint64_t knn_cols, umap_manifold** out);
+int umap_learn_manifold_device(const umap_config* cfg, uint64_t n_samples,
+                               const uint32_t* dev_knn_indices, const float* dev_knn_dists,
+                               uint64_t knn_rows, uint64_t knn_cols, umap_manifold** out);
+
+/* ---- LearnedManifold accessors (manifold.rs:40-55) --------------------------------- */
+int umap_manifold_n_vertices(const umap_manifold* m, uint64_t* out);
+int umap_manifold_curve_params(const umap_manifold* m, float* a, float* b);
+/* graph(): CsMatI<f32,u32,usize>; nnz then copy of indptr[n+1], indices[nnz], data[nnz]. */
+int umap_manifold_graph_nnz(const umap_manifold* m, uint64_t* nnz);
+int umap_manifold_graph_copy(const umap_manifold* m, uint64_t* host_indptr,
+                             uint32_t* host_indices, float* host_data);
+/* sigmas / rhos fields (manifold.rs:20-26). */
+int umap_manifold_sigmas_rhos(const umap_manifold* m, float* host_sigmas, float* host_rhos);
+/* Counts behind raise_disconnected_warning (embedding.rs:187-230). */
+int umap_manifold_disconnection_counts(const umap_manifold* m, uint64_t* edges_removed,
+                                       uint64_t* vertices_disconnected);
+/* #[derive(Clone)] on LearnedManifold (manifold.rs:14). */
+int umap_manifold_clone(const umap_manifold* m, umap_manifold** out);
+int umap_manifold_free(umap_manifold* m);
+
+/* ---- Optimizer (optimizer.rs:74-403) ----------------------------------------------- */
+/* Optimizer::new (optimizer.rs:74-290).  Consumes `manifold`.  init f32[rows, dims]. */
+int umap_optimizer_new(umap_manifold* manifold, const float* host_init, uint64_t rows,
+                       uint64_t dims, uint64_t total_epochs, const umap_config* cfg,
+                       int metric_type, umap_optimizer** out);
+int umap_optimizer_new_device(umap_manifold* manifold, const float* dev_init, uint64_t rows,
+                              uint64_t dims, uint64_t total_epochs, const umap_config* cfg,
+                              int metric_type, umap_optimizer** out);
+/* Optimizer::step_epochs (optimizer.rs:297-366).  UMAP_ERR_OVERSTEP with the reference's
+ * message when current_epoch + n > total_epochs. */
+int umap_optimizer_step_epochs(umap_optimizer* opt, uint64_t n);
+int umap_optimizer_current_epoch(const umap_optimizer* opt, uint64_t* out);   /* :369 */
+int umap_optimizer_total_epochs(const umap_optimizer* opt, uint64_t* out);    /* :374 */
+int umap_optimizer_remaining_epochs(const umap_optimizer* opt, uint64_t* out);/* :379 */
+/* embedding() (optimizer.rs:384): copies f32[n_vertices, dims] to host. */
+int umap_optimizer_embedding(const umap_optimizer* opt, float* host_out);
+/* Device pointer to the live embedding (valid until the next call on `opt`). */
+int umap_optimizer_embedding_device(umap_optimizer* opt, float** dev_ptr);
+int umap_optimizer_dims(const umap_optimizer* opt, uint64_t* n_vertices, uint64_t* dims);
+/* manifold() (optimizer.rs:389): borrowed, owned by `opt`. */
+int umap_optimizer_manifold(const umap_optimizer* opt, const umap_manifold** out);
+/* into_fitted (optimizer.rs:397-403).  Consumes `opt`. */
+int umap_optimizer_into_fitted(umap_optimizer* opt, const umap_config* cfg, umap_fitted** out);
+int umap_optimizer_free(umap_optimizer* opt);
+/* Extension (the reference has no seed API; its RNG is unseeded): the Philox key for
+ * negative sampling.  Default 0. */
+int umap_optimizer_set_seed(umap_optimizer* opt, uint64_t seed);
+/* Number of kept edges (the reference's head/tail length, optimizer.rs:133-163). */
+int umap_optimizer_n_edges(const umap_optimizer* opt, uint64_t* out);
+/* The reference's per-edge arrays in its row-major edge order: head/tail u32[E],
+ * epochs_per_sample f64[E] (optimizer.rs:33-35) and the schedule state at current_epoch
+ * (optimizer.rs:41-43).  Any pointer may be NULL to skip that array. */
+int umap_optimizer_export_edges(const umap_optimizer* opt, uint32_t* head, uint32_t* tail,
+                                double* epochs_per_sample, double* epoch_of_next_sample,
+                                double* epoch_of_next_negative_sample,
+                                double* epochs_per_negative_sample);
+/* Extension: exact totals of fired edges and negative samples that step_epochs would
+ * process over epochs [start, end) (for throughput accounting). */
+int umap_optimizer_schedule_totals(const umap_optimizer* opt, uint64_t start, uint64_t end,
+                                   uint64_t* fired, uint64_t* negatives);
+
+/* Extension: CUDA-event time (ms) of the epoch loop of the last step_epochs call, measured
+ * on the optimizer's stream (the SGD kernels only; no host overhead). */
+int umap_optimizer_last_step_ms(const umap_optimizer* opt, float* ms);
+/* Extension: number of this library's kernel launches so far in this process. */
+int umap_kernel_launches(uint64_t* out);
+
+/* ---- FittedUmap (embedding.rs:438-524) --------------------------------------------- */
+int umap_fitted_embedding(const umap_fitted* f, float* host_out);             /* :462 */
+int umap_fitted_dims(const umap_fitted* f, uint64_t* n_vertices, uint64_t* dims);
+int umap_fitted_manifold(const umap_fitted* f, const umap_manifold** out);    /* :485 */
+int umap_fitted_config(const umap_fitted* f, umap_config* out);               /* :490 */
+int umap_fitted_free(umap_fitted* f);
+
+/* ---- Umap::fit (embedding.rs:274-337) ---------------------------------------------- */
+/* learn_manifold -> Optimizer::new -> one step_epochs(total) -> into_fitted -> rows whose
+ * graph row sums to 0 become NaN.  init f32[init_rows, init_cols]. */
+int umap_fit(const umap_config* cfg, uint64_t n_samples, const uint32_t* host_knn_indices,
+             const float* host_knn_dists, uint64_t knn_rows, uint64_t knn_cols,
+             const float* host_init, uint64_t init_rows, uint64_t init_cols,
+             umap_fitted** out);
+int umap_fit_device(const umap_config* cfg, uint64_t n_samples, const uint32_t* dev_knn_indices,
+                    const float* dev_knn_dists, uint64_t knn_rows, uint64_t knn_cols,
+                    const float* dev_init, uint64_t init_rows, uint64_t init_cols,
+                    umap_fitted** out);
+
+/* ---- serde checkpoints (optimizer.rs:27, manifold.rs:14, embedding.rs:438) ---------
+ * The byte format is this library's own little-endian layout carrying every field of the
+ * reference struct (not bincode).  *_serialize writes at most `cap` bytes and sets
+ * *needed to the full size (call with buf=NULL, cap=0 to query). */
+int umap_manifold_serialize(const umap_manifold* m, uint8_t* buf, uint64_t cap, uint64_t* needed);
+int umap_manifold_deserialize(const uint8_t* buf, uint64_t len, umap_manifold** out);
+int umap_optimizer_serialize(const umap_optimizer* o, uint8_t* buf, uint64_t cap, uint64_t* needed);
+int umap_optimizer_deserialize(const uint8_t* buf, uint64_t len, umap_optimizer** out);
+int umap_fitted_serialize(const umap_fitted* f, uint8_t* buf, uint64_t cap, uint64_t* needed);
+int umap_fitted_deserialize(const uint8_t* buf, uint64_t len, umap_fitted** out);
+
+/* ---- kernel-level entry points (parity hooks, device pointers) ---------------------- */
+/* SmoothKnnDist::exec (umap/smooth_knn_dist.rs:60-198) on device arrays. */
+int umap_smooth_knn_dist_device(const float* dev_dists, uint64_t n, uint64_t k,
+                                uint64_t n_iter, float local_connectivity, float bandwidth,
+                                float* dev_sigmas, float* dev_rhos);
+/* Stable LSD radix sort of (u32 key, u32 value) pairs by key bits [0, end_bit): the
+ * transpose step that replaces build_csc_structure (fuzzy_simplicial_set.rs:310-370).
+ * dev_values_in may be NULL (values = 0..n-1). */
+int umap_radix_sort_pairs_device(const uint32_t* dev_keys_in, const uint32_t* dev_values_in,
+                                 uint32_t* dev_keys_out, uint32_t* dev_values_out,
+                                 uint64_t n, int end_bit);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* UMAP_B200_H */

@@ -1,0 +1,131 @@
+"""CPU tests of the C ABI boundary: the library loads without a GPU, exports every symbol
+include/umap_b200.h declares, and its host-only logic (defaults, curve fit, validation with
+the reference's panic texts) behaves like the reference.  No compute call is made here."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+HEADER = os.path.join(ROOT, "include", "umap_b200.h")
+
+
+def declared_functions():
+    txt = open(HEADER).read()
+    return sorted(set(re.findall(r"^\s*(?:int|const char\*)\s+(umap_\w+)\s*\(", txt, re.M)))
+
+
+def test_every_declared_symbol_is_exported(ub):
+    L = ub.lib()
+    names = declared_functions()
+    assert len(names) >= 40
+    for n in names:
+        assert hasattr(L, n), n
+
+
+def test_python_binding_covers_header(ub):
+    from umap_b200 import _lib
+    names = set(declared_functions()) - {"umap_last_error", "umap_abi_version"}
+    assert names == set(_lib.SIGNATURES)
+
+
+def test_config_default_matches_reference(ub):
+    # config.rs:43-52, :117-127, :171-180, :226-235
+    c = ub._lib.UmapConfigC()
+    assert ub.lib().umap_config_default(C.byref(c)) == 0
+    py = ub.UmapConfig.from_c(c)
+    assert py == ub.UmapConfig()
+    assert (py.n_components, py.manifold.min_dist, py.manifold.spread) == (2, np.float32(0.1), 1.0)
+    assert (py.graph.n_neighbors, py.graph.local_connectivity, py.graph.set_op_mix_ratio) == (15, 1.0, 1.0)
+    assert py.graph.disconnection_distance is None and py.graph.symmetrize is True
+    assert py.optimization == ub.OptimizationParams(None, 1.0, 5, 1.0)
+
+
+def test_config_roundtrip(ub):
+    cfg = ub.UmapConfig(n_components=3, manifold=ub.ManifoldParams(0.25, 1.5, 1.2, 0.8),
+                        graph=ub.GraphParams(30, 2.0, 0.5, 7.5, False),
+                        optimization=ub.OptimizationParams(123, 0.5, 7, 2.0))
+    assert ub.UmapConfig.from_c(cfg.to_c()) == cfg
+
+
+@pytest.mark.parametrize("spread,min_dist", [(1.0, 0.1), (1.0, 0.0), (2.0, 0.5), (0.5, 0.25), (1.0, 0.99)])
+def test_find_ab_params_bit_identical_to_oracle(ub, oracle, spread, min_dist):
+    assert ub.find_ab_params(spread, min_dist) == oracle.find_ab_params(spread, min_dist)
+
+
+def _learn(ub, cfg, n, rows, cols):
+    idx = np.zeros((rows, cols), np.uint32)
+    dist = np.zeros((rows, cols), np.float32)
+    return ub.Umap(cfg).learn_manifold(n, idx, dist)
+
+
+@pytest.mark.parametrize("mutate,message", [
+    (lambda c: setattr(c.graph, "set_op_mix_ratio", 1.5), "set_op_mix_ratio must be between 0.0 and 1.0, got 1.5"),
+    (lambda c: setattr(c.graph, "n_neighbors", 1), "n_neighbors must be >= 2, got 1"),
+    (lambda c: setattr(c.optimization, "repulsion_strength", -0.5), "repulsion_strength cannot be negative, got -0.5"),
+    (lambda c: setattr(c.manifold, "min_dist", 2.0), "min_dist (2) must be <= spread (1)"),
+    (lambda c: (setattr(c.manifold, "min_dist", -0.1)), "min_dist cannot be negative, got -0.1"),
+    (lambda c: setattr(c.optimization, "learning_rate", -1.0), "learning_rate must be positive, got -1"),
+    (lambda c: setattr(c, "n_components", 0), "n_components must be >= 1, got 0"),
+])
+def test_validation_messages(ub, mutate, message):
+    # embedding.rs:339-429: each panic becomes UMAP_ERR_INVALID_ARGUMENT with the same text.
+    cfg = ub.UmapConfig()
+    mutate(cfg)
+    with pytest.raises(ub.UmapError) as e:
+        _learn(ub, cfg, 100, 100, cfg.graph.n_neighbors)
+    assert e.value.code == ub.ERR_INVALID_ARGUMENT
+    assert str(e.value) == message
+
+
+def test_shape_messages(ub):
+    cfg = ub.UmapConfig()
+    with pytest.raises(ub.UmapError, match=r"^knn_dists has 10 neighbors but n_neighbors is 15$"):
+        _learn(ub, cfg, 100, 100, 10)
+    with pytest.raises(ub.UmapError, match=r"^knn_dists has 99 samples but data has 100 samples$"):
+        _learn(ub, cfg, 100, 99, 15)
+    with pytest.raises(ub.UmapError, match=r"^Number of samples \(15\) must be > n_neighbors \(15\)$"):
+        _learn(ub, cfg, 15, 15, 15)
+    with pytest.raises(ub.UmapError, match=r"^knn_dists and knn_indices must have the same shape"):
+        ub.Umap(cfg).learn_manifold(100, np.zeros((100, 15), np.uint32), np.zeros((100, 14), np.float32))
+
+
+def test_fit_init_shape_messages(ub):
+    # embedding.rs:284-297 (checked before the manifold is learned)
+    cfg = ub.UmapConfig()
+    idx = np.zeros((100, 15), np.uint32)
+    dist = np.zeros((100, 15), np.float32)
+    with pytest.raises(ub.UmapError, match=r"^init has 3 components but n_components is 2$"):
+        ub.Umap(cfg).fit(100, idx, dist, np.zeros((100, 3), np.float32))
+    with pytest.raises(ub.UmapError, match=r"^init has 50 samples but data has 100 samples$"):
+        ub.Umap(cfg).fit(100, idx, dist, np.zeros((50, 2), np.float32))
+
+
+def test_null_and_moved_handles(ub):
+    L = ub.lib()
+    v = C.c_uint64()
+    assert L.umap_manifold_n_vertices(None, C.byref(v)) == ub.ERR_NULL
+    assert "NULL" in L.umap_last_error().decode()
+    m = ub.LearnedManifold(None)
+    with pytest.raises(ub.UmapError, match="moved or freed"):
+        m.n_vertices()
+    assert L.umap_manifold_free(None) == 0
+
+
+def test_deserialize_rejects_garbage_without_gpu(ub):
+    for fn in (ub.LearnedManifold.from_bytes, ub.Optimizer.from_bytes, ub.FittedUmap.from_bytes):
+        with pytest.raises(ub.UmapError) as e:
+            fn(b"not a checkpoint at all")
+        assert e.value.code == ub.ERR_FORMAT
+        with pytest.raises(ub.UmapError) as e:
+            fn(b"")
+        assert e.value.code == ub.ERR_FORMAT
+
+
+def test_transform_is_todo_like_reference(ub):
+    f = ub.FittedUmap(None)
+    with pytest.raises(NotImplementedError, match="Transform not yet implemented"):
+        f.transform(None, None, None)

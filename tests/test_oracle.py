@@ -1,0 +1,229 @@
+"""CPU tests of the oracle (the C++ restatement of the reference's CPU path).
+
+The reference pins no numeric value on this path (umap-rs/src/tests.rs holds smoke tests
+only), so the oracle is checked here against (1) hand-derived known answers of each
+reference function and (2) the reference's own smoke-test assertions, re-expressed.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from conftest import ring_fixture, small_gauss
+
+
+def np_unrolled_mean(x):
+    """ndarray 0.17 mean (sum via 8-way unrolled fold), written in numpy float32."""
+    x = np.asarray(x, np.float32)
+    f = np.float32
+    p = [f(0)] * 8
+    n = len(x)
+    i = 0
+    while n - i >= 8:
+        for j in range(8):
+            p[j] = f(p[j] + x[i + j])
+        i += 8
+    acc = f(0)
+    for a, b in ((0, 4), (1, 5), (2, 6), (3, 7)):
+        acc = f(acc + f(p[a] + p[b]))
+    for t in range(min(n - i, 7)):
+        acc = f(acc + x[i + t])
+    return f(acc / f(n))
+
+
+@pytest.mark.parametrize("n", [1, 7, 8, 9, 15, 16, 17, 31, 100, 1001])
+def test_ndarray_mean_order(oracle, n):
+    x = np.random.Generator(np.random.PCG64(n)).random(n, dtype=np.float32) * 3
+    assert oracle.ndarray_mean(x) == np_unrolled_mean(x)
+
+
+def test_find_ab_params_fits_curve(oracle):
+    # find_ab_params.rs: 1 / (1 + a x^(2b)) fitted to the offset exponential on [0, 3*spread].
+    for spread, min_dist in [(1.0, 0.1), (1.0, 0.0), (2.0, 0.5), (1.0, 0.99)]:
+        a, b = oracle.find_ab_params(spread, min_dist)
+        assert 0.001 <= a <= 10 and 0.001 <= b <= 10
+        x = np.linspace(0, 3 * spread, 300)
+        y = np.where(x < min_dist, 1.0, np.exp(-(x - min_dist) / spread))
+        fit = 1.0 / (1.0 + a * x ** (2 * b))
+        start = 1.0 / (1.0 + 1.5 * x ** (2 * 0.9))   # the GD's initial guess (a=1.5, b=0.9)
+        assert np.mean((fit - y) ** 2) < np.mean((start - y) ** 2)
+    a, b = oracle.find_ab_params(1.0, 0.1)
+    assert a > 0 and b > 0  # tests.rs:77-78
+
+
+def test_smooth_knn_equal_distances(oracle):
+    # All neighbour distances equal d: rho = d, every term is 1 so psum = k-1 > log2(k) at
+    # every step; mid halves 64 times, then the MIN_K_DIST_SCALE clamp gives 1e-3 * mean.
+    k = 10
+    d = np.zeros((1, k), np.float32)
+    d[0, 1:] = 2.5
+    s, r = oracle.smooth_knn_dist(d)
+    assert r[0] == np.float32(2.5)
+    assert s[0] == np.float32(np.float32(1e-3) * np_unrolled_mean(d[0]))
+
+
+def test_smooth_knn_solves_target(oracle):
+    g = np.random.Generator(np.random.PCG64(3))
+    d = np.sort(g.random((200, 15), dtype=np.float32) * 4, axis=1)
+    d[:, 0] = 0
+    s, r = oracle.smooth_knn_dist(d)
+    assert np.array_equal(r, d[:, 1])  # rho = first non-zero distance (local_connectivity 1)
+    target = math.log2(15)
+    for i in range(200):
+        terms = np.where(d[i, 1:] - r[i] > 0, np.exp(-(d[i, 1:] - r[i]) / s[i]), 1.0)
+        assert abs(terms.sum() - target) < 1e-4
+
+
+def test_smooth_knn_local_connectivity_interpolation(oracle):
+    d = np.array([[0, 1, 2, 4, 8, 9, 10, 11]], np.float32)
+    _, r = oracle.smooth_knn_dist(d, local_connectivity=1.5)   # rho = d1 + 0.5 (d2 - d1)
+    assert r[0] == np.float32(1.5)
+    _, r = oracle.smooth_knn_dist(d, local_connectivity=0.5)   # index 0: 0.5 * first non-zero
+    assert r[0] == np.float32(0.5)
+    _, r = oracle.smooth_knn_dist(np.zeros((1, 8), np.float32))  # no non-zero -> 0
+    assert r[0] == 0
+    d2 = np.array([[0, 0, 0, 3, 0, 0, 0, 0]], np.float32)
+    _, r = oracle.smooth_knn_dist(d2, local_connectivity=2.0)  # fewer non-zeros -> max
+    assert r[0] == np.float32(3)
+
+
+def test_zero_rho_uses_global_mean(oracle):
+    d = np.ones((4, 6), np.float32)
+    d[2] = 0.0
+    s, r = oracle.smooth_knn_dist(d)
+    assert r[2] == 0
+    assert s[2] >= np.float32(1e-3) * np_unrolled_mean(d.ravel()) - 1e-12
+
+
+def test_membership_and_union_known_answers(oracle):
+    # 3 points; 0 -> 1 (dist 1 = rho, weight 1), 1 -> 2, 2 -> 0 with an extra self and
+    # sentinel column that must be skipped.
+    idx = np.array([[0, 1, 0xFFFFFFFF], [1, 2, 0], [2, 0, 1]], np.uint32)
+    dist = np.array([[0, 1, 5], [0, 1, 3], [0, 2, 2.5]], np.float32)
+    cfg = oracle.OracleConfig(n_neighbors=3, symmetrize=False)
+    # n_samples must exceed n_neighbors: pad with an isolated 4th point
+    idx4 = np.vstack([idx, [[3, 3, 3]]]).astype(np.uint32)
+    dist4 = np.vstack([dist, [[0, 0, 0]]]).astype(np.float32)
+    m = oracle.learn_manifold(idx4, dist4, cfg)
+    ip, ix, dt = m.directed()
+    sig, rho = m.sigmas_rhos()
+    assert list(ip) == [0, 1, 3, 5, 5]
+    assert list(ix[:1]) == [1]            # sentinel skipped, self skipped
+    assert dt[0] == 1.0                   # d - rho <= 0
+    # row 1: cols sorted (0, 2); weight for col 0 = exp(-(3 - 1)/sigma_1)
+    assert list(ix[1:3]) == [0, 2]
+    x = np.float32(np.float32(-(np.float32(3) - rho[1])) / sig[1])
+    expect = np.float32(np.exp(np.float64(x)))   # correctly rounded; glibc expf is within 1 ulp
+    assert abs(int(dt[1].view(np.int32)) - int(expect.view(np.int32))) <= 1
+    # union with mix = 1: A + A^T - A o A^T
+    cfg_u = oracle.OracleConfig(n_neighbors=3, symmetrize=True)
+    mu = oracle.learn_manifold(idx4, dist4, cfg_u)
+    Ad = np.zeros((4, 4), np.float32)
+    for r_ in range(4):
+        for q in range(ip[r_], ip[r_ + 1]):
+            Ad[r_, ix[q]] = dt[q]
+    uip, uix, udt = mu.graph()
+    U = np.zeros((4, 4), np.float32)
+    for r_ in range(4):
+        for q in range(uip[r_], uip[r_ + 1]):
+            U[r_, uix[q]] = udt[q]
+    f = np.float32
+    for i in range(4):
+        for j in range(4):
+            a, b = Ad[i, j], Ad[j, i]
+            if a == 0 and b == 0:
+                assert U[i, j] == 0
+            elif a != 0:
+                assert U[i, j] == f(f(f(1) * a + f(1) * b) + f(f(f(-1) * a) * b))
+            else:
+                assert U[i, j] == b
+    assert np.array_equal(U, U.T)
+
+
+def test_intersection_drops_one_sided(oracle):
+    idx, dist, _ = ring_fixture()
+    cfg = oracle.OracleConfig(n_neighbors=10, set_op_mix_ratio=0.0)
+    m = oracle.learn_manifold(idx, dist, cfg)
+    ip, ix, dt = m.graph()
+    # ring kNN (i -> i+1..i+10) has no reciprocal pairs, so intersection is empty
+    assert len(ix) == 0
+
+
+def test_disconnection_distance(oracle):
+    idx, dist, _ = ring_fixture()
+    cfg = oracle.OracleConfig(n_neighbors=10, disconnection_distance=1.0, symmetrize=False)
+    m = oracle.learn_manifold(idx, dist, cfg)
+    info = m.info()
+    assert info["edges_removed"] == int((dist >= 1.0).sum())
+    ip, ix, _ = m.directed()
+    assert ip[-1] <= int((dist < 1.0).sum())
+    for r in range(len(idx)):            # no kept entry has a removed (>= 1.0) distance
+        d_of = {int(c): float(d) for c, d in zip(idx[r], dist[r])}
+        assert all(d_of[int(c)] < 1.0 for c in ix[ip[r]:ip[r + 1]])
+
+
+# ---- the reference's smoke tests (umap-rs/src/tests.rs), against the oracle
+def test_ref_learn_manifold(oracle, ring):
+    idx, dist, _ = ring
+    m = oracle.learn_manifold(idx, dist, oracle.OracleConfig(n_neighbors=10))
+    info = m.info()
+    assert info["n_vertices"] == 50
+    assert len(m.graph()[1]) > 0
+    assert info["a"] > 0 and info["b"] > 0
+
+
+def test_ref_high_level_fit(oracle, ring):
+    idx, dist, init = ring
+    emb, _, _ = oracle.fit(idx, dist, init, oracle.OracleConfig(n_neighbors=10, n_epochs=10))
+    assert emb.shape == (50, 2)
+    assert np.all(np.isfinite(emb) | np.isnan(emb))
+
+
+def test_ref_optimizer_step_epochs_and_overstep(oracle, ring):
+    idx, dist, init = ring
+    cfg = oracle.OracleConfig(n_neighbors=10)
+    m = oracle.learn_manifold(idx, dist, cfg)
+    opt = oracle.Optimizer(m, init, 20, cfg)
+    assert (opt.current_epoch(), opt.remaining_epochs()) == (0, 20)
+    opt.step_epochs(5)
+    assert (opt.current_epoch(), opt.remaining_epochs()) == (5, 15)
+    opt.step_epochs(13)
+    with pytest.raises(oracle.OracleError, match=r"^Cannot step 5 epochs: would exceed total_epochs 20 \(current: 18\)$"):
+        opt.step_epochs(5)
+
+
+def fixed_point_schedule(eps, total, neg):
+    """The GPU's stateless schedule in exact integer arithmetic: Q = ceil(2^32/eps),
+    m(n) = (n*Q) >> 32 firings by epoch n, y(x) = (x*neg*Q) >> 32; a firing at n with index m
+    draws y(n) - y(p) negatives (p = epoch of firing m-1; y(n) - 1 for the first firing)."""
+    Q = np.clip(np.ceil(4294967296.0 / eps), 1, 2 ** 32).astype(np.uint64)
+    F, N = [], []
+    for n in range(total):
+        n64 = np.uint64(n)
+        m = (n64 * Q) >> np.uint64(32)
+        mp = ((np.uint64(n - 1) * Q) >> np.uint64(32)) if n > 0 else np.zeros_like(Q)
+        fired = m > mp
+        y = (n64 * np.uint64(neg) * Q) >> np.uint64(32)
+        mm1 = np.maximum(m, np.uint64(1)) - np.uint64(1)
+        p = ((mm1 << np.uint64(32)) + Q - np.uint64(1)) // Q
+        yp = (p * np.uint64(neg) * Q) >> np.uint64(32)
+        nn = np.where(m <= 1, y.astype(np.int64) - 1, y.astype(np.int64) - yp.astype(np.int64))
+        F.append(int(fired.sum()))
+        N.append(int(np.where(fired, np.maximum(nn, 0), 0).sum()))
+    return np.array(F), np.array(N)
+
+
+def test_schedule_closed_form_matches_state_arrays(oracle):
+    """The GPU keeps one fixed-point value per edge and recomputes the schedule in closed
+    form; it must reproduce the reference's f64 state evolution
+    (optimize_layout_euclidean.rs:277-343) epoch by epoch."""
+    idx, dist, init = small_gauss(600, 10, seed=5)
+    cfg = oracle.OracleConfig(n_neighbors=10)
+    m = oracle.learn_manifold(idx, dist, cfg)
+    total = 60
+    opt = oracle.Optimizer(m, init, total, cfg, seed=1)
+    _, _, eps = opt.edges()
+    F, N = opt.step_epochs(total, counts=True)
+    gF, gN = fixed_point_schedule(eps, total, 5)
+    assert np.abs(gF - F.astype(np.int64)).sum() <= 1e-5 * F.sum() + 1
+    assert np.abs(gN - N.astype(np.int64)).sum() <= 1e-5 * N.sum() + 5

@@ -1,0 +1,1241 @@
+// C-ABI implementation: handle types, orchestration of the fit path on one CUDA stream per
+// handle, and checkpoints.  Mirrors the reference's Rust API (see include/umap_b200.h).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/umap_b200.h"
+#include "host_math.hpp"
+#include "ub_internal.hpp"
+
+namespace ub {
+
+thread_local std::string g_last_error;
+static std::atomic<uint64_t> g_launches{0};
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+[[noreturn]] void throw_cuda(cudaError_t e, const char* what, const char* file, int line) {
+  (void)cudaGetLastError();
+  int code = e == cudaErrorMemoryAllocation ? OUT_OF_MEMORY : CUDA;
+  const char* f = strrchr(file, '/');
+  throw Error(code, std::string(what) + ": " + cudaGetErrorString(e) + " (" + (f ? f + 1 : file) +
+                        ":" + std::to_string(line) + ")");
+}
+
+namespace {
+
+// ------------------------------------------------------------------ stream ownership
+// Keeps freed blocks in the device's default stream-ordered pool (process lifetime) so
+// that repeated fits do not pay for fresh device allocations.
+void keep_pool_warm(int device) {
+  static std::atomic<uint64_t> done_mask{0};
+  if (device < 0 || device >= 64 || (done_mask.load() >> device) & 1ull) return;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    uint64_t thr = UINT64_MAX;
+    (void)cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+  }
+  (void)cudaGetLastError();
+  done_mask.fetch_or(1ull << device);
+}
+
+struct Stream {
+  cudaStream_t s = nullptr;
+  int device = 0;
+  Stream() {
+    UB_CUDA(cudaGetDevice(&device));
+    keep_pool_warm(device);
+    UB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  }
+  ~Stream() {
+    if (s) {
+      (void)cudaStreamSynchronize(s);
+      (void)cudaStreamDestroy(s);
+    }
+  }
+  Stream(const Stream&) = delete;
+  Stream& operator=(const Stream&) = delete;
+  void sync() const { UB_CUDA(cudaStreamSynchronize(s)); }
+  void activate() const { UB_CUDA(cudaSetDevice(device)); }
+};
+
+// Phase timing with the reference's tracing phase names (fuzzy_simplicial_set.rs:133-162,
+// optimizer.rs:103-272), measured by CUDA events on the handle's stream; printed to stderr
+// when UMAP_B200_LOG is set.
+struct PhaseLog {
+  cudaStream_t s;
+  bool on;
+  cudaEvent_t last = nullptr;
+  explicit PhaseLog(cudaStream_t st) : s(st), on(getenv("UMAP_B200_LOG") != nullptr) {
+    if (on) {
+      UB_CUDA(cudaEventCreate(&last));
+      UB_CUDA(cudaEventRecord(last, s));
+    }
+  }
+  void mark(const char* name) {
+    if (!on) return;
+    cudaEvent_t e;
+    UB_CUDA(cudaEventCreate(&e));
+    UB_CUDA(cudaEventRecord(e, s));
+    UB_CUDA(cudaEventSynchronize(e));
+    float ms = 0;
+    UB_CUDA(cudaEventElapsedTime(&ms, last, e));
+    fprintf(stderr, "[umap_b200] duration_ms=%.3f %s\n", ms, name);
+    (void)cudaEventDestroy(last);
+    last = e;
+  }
+  ~PhaseLog() {
+    if (last) (void)cudaEventDestroy(last);
+  }
+};
+
+template <class T>
+void d2h(T* dst, const T* src, uint64_t n, cudaStream_t s) {
+  if (n) UB_CUDA(cudaMemcpyAsync(dst, src, n * sizeof(T), cudaMemcpyDeviceToHost, s));
+}
+template <class T>
+void h2d(T* dst, const T* src, uint64_t n, cudaStream_t s) {
+  if (n) UB_CUDA(cudaMemcpyAsync(dst, src, n * sizeof(T), cudaMemcpyHostToDevice, s));
+}
+template <class T>
+void d2d(T* dst, const T* src, uint64_t n, cudaStream_t s) {
+  if (n) UB_CUDA(cudaMemcpyAsync(dst, src, n * sizeof(T), cudaMemcpyDeviceToDevice, s));
+}
+
+}  // namespace
+}  // namespace ub
+
+// ------------------------------------------------------------------ handle types
+struct umap_manifold {
+  std::unique_ptr<ub::Stream> stream;  // declared first: destroyed last
+  uint64_t n_vertices = 0, nnz = 0;
+  float a = 0, b = 0;
+  uint64_t edges_removed = 0, vertices_disconnected = 0;
+  ub::DevBuf<uint64_t> indptr;
+  ub::DevBuf<uint32_t> indices;
+  ub::DevBuf<float> data;
+  ub::DevBuf<float> sigmas, rhos;
+  cudaStream_t s() const { return stream->s; }
+};
+
+struct umap_optimizer {
+  std::unique_ptr<umap_manifold> manifold;  // declared first: owns the stream
+  uint64_t n = 0, dim = 0;
+  ub::DevBuf<float> emb2;  // [live | snapshot], each n*dim
+  ub::SgdLayout layout;
+  uint64_t current_epoch = 0, total_epochs = 0;
+  float gamma = 1, initial_alpha = 1;
+  uint64_t negative_sample_rate = 5;
+  int metric_type = UMAP_METRIC_EUCLIDEAN;
+  float max_val = 0, threshold = 0, max_w = 1;
+  uint64_t seed = 0;
+  float last_step_ms = 0;  // CUDA-event time of the last step_epochs epoch loop
+  cudaStream_t s() const { return manifold->s(); }
+};
+
+struct umap_fitted {
+  std::unique_ptr<umap_manifold> manifold;
+  uint64_t n = 0, dim = 0;
+  ub::DevBuf<float> embedding;
+  umap_config config{};
+  cudaStream_t s() const { return manifold->s(); }
+};
+
+namespace ub {
+namespace {
+
+void set_error(const std::string& m) { g_last_error = m; }
+
+#define API_BEGIN try {
+#define API_END                                                  \
+  }                                                              \
+  catch (const ub::Error& e) {                                   \
+    ub::set_error(e.what());                                     \
+    return e.code;                                               \
+  }                                                              \
+  catch (const std::bad_alloc&) {                                \
+    ub::set_error("host allocation failed");                     \
+    return UMAP_ERR_OUT_OF_MEMORY;                               \
+  }                                                              \
+  catch (const std::exception& e) {                              \
+    ub::set_error(e.what());                                     \
+    return UMAP_ERR_CUDA;                                        \
+  }                                                              \
+  ub::set_error("");                                             \
+  return UMAP_OK;
+
+void need(const void* p, const char* what) {
+  if (!p) throw Error(NULLPTR, std::string(what) + " is NULL");
+}
+
+GraphParams graph_params(const umap_config& c) {
+  GraphParams gp{};
+  gp.local_connectivity = c.local_connectivity;
+  const float lcf = floorf(c.local_connectivity);
+  gp.interpolation = c.local_connectivity - lcf;
+  gp.lc_usize = rust_f32_as_usize(c.local_connectivity);
+  gp.lc_index = rust_f32_as_usize(lcf);
+  gp.target = log2f((float)c.n_neighbors) * 1.0f;  // smooth_knn_dist.rs:71, bandwidth 1
+  gp.disc_thr = c.has_disconnection_distance ? c.disconnection_distance : INFINITY;
+  gp.mix = c.set_op_mix_ratio;
+  gp.prod_coeff = 1.0f - 2.0f * c.set_op_mix_ratio;  // fuzzy_simplicial_set.rs:394
+  gp.n_iter = 64;
+  return gp;
+}
+
+// ------------------------------------------------------------------ learn_manifold
+// embedding.rs:149-240 on device arrays.
+std::unique_ptr<umap_manifold> learn_manifold_impl(const umap_config& c, uint64_t n_samples,
+                                                   const uint32_t* idx, const float* dist,
+                                                   uint64_t rows, uint64_t cols) {
+  std::string err = validate_parameters(c, n_samples, rows, cols);
+  if (!err.empty()) throw Error(INVALID_ARGUMENT, err);
+  const uint64_t n = n_samples, k = cols;
+  if (n * k >= 0xFFFFFFFFull)
+    throw Error(UNSUPPORTED, "n_samples * n_neighbors must be < 2^32 on this build");
+  auto m = std::make_unique<umap_manifold>();
+  m->stream = std::make_unique<Stream>();
+  cudaStream_t s = m->s();
+  m->n_vertices = n;
+  if (c.has_a && c.has_b) {  // embedding.rs:161-166
+    m->a = c.a;
+    m->b = c.b;
+  } else {
+    find_ab_params(c.spread, c.min_dist, &m->a, &m->b);
+  }
+  const GraphParams gp = graph_params(c);
+  PhaseLog log(s);
+
+  m->sigmas.alloc(n, s);
+  m->rhos.alloc(n, s);
+  smooth_knn(dist, n, k, gp, m->sigmas.p, m->rhos.p, s);
+  log.mark("smooth_knn_dist complete");
+
+  DevBuf<uint32_t> pcol(n * k, s), cnt(n, s);
+  DevBuf<float> pw(n * k, s);
+  DevBuf<unsigned long long> dcount(2, s);
+  UB_CUDA(cudaMemsetAsync(dcount.p, 0, 16, s));
+  membership(idx, dist, n, k, gp, m->sigmas.p, m->rhos.p, pcol.p, pw.p, cnt.p, dcount.p, s);
+  DevBuf<uint64_t> dptr(n + 1, s);
+  scan_u32_to_u64(cnt.p, dptr.p, n, s);
+  uint64_t nnz_dir = 0;
+  d2h(&nnz_dir, dptr.p + n, 1, s);
+  UB_CUDA(cudaStreamSynchronize(s));
+  DevBuf<uint32_t> keys(nnz_dir, s), vals(nnz_dir, s);
+  compact_directed(pcol.p, cnt.p, dptr.p, n, k, keys.p, vals.p, s);
+  log.mark("build_membership_csr complete");
+
+  if (c.symmetrize) {
+    // Transpose: stable radix sort of (column, position) -> per-column source rows ascending.
+    DevBuf<uint32_t> tkeys(nnz_dir, s), tvals(nnz_dir, s);
+    radix_sort_pairs(keys.p, vals.p, tkeys.p, tvals.p, nnz_dir, bits_for(n ? n - 1 : 0), s);
+    keys.reset();
+    vals.reset();
+    DevBuf<uint64_t> tptr(n + 1, s);
+    segment_starts(tkeys.p, nnz_dir, n, tptr.p, s);
+    tkeys.reset();
+    DevBuf<uint32_t> ucnt(n, s);
+    union_rows(pcol.p, pw.p, cnt.p, k, tptr.p, tvals.p, n, gp, ucnt.p, nullptr, nullptr, nullptr,
+               false, s);
+    m->indptr.alloc(n + 1, s);
+    scan_u32_to_u64(ucnt.p, m->indptr.p, n, s);
+    d2h(&m->nnz, m->indptr.p + n, 1, s);
+    UB_CUDA(cudaStreamSynchronize(s));
+    m->indices.alloc(m->nnz, s);
+    m->data.alloc(m->nnz, s);
+    union_rows(pcol.p, pw.p, cnt.p, k, tptr.p, tvals.p, n, gp, nullptr, m->indptr.p, m->indices.p,
+               m->data.p, true, s);
+    log.mark("set_operations complete");
+  } else {
+    m->nnz = nnz_dir;
+    m->indptr = std::move(dptr);
+    m->indices = std::move(keys);
+    m->data.alloc(nnz_dir, s);
+    gather_weights(pw.p, vals.p, nnz_dir, m->data.p, s);
+  }
+  count_empty_rows(m->indptr.p, m->data.p, n, dcount.p + 1, s);
+  unsigned long long counts[2];
+  d2h(counts, dcount.p, 2, s);
+  UB_CUDA(cudaStreamSynchronize(s));
+  m->edges_removed = counts[0];
+  m->vertices_disconnected = counts[1];
+  log.mark("disconnected vertex count complete");
+  if (getenv("UMAP_B200_LOG")) {  // raise_disconnected_warning.rs:4-26 (counts only)
+    fprintf(stderr, "[umap_b200] learn_manifold: n=%llu nnz=%llu edges_removed=%llu vertices_disconnected=%llu\n",
+            (unsigned long long)n, (unsigned long long)m->nnz, counts[0], counts[1]);
+  }
+  return m;
+}
+
+std::unique_ptr<umap_manifold> clone_manifold(const umap_manifold& src) {
+  auto m = std::make_unique<umap_manifold>();
+  m->stream = std::make_unique<Stream>();
+  cudaStream_t s = m->s();
+  UB_CUDA(cudaStreamSynchronize(src.s()));
+  m->n_vertices = src.n_vertices;
+  m->nnz = src.nnz;
+  m->a = src.a;
+  m->b = src.b;
+  m->edges_removed = src.edges_removed;
+  m->vertices_disconnected = src.vertices_disconnected;
+  m->indptr.alloc(src.n_vertices + 1, s);
+  m->indices.alloc(src.nnz, s);
+  m->data.alloc(src.nnz, s);
+  m->sigmas.alloc(src.n_vertices, s);
+  m->rhos.alloc(src.n_vertices, s);
+  d2d(m->indptr.p, src.indptr.p, src.n_vertices + 1, s);
+  d2d(m->indices.p, src.indices.p, src.nnz, s);
+  d2d(m->data.p, src.data.p, src.nnz, s);
+  d2d(m->sigmas.p, src.sigmas.p, src.n_vertices, s);
+  d2d(m->rhos.p, src.rhos.p, src.n_vertices, s);
+  UB_CUDA(cudaStreamSynchronize(s));
+  return m;
+}
+
+// ------------------------------------------------------------------ Optimizer
+void set_l2_window(umap_optimizer& o, bool enable) {
+  static const bool disabled = [] {
+    const char* e = getenv("UMAP_B200_L2_PERSIST");
+    return e && e[0] == '0';
+  }();
+  cudaStreamAttrValue attr;
+  memset(&attr, 0, sizeof attr);
+  if (enable && !disabled && o.emb2.p) {
+    int dev = o.manifold->stream->device, max_persist = 0, max_window = 0;
+    UB_CUDA(cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, dev));
+    UB_CUDA(cudaDeviceGetAttribute(&max_window, cudaDevAttrMaxAccessPolicyWindowSize, dev));
+    if (max_persist <= 0 || max_window <= 0) return;
+    const size_t bytes = o.emb2.bytes();
+    const size_t lim = std::min(bytes, (size_t)max_persist);
+    UB_CUDA(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, lim));
+    attr.accessPolicyWindow.base_ptr = o.emb2.p;
+    attr.accessPolicyWindow.num_bytes = std::min(bytes, (size_t)max_window);
+    attr.accessPolicyWindow.hitRatio =
+        (float)std::min(1.0, (double)lim / (double)attr.accessPolicyWindow.num_bytes);
+    attr.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+    attr.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+  }
+  UB_CUDA(cudaStreamSetAttribute(o.s(), cudaStreamAttributeAccessPolicyWindow, &attr));
+}
+
+// Kept edges in the reference's order (optimizer.rs:85-172).
+struct KeptEdges {
+  uint64_t E = 0;
+  DevBuf<uint64_t> ptr;
+  DevBuf<uint32_t> tail;
+  DevBuf<double> eps;
+};
+
+void compute_kept_edges(const umap_optimizer& o, KeptEdges& K, bool want_tail, bool want_eps) {
+  const umap_manifold& m = *o.manifold;
+  cudaStream_t s = o.s();
+  K.ptr.alloc(m.n_vertices + 1, s);
+  prune_edges(m.indptr.p, m.data.p, m.n_vertices, o.threshold, K.ptr.p, &K.E, s);
+  if (want_tail) K.tail.alloc(K.E, s);
+  if (want_eps) K.eps.alloc(K.E, s);
+  export_edges(m.indptr.p, m.indices.p, m.data.p, m.n_vertices, o.threshold, o.max_w, o.total_epochs,
+               K.ptr.p, nullptr, want_tail ? K.tail.p : nullptr, want_eps ? K.eps.p : nullptr, s);
+}
+
+// optimizer.rs:74-290.  `init` is a device array of n*dim floats on stream `s` (or host).
+std::unique_ptr<umap_optimizer> optimizer_new_impl(std::unique_ptr<umap_manifold> man, const float* init,
+                                                   bool init_on_host, uint64_t rows, uint64_t dims,
+                                                   uint64_t total_epochs, const umap_config& c,
+                                                   int metric_type) {
+  if (metric_type == UMAP_METRIC_GENERIC)
+    throw Error(UNSUPPORTED,
+                "MetricType::Generic output metrics are not implemented on the GPU path "
+                "(only the Euclidean specialisation, optimize_layout_euclidean.rs)");
+  if (metric_type != UMAP_METRIC_EUCLIDEAN) throw Error(INVALID_ARGUMENT, "unknown metric_type");
+  if (rows != man->n_vertices)
+    throw Error(INVALID_ARGUMENT, "init has " + std::to_string(rows) + " samples but data has " +
+                                      std::to_string(man->n_vertices) + " samples");
+  if (dims < 1) throw Error(INVALID_ARGUMENT, "n_components must be >= 1, got 0");
+  if (man->n_vertices >= 0xFFFFFFFFull) throw Error(UNSUPPORTED, "n_vertices must be < 2^32");
+  auto o = std::make_unique<umap_optimizer>();
+  o->manifold = std::move(man);
+  cudaStream_t s = o->s();
+  o->gamma = c.repulsion_strength;
+  o->initial_alpha = c.learning_rate;
+  o->negative_sample_rate = c.negative_sample_rate;
+  o->metric_type = metric_type;
+  o->n = rows;
+  o->dim = dims;
+  o->total_epochs = total_epochs;
+  o->current_epoch = 0;
+  const uint64_t n = o->manifold->n_vertices;
+
+  // :90-102 threshold
+  PhaseLog log(s);
+  DevBuf<float> dmax(1, s);
+  reduce_max_f32(o->manifold->data.p, o->manifold->nnz, 0.0f, dmax.p, s);
+  float max_val = 0.0f;
+  d2h(&max_val, dmax.p, 1, s);
+  UB_CUDA(cudaStreamSynchronize(s));
+  const uint64_t default_epochs = n <= 10000 ? 500 : 200;
+  const uint64_t threshold_epochs = total_epochs > 10 ? total_epochs : default_epochs;
+  o->max_val = max_val;
+  o->threshold = max_val / (float)threshold_epochs;
+  // make_epochs_per_sample.rs:26-32: max over kept weights (max_val itself is kept).
+  o->max_w = (o->manifold->nnz > 0 && max_val > 0.0f) ? max_val : 1.0f;
+  log.mark("optimizer threshold computed");
+
+  {
+    KeptEdges K;
+    compute_kept_edges(*o, K, true, true);
+    log.mark("optimizer edge filtering + epochs_per_sample complete");
+    build_sgd_layout(K.ptr.p, K.tail.p, K.eps.p, n, 0, o->layout, s);
+    log.mark("optimizer task layout complete");
+  }
+  // :181-230 normalise init
+  o->emb2.alloc(2 * n * dims, s);
+  if (init_on_host) h2d(o->emb2.p, init, n * dims, s);
+  else d2d(o->emb2.p, init, n * dims, s);
+  normalize_init(o->emb2.p, n, (uint32_t)dims, s);
+  log.mark("optimizer embedding normalization complete");
+  if (log.on)
+    fprintf(stderr, "[umap_b200] edges=%llu tasks=%llu split_tasks=%llu chunk=%u max_degree=%u entries=%llu\n",
+            (unsigned long long)o->layout.n_edges, (unsigned long long)o->layout.n_tasks,
+            (unsigned long long)o->layout.split_tasks, o->layout.chunk, o->layout.max_degree,
+            (unsigned long long)o->layout.n_entries);
+  set_l2_window(*o, true);
+  UB_CUDA(cudaStreamSynchronize(s));
+  return o;
+}
+
+SgdParams sgd_params(const umap_optimizer& o) {
+  SgdParams p{};
+  p.a = o.manifold->a;
+  p.b = o.manifold->b;
+  p.gamma = o.gamma;
+  p.neg_attr = (-2.0f * p.a) * p.b;     // optimize_layout_euclidean.rs:292
+  p.pos_rep = (2.0f * p.gamma) * p.b;   // :329
+  p.neg_rate = (uint32_t)o.negative_sample_rate;
+  p.n_vertices = (uint32_t)o.manifold->n_vertices;
+  p.dim = (uint32_t)o.dim;
+  p.seed = o.seed;
+  return p;
+}
+
+// optimizer.rs:297-366.
+void step_epochs_impl(umap_optimizer& o, uint64_t n_ep) {
+  if (o.current_epoch + n_ep > o.total_epochs)
+    throw Error(OVERSTEP, "Cannot step " + std::to_string(n_ep) + " epochs: would exceed total_epochs " +
+                              std::to_string(o.total_epochs) + " (current: " +
+                              std::to_string(o.current_epoch) + ")");
+  cudaStream_t s = o.s();
+  const uint64_t nd = o.n * o.dim;
+  float* live = o.emb2.p;
+  float* snap = o.emb2.p + nd;
+  d2d(snap, live, nd, s);  // :314 embedding_copy
+  const SgdParams p = sgd_params(o);
+  cudaEvent_t ev[2];
+  UB_CUDA(cudaEventCreate(&ev[0]));
+  UB_CUDA(cudaEventCreate(&ev[1]));
+  UB_CUDA(cudaEventRecord(ev[0], s));
+  for (uint64_t epoch = o.current_epoch; epoch < o.current_epoch + n_ep; ++epoch) {
+    const float alpha = o.initial_alpha * (1.0f - ((float)epoch / (float)o.total_epochs));  // :317
+    sgd_epoch(o.layout, live, snap, p, (uint32_t)epoch, alpha, s);
+  }
+  UB_CUDA(cudaEventRecord(ev[1], s));
+  UB_CUDA(cudaStreamSynchronize(s));
+  float ms = 0.0f;
+  (void)cudaEventElapsedTime(&ms, ev[0], ev[1]);
+  (void)cudaEventDestroy(ev[0]);
+  (void)cudaEventDestroy(ev[1]);
+  o.last_step_ms = ms;
+  if (getenv("UMAP_B200_LOG"))
+    fprintf(stderr, "[umap_b200] duration_ms=%.3f step_epochs %llu epochs (%.4f ms/epoch)\n", ms,
+            (unsigned long long)n_ep, n_ep ? ms / n_ep : 0.0);
+  o.current_epoch += n_ep;
+}
+
+std::unique_ptr<umap_fitted> into_fitted_impl(std::unique_ptr<umap_optimizer> o, const umap_config& c) {
+  auto f = std::make_unique<umap_fitted>();
+  cudaStream_t s = o->s();
+  set_l2_window(*o, false);
+  f->n = o->n;
+  f->dim = o->dim;
+  f->embedding.alloc(o->n * o->dim, s);
+  d2d(f->embedding.p, o->emb2.p, o->n * o->dim, s);
+  f->config = c;
+  o->emb2.reset();
+  o->layout = SgdLayout();
+  f->manifold = std::move(o->manifold);
+  UB_CUDA(cudaStreamSynchronize(f->s()));
+  return f;
+}
+
+std::unique_ptr<umap_fitted> fit_impl(const umap_config& c, uint64_t n_samples, const uint32_t* idx,
+                                      const float* dist, uint64_t rows, uint64_t cols, const float* init,
+                                      uint64_t irows, uint64_t icols, bool host) {
+  // embedding.rs:284-297
+  if (icols != c.n_components)
+    throw Error(INVALID_ARGUMENT, "init has " + std::to_string(icols) + " components but n_components is " +
+                                      std::to_string(c.n_components));
+  if (irows != n_samples)
+    throw Error(INVALID_ARGUMENT, "init has " + std::to_string(irows) + " samples but data has " +
+                                      std::to_string(n_samples) + " samples");
+  std::unique_ptr<umap_manifold> m;
+  if (host) {
+    std::string err = validate_parameters(c, n_samples, rows, cols);
+    if (!err.empty()) throw Error(INVALID_ARGUMENT, err);
+    // Upload on a temporary stream-ordered allocation of the manifold's future stream.
+    cudaStream_t s0;
+    UB_CUDA(cudaStreamCreateWithFlags(&s0, cudaStreamNonBlocking));
+    struct SGuard { cudaStream_t s; ~SGuard() { (void)cudaStreamSynchronize(s); (void)cudaStreamDestroy(s); } } g{s0};
+    DevBuf<uint32_t> di(rows * cols, s0);
+    DevBuf<float> dd(rows * cols, s0);
+    h2d(di.p, idx, rows * cols, s0);
+    h2d(dd.p, dist, rows * cols, s0);
+    UB_CUDA(cudaStreamSynchronize(s0));
+    m = learn_manifold_impl(c, n_samples, di.p, dd.p, rows, cols);
+    UB_CUDA(cudaStreamSynchronize(m->s()));
+  } else {
+    m = learn_manifold_impl(c, n_samples, idx, dist, rows, cols);
+  }
+  const uint64_t total = c.has_n_epochs ? c.n_epochs : (n_samples <= 10000 ? 500 : 200);  // :304-308
+  auto o = optimizer_new_impl(std::move(m), init, host, irows, icols, total, c, UMAP_METRIC_EUCLIDEAN);
+  step_epochs_impl(*o, total);  // :321
+  auto f = into_fitted_impl(std::move(o), c);
+  nan_empty_rows(f->manifold->indptr.p, f->n, (uint32_t)f->dim, f->embedding.p, f->s());  // :327-334
+  UB_CUDA(cudaStreamSynchronize(f->s()));
+  return f;
+}
+
+// ------------------------------------------------------------------ serialization
+constexpr char MAGIC[8] = {'U', 'M', 'A', 'P', 'B', '2', '0', '0'};
+constexpr uint32_t FORMAT_VERSION = 1;
+enum Kind : uint32_t { KIND_MANIFOLD = 1, KIND_OPTIMIZER = 2, KIND_FITTED = 3 };
+
+struct Writer {
+  std::vector<uint8_t> b;
+  void raw(const void* p, size_t n) {
+    const uint8_t* c = (const uint8_t*)p;
+    b.insert(b.end(), c, c + n);
+  }
+  template <class T>
+  void put(T v) { raw(&v, sizeof v); }
+};
+
+struct Reader {
+  const uint8_t* p;
+  uint64_t n, off = 0;
+  void raw(void* dst, uint64_t len) {
+    if (len > n - off) throw Error(FORMAT, "checkpoint truncated");
+    memcpy(dst, p + off, len);
+    off += len;
+  }
+  template <class T>
+  T get() {
+    T v;
+    raw(&v, sizeof v);
+    return v;
+  }
+  uint64_t count(uint64_t elem_size) {
+    uint64_t c = get<uint64_t>();
+    if (elem_size && c > (n - off) / elem_size) throw Error(FORMAT, "checkpoint truncated (array length)");
+    return c;
+  }
+};
+
+void write_header(Writer& w, Kind k) {
+  w.raw(MAGIC, 8);
+  w.put<uint32_t>(FORMAT_VERSION);
+  w.put<uint32_t>(k);
+}
+void read_header(Reader& r, Kind k) {
+  char m[8];
+  r.raw(m, 8);
+  if (memcmp(m, MAGIC, 8) != 0) throw Error(FORMAT, "not a umap_b200 checkpoint (bad magic)");
+  uint32_t v = r.get<uint32_t>();
+  if (v != FORMAT_VERSION) throw Error(FORMAT, "unsupported checkpoint version " + std::to_string(v));
+  uint32_t kk = r.get<uint32_t>();
+  if (kk != k) throw Error(FORMAT, "checkpoint holds a different object kind");
+}
+
+template <class T>
+void put_device_array(Writer& w, const T* dev, uint64_t n, cudaStream_t s) {
+  w.put<uint64_t>(n);
+  size_t at = w.b.size();
+  w.b.resize(at + n * sizeof(T));
+  d2h((T*)(w.b.data() + at), dev, n, s);
+  UB_CUDA(cudaStreamSynchronize(s));
+}
+template <class T>
+void get_device_array(Reader& r, DevBuf<T>& buf, uint64_t expect, cudaStream_t s) {
+  uint64_t n = r.count(sizeof(T));
+  if (expect != UINT64_MAX && n != expect) throw Error(FORMAT, "checkpoint array length mismatch");
+  buf.alloc(n, s);
+  if (n) {
+    h2d(buf.p, (const T*)(r.p + r.off), n, s);
+    UB_CUDA(cudaStreamSynchronize(s));
+  }
+  r.off += n * sizeof(T);
+}
+
+// LearnedManifold fields (manifold.rs:14-38): graph, sigmas, rhos, n_vertices, a, b.
+void write_manifold(Writer& w, const umap_manifold& m) {
+  cudaStream_t s = m.s();
+  w.put<uint64_t>(m.n_vertices);  // graph shape (n, n)
+  w.put<uint64_t>(m.n_vertices);
+  put_device_array(w, m.indptr.p, m.n_vertices + 1, s);
+  put_device_array(w, m.indices.p, m.nnz, s);
+  put_device_array(w, m.data.p, m.nnz, s);
+  put_device_array(w, m.sigmas.p, m.n_vertices, s);
+  put_device_array(w, m.rhos.p, m.n_vertices, s);
+  w.put<uint64_t>(m.n_vertices);
+  w.put<float>(m.a);
+  w.put<float>(m.b);
+  w.put<uint64_t>(m.edges_removed);
+  w.put<uint64_t>(m.vertices_disconnected);
+}
+
+std::unique_ptr<umap_manifold> read_manifold(Reader& r) {
+  auto m = std::make_unique<umap_manifold>();
+  m->stream = std::make_unique<Stream>();
+  cudaStream_t s = m->s();
+  uint64_t rows = r.get<uint64_t>(), cols = r.get<uint64_t>();
+  if (rows != cols) throw Error(FORMAT, "graph must be square");
+  get_device_array(r, m->indptr, rows + 1, s);
+  get_device_array(r, m->indices, UINT64_MAX, s);
+  m->nnz = m->indices.n;
+  get_device_array(r, m->data, m->nnz, s);
+  get_device_array(r, m->sigmas, rows, s);
+  get_device_array(r, m->rhos, rows, s);
+  m->n_vertices = r.get<uint64_t>();
+  if (m->n_vertices != rows) throw Error(FORMAT, "n_vertices does not match the graph shape");
+  m->a = r.get<float>();
+  m->b = r.get<float>();
+  m->edges_removed = r.get<uint64_t>();
+  m->vertices_disconnected = r.get<uint64_t>();
+  uint64_t last = 0;
+  d2h(&last, m->indptr.p + rows, 1, s);
+  UB_CUDA(cudaStreamSynchronize(s));
+  if (last != m->nnz) throw Error(FORMAT, "graph indptr does not match nnz");
+  return m;
+}
+
+void write_config(Writer& w, const umap_config& c) {
+  w.put(c.n_components);
+  w.put(c.min_dist); w.put(c.spread); w.put(c.has_a); w.put(c.a); w.put(c.has_b); w.put(c.b);
+  w.put(c.n_neighbors); w.put(c.local_connectivity); w.put(c.set_op_mix_ratio);
+  w.put(c.has_disconnection_distance); w.put(c.disconnection_distance); w.put(c.symmetrize);
+  w.put(c.has_n_epochs); w.put(c.n_epochs); w.put(c.learning_rate); w.put(c.negative_sample_rate);
+  w.put(c.repulsion_strength);
+}
+umap_config read_config(Reader& r) {
+  umap_config c{};
+  c.n_components = r.get<uint64_t>();
+  c.min_dist = r.get<float>(); c.spread = r.get<float>(); c.has_a = r.get<int32_t>(); c.a = r.get<float>();
+  c.has_b = r.get<int32_t>(); c.b = r.get<float>();
+  c.n_neighbors = r.get<uint64_t>(); c.local_connectivity = r.get<float>(); c.set_op_mix_ratio = r.get<float>();
+  c.has_disconnection_distance = r.get<int32_t>(); c.disconnection_distance = r.get<float>();
+  c.symmetrize = r.get<int32_t>();
+  c.has_n_epochs = r.get<int32_t>(); c.n_epochs = r.get<uint64_t>(); c.learning_rate = r.get<float>();
+  c.negative_sample_rate = r.get<uint64_t>(); c.repulsion_strength = r.get<float>();
+  return c;
+}
+
+int copy_out(const Writer& w, uint8_t* buf, uint64_t cap, uint64_t* needed) {
+  if (needed) *needed = w.b.size();
+  if (buf && cap) memcpy(buf, w.b.data(), std::min<uint64_t>(cap, w.b.size()));
+  return (buf && cap < w.b.size()) ? UMAP_ERR_INVALID_ARGUMENT : UMAP_OK;
+}
+
+}  // namespace
+}  // namespace ub
+
+using namespace ub;
+
+// =================================================================== C ABI
+extern "C" {
+
+const char* umap_last_error(void) { return ub::g_last_error.c_str(); }
+int umap_abi_version(void) { return UMAP_B200_ABI_VERSION; }
+
+int umap_config_default(umap_config* out) {
+  API_BEGIN
+  need(out, "out");
+  memset(out, 0, sizeof *out);
+  out->n_components = 2;
+  out->min_dist = 0.1f;
+  out->spread = 1.0f;
+  out->n_neighbors = 15;
+  out->local_connectivity = 1.0f;
+  out->set_op_mix_ratio = 1.0f;
+  out->symmetrize = 1;
+  out->learning_rate = 1.0f;
+  out->negative_sample_rate = 5;
+  out->repulsion_strength = 1.0f;
+  API_END
+}
+
+int umap_find_ab_params(float spread, float min_dist, float* a_out, float* b_out) {
+  API_BEGIN
+  need(a_out, "a_out");
+  need(b_out, "b_out");
+  find_ab_params(spread, min_dist, a_out, b_out);
+  API_END
+}
+
+int umap_learn_manifold(const umap_config* cfg, uint64_t n_samples, const uint32_t* idx, const float* dist,
+                        uint64_t rows, uint64_t cols, umap_manifold** out) {
+  API_BEGIN
+  need(cfg, "cfg"); need(idx, "knn_indices"); need(dist, "knn_dists"); need(out, "out");
+  *out = nullptr;
+  std::string err = validate_parameters(*cfg, n_samples, rows, cols);
+  if (!err.empty()) throw Error(INVALID_ARGUMENT, err);
+  cudaStream_t s0;
+  UB_CUDA(cudaStreamCreateWithFlags(&s0, cudaStreamNonBlocking));
+  struct SGuard { cudaStream_t s; ~SGuard() { (void)cudaStreamSynchronize(s); (void)cudaStreamDestroy(s); } } g{s0};
+  DevBuf<uint32_t> di(rows * cols, s0);
+  DevBuf<float> dd(rows * cols, s0);
+  h2d(di.p, idx, rows * cols, s0);
+  h2d(dd.p, dist, rows * cols, s0);
+  UB_CUDA(cudaStreamSynchronize(s0));
+  auto m = learn_manifold_impl(*cfg, n_samples, di.p, dd.p, rows, cols);
+  UB_CUDA(cudaStreamSynchronize(m->s()));
+  *out = m.release();
+  API_END
+}
+
+int umap_learn_manifold_device(const umap_config* cfg, uint64_t n_samples, const uint32_t* idx,
+                               const float* dist, uint64_t rows, uint64_t cols, umap_manifold** out) {
+  API_BEGIN
+  need(cfg, "cfg"); need(idx, "knn_indices"); need(dist, "knn_dists"); need(out, "out");
+  *out = nullptr;
+  UB_CUDA(cudaDeviceSynchronize());
+  auto m = learn_manifold_impl(*cfg, n_samples, idx, dist, rows, cols);
+  *out = m.release();
+  API_END
+}
+
+int umap_manifold_n_vertices(const umap_manifold* m, uint64_t* out) {
+  API_BEGIN
+  need(m, "manifold"); need(out, "out");
+  *out = m->n_vertices;
+  API_END
+}
+
+int umap_manifold_curve_params(const umap_manifold* m, float* a, float* b) {
+  API_BEGIN
+  need(m, "manifold"); need(a, "a"); need(b, "b");
+  *a = m->a;
+  *b = m->b;
+  API_END
+}
+
+int umap_manifold_graph_nnz(const umap_manifold* m, uint64_t* nnz) {
+  API_BEGIN
+  need(m, "manifold"); need(nnz, "nnz");
+  *nnz = m->nnz;
+  API_END
+}
+
+int umap_manifold_graph_copy(const umap_manifold* m, uint64_t* indptr, uint32_t* indices, float* data) {
+  API_BEGIN
+  need(m, "manifold");
+  m->stream->activate();
+  if (indptr) d2h(indptr, m->indptr.p, m->n_vertices + 1, m->s());
+  if (indices) d2h(indices, m->indices.p, m->nnz, m->s());
+  if (data) d2h(data, m->data.p, m->nnz, m->s());
+  m->stream->sync();
+  API_END
+}
+
+int umap_manifold_sigmas_rhos(const umap_manifold* m, float* sigmas, float* rhos) {
+  API_BEGIN
+  need(m, "manifold");
+  m->stream->activate();
+  if (sigmas) d2h(sigmas, m->sigmas.p, m->n_vertices, m->s());
+  if (rhos) d2h(rhos, m->rhos.p, m->n_vertices, m->s());
+  m->stream->sync();
+  API_END
+}
+
+int umap_manifold_disconnection_counts(const umap_manifold* m, uint64_t* edges_removed,
+                                       uint64_t* vertices_disconnected) {
+  API_BEGIN
+  need(m, "manifold");
+  if (edges_removed) *edges_removed = m->edges_removed;
+  if (vertices_disconnected) *vertices_disconnected = m->vertices_disconnected;
+  API_END
+}
+
+int umap_manifold_clone(const umap_manifold* m, umap_manifold** out) {
+  API_BEGIN
+  need(m, "manifold"); need(out, "out");
+  *out = nullptr;
+  m->stream->activate();
+  *out = clone_manifold(*m).release();
+  API_END
+}
+
+int umap_manifold_free(umap_manifold* m) {
+  API_BEGIN
+  if (m) {
+    m->stream->activate();
+    delete m;
+  }
+  API_END
+}
+
+int umap_optimizer_new(umap_manifold* manifold, const float* init, uint64_t rows, uint64_t dims,
+                       uint64_t total_epochs, const umap_config* cfg, int metric_type, umap_optimizer** out) {
+  std::unique_ptr<umap_manifold> owned(manifold);
+  API_BEGIN
+  need(manifold, "manifold"); need(init, "init"); need(cfg, "cfg"); need(out, "out");
+  *out = nullptr;
+  owned->stream->activate();
+  *out = optimizer_new_impl(std::move(owned), init, true, rows, dims, total_epochs, *cfg, metric_type).release();
+  API_END
+}
+
+int umap_optimizer_new_device(umap_manifold* manifold, const float* init, uint64_t rows, uint64_t dims,
+                              uint64_t total_epochs, const umap_config* cfg, int metric_type,
+                              umap_optimizer** out) {
+  std::unique_ptr<umap_manifold> owned(manifold);
+  API_BEGIN
+  need(manifold, "manifold"); need(init, "init"); need(cfg, "cfg"); need(out, "out");
+  *out = nullptr;
+  owned->stream->activate();
+  UB_CUDA(cudaDeviceSynchronize());
+  *out = optimizer_new_impl(std::move(owned), init, false, rows, dims, total_epochs, *cfg, metric_type).release();
+  API_END
+}
+
+int umap_optimizer_step_epochs(umap_optimizer* opt, uint64_t n) {
+  API_BEGIN
+  need(opt, "optimizer");
+  opt->manifold->stream->activate();
+  step_epochs_impl(*opt, n);
+  API_END
+}
+
+int umap_optimizer_current_epoch(const umap_optimizer* opt, uint64_t* out) {
+  API_BEGIN
+  need(opt, "optimizer"); need(out, "out");
+  *out = opt->current_epoch;
+  API_END
+}
+
+int umap_optimizer_total_epochs(const umap_optimizer* opt, uint64_t* out) {
+  API_BEGIN
+  need(opt, "optimizer"); need(out, "out");
+  *out = opt->total_epochs;
+  API_END
+}
+
+int umap_optimizer_remaining_epochs(const umap_optimizer* opt, uint64_t* out) {
+  API_BEGIN
+  need(opt, "optimizer"); need(out, "out");
+  *out = opt->total_epochs - opt->current_epoch;
+  API_END
+}
+
+int umap_optimizer_embedding(const umap_optimizer* opt, float* out) {
+  API_BEGIN
+  need(opt, "optimizer"); need(out, "out");
+  opt->manifold->stream->activate();
+  d2h(out, opt->emb2.p, opt->n * opt->dim, opt->s());
+  opt->manifold->stream->sync();
+  API_END
+}
+
+int umap_optimizer_embedding_device(umap_optimizer* opt, float** dev_ptr) {
+  API_BEGIN
+  need(opt, "optimizer"); need(dev_ptr, "dev_ptr");
+  *dev_ptr = opt->emb2.p;
+  API_END
+}
+
+int umap_optimizer_dims(const umap_optimizer* opt, uint64_t* n_vertices, uint64_t* dims) {
+  API_BEGIN
+  need(opt, "optimizer");
+  if (n_vertices) *n_vertices = opt->n;
+  if (dims) *dims = opt->dim;
+  API_END
+}
+
+int umap_optimizer_manifold(const umap_optimizer* opt, const umap_manifold** out) {
+  API_BEGIN
+  need(opt, "optimizer"); need(out, "out");
+  *out = opt->manifold.get();
+  API_END
+}
+
+int umap_optimizer_into_fitted(umap_optimizer* opt, const umap_config* cfg, umap_fitted** out) {
+  std::unique_ptr<umap_optimizer> owned(opt);
+  API_BEGIN
+  need(opt, "optimizer"); need(cfg, "cfg"); need(out, "out");
+  *out = nullptr;
+  owned->manifold->stream->activate();
+  *out = into_fitted_impl(std::move(owned), *cfg).release();
+  API_END
+}
+
+int umap_optimizer_free(umap_optimizer* opt) {
+  API_BEGIN
+  if (opt) {
+    opt->manifold->stream->activate();
+    delete opt;
+  }
+  API_END
+}
+
+int umap_optimizer_set_seed(umap_optimizer* opt, uint64_t seed) {
+  API_BEGIN
+  need(opt, "optimizer");
+  opt->seed = seed;
+  API_END
+}
+
+int umap_optimizer_n_edges(const umap_optimizer* opt, uint64_t* out) {
+  API_BEGIN
+  need(opt, "optimizer"); need(out, "out");
+  *out = opt->layout.n_edges;
+  API_END
+}
+
+int umap_optimizer_export_edges(const umap_optimizer* opt, uint32_t* head, uint32_t* tail, double* eps,
+                                double* eons, double* eonns, double* epns) {
+  API_BEGIN
+  need(opt, "optimizer");
+  opt->manifold->stream->activate();
+  cudaStream_t s = opt->s();
+  KeptEdges K;
+  compute_kept_edges(*opt, K, true, true);
+  const uint64_t E = K.E;
+  if (head) {
+    DevBuf<uint32_t> h(E, s);
+    head_from_ptr(K.ptr.p, opt->manifold->n_vertices, h.p, s);
+    d2h(head, h.p, E, s);
+    UB_CUDA(cudaStreamSynchronize(s));
+  }
+  if (tail) d2h(tail, K.tail.p, E, s);
+  if (eps) d2h(eps, K.eps.p, E, s);
+  if (eons || eonns || epns) {
+    DevBuf<double> a(E, s), b(E, s), c(E, s);
+    export_state(K.eps.p, E, opt->negative_sample_rate, opt->current_epoch, a.p, b.p, c.p, s);
+    if (eons) d2h(eons, a.p, E, s);
+    if (eonns) d2h(eonns, b.p, E, s);
+    if (epns) d2h(epns, c.p, E, s);
+    UB_CUDA(cudaStreamSynchronize(s));
+  }
+  UB_CUDA(cudaStreamSynchronize(s));
+  API_END
+}
+
+int umap_optimizer_schedule_totals(const umap_optimizer* opt, uint64_t start, uint64_t end, uint64_t* fired,
+                                   uint64_t* negatives) {
+  API_BEGIN
+  need(opt, "optimizer");
+  opt->manifold->stream->activate();
+  cudaStream_t s = opt->s();
+  DevBuf<unsigned long long> d(2, s);
+  schedule_totals(opt->layout, (uint32_t)opt->negative_sample_rate, (uint32_t)start, (uint32_t)end, d.p,
+                  d.p + 1, s);
+  unsigned long long h[2];
+  d2h(h, d.p, 2, s);
+  UB_CUDA(cudaStreamSynchronize(s));
+  if (fired) *fired = h[0];
+  if (negatives) *negatives = h[1];
+  API_END
+}
+
+int umap_optimizer_last_step_ms(const umap_optimizer* opt, float* ms) {
+  API_BEGIN
+  need(opt, "optimizer"); need(ms, "ms");
+  *ms = opt->last_step_ms;
+  API_END
+}
+
+int umap_kernel_launches(uint64_t* out) {
+  API_BEGIN
+  need(out, "out");
+  *out = ub::g_launches.load(std::memory_order_relaxed);
+  API_END
+}
+
+int umap_fitted_embedding(const umap_fitted* f, float* out) {
+  API_BEGIN
+  need(f, "fitted"); need(out, "out");
+  f->manifold->stream->activate();
+  d2h(out, f->embedding.p, f->n * f->dim, f->s());
+  f->manifold->stream->sync();
+  API_END
+}
+
+int umap_fitted_dims(const umap_fitted* f, uint64_t* n_vertices, uint64_t* dims) {
+  API_BEGIN
+  need(f, "fitted");
+  if (n_vertices) *n_vertices = f->n;
+  if (dims) *dims = f->dim;
+  API_END
+}
+
+int umap_fitted_manifold(const umap_fitted* f, const umap_manifold** out) {
+  API_BEGIN
+  need(f, "fitted"); need(out, "out");
+  *out = f->manifold.get();
+  API_END
+}
+
+int umap_fitted_config(const umap_fitted* f, umap_config* out) {
+  API_BEGIN
+  need(f, "fitted"); need(out, "out");
+  *out = f->config;
+  API_END
+}
+
+int umap_fitted_free(umap_fitted* f) {
+  API_BEGIN
+  if (f) {
+    f->manifold->stream->activate();
+    delete f;
+  }
+  API_END
+}
+
+int umap_fit(const umap_config* cfg, uint64_t n_samples, const uint32_t* idx, const float* dist, uint64_t rows,
+             uint64_t cols, const float* init, uint64_t irows, uint64_t icols, umap_fitted** out) {
+  API_BEGIN
+  need(cfg, "cfg"); need(idx, "knn_indices"); need(dist, "knn_dists"); need(init, "init"); need(out, "out");
+  *out = nullptr;
+  *out = fit_impl(*cfg, n_samples, idx, dist, rows, cols, init, irows, icols, true).release();
+  API_END
+}
+
+int umap_fit_device(const umap_config* cfg, uint64_t n_samples, const uint32_t* idx, const float* dist,
+                    uint64_t rows, uint64_t cols, const float* init, uint64_t irows, uint64_t icols,
+                    umap_fitted** out) {
+  API_BEGIN
+  need(cfg, "cfg"); need(idx, "knn_indices"); need(dist, "knn_dists"); need(init, "init"); need(out, "out");
+  *out = nullptr;
+  UB_CUDA(cudaDeviceSynchronize());
+  *out = fit_impl(*cfg, n_samples, idx, dist, rows, cols, init, irows, icols, false).release();
+  API_END
+}
+
+// ---- checkpoints
+int umap_manifold_serialize(const umap_manifold* m, uint8_t* buf, uint64_t cap, uint64_t* needed) {
+  API_BEGIN
+  need(m, "manifold");
+  m->stream->activate();
+  Writer w;
+  write_header(w, KIND_MANIFOLD);
+  write_manifold(w, *m);
+  int rc = copy_out(w, buf, cap, needed);
+  if (rc) throw Error(rc, "buffer too small for the serialized manifold");
+  API_END
+}
+
+int umap_manifold_deserialize(const uint8_t* buf, uint64_t len, umap_manifold** out) {
+  API_BEGIN
+  need(buf, "buf"); need(out, "out");
+  *out = nullptr;
+  Reader r{buf, len};
+  read_header(r, KIND_MANIFOLD);
+  auto m = read_manifold(r);
+  if (r.off != len) throw Error(FORMAT, "trailing bytes after the manifold");
+  *out = m.release();
+  API_END
+}
+
+// Optimizer fields in the reference's declaration order (optimizer.rs:27-56), then this
+// library's extensions (seed, max_val, threshold).
+int umap_optimizer_serialize(const umap_optimizer* o, uint8_t* buf, uint64_t cap, uint64_t* needed) {
+  API_BEGIN
+  need(o, "optimizer");
+  o->manifold->stream->activate();
+  cudaStream_t s = o->s();
+  Writer w;
+  write_header(w, KIND_OPTIMIZER);
+  write_manifold(w, *o->manifold);
+  KeptEdges K;
+  compute_kept_edges(*o, K, true, true);
+  const uint64_t E = K.E;
+  {
+    DevBuf<uint32_t> h(E, s);
+    head_from_ptr(K.ptr.p, o->manifold->n_vertices, h.p, s);
+    put_device_array(w, h.p, E, s);
+  }
+  put_device_array(w, K.tail.p, E, s);
+  put_device_array(w, K.eps.p, E, s);
+  w.put<uint64_t>(o->n);
+  w.put<uint64_t>(o->dim);
+  put_device_array(w, o->emb2.p, o->n * o->dim, s);
+  {
+    DevBuf<double> a(E, s), b(E, s), c(E, s);
+    export_state(K.eps.p, E, o->negative_sample_rate, o->current_epoch, a.p, b.p, c.p, s);
+    put_device_array(w, a.p, E, s);  // epoch_of_next_sample
+    put_device_array(w, b.p, E, s);  // epoch_of_next_negative_sample
+    put_device_array(w, c.p, E, s);  // epochs_per_negative_sample
+  }
+  w.put<uint64_t>(o->current_epoch);
+  w.put<uint64_t>(o->total_epochs);
+  w.put<float>(o->gamma);
+  w.put<float>(o->initial_alpha);
+  w.put<double>((double)o->negative_sample_rate);
+  w.put<uint32_t>((uint32_t)o->metric_type);
+  w.put<uint64_t>(o->seed);
+  w.put<float>(o->max_val);
+  w.put<float>(o->threshold);
+  w.put<float>(o->max_w);
+  int rc = copy_out(w, buf, cap, needed);
+  if (rc) throw Error(rc, "buffer too small for the serialized optimizer");
+  API_END
+}
+
+int umap_optimizer_deserialize(const uint8_t* buf, uint64_t len, umap_optimizer** out) {
+  API_BEGIN
+  need(buf, "buf"); need(out, "out");
+  *out = nullptr;
+  Reader r{buf, len};
+  read_header(r, KIND_OPTIMIZER);
+  auto o = std::make_unique<umap_optimizer>();
+  o->manifold = read_manifold(r);
+  cudaStream_t s = o->s();
+  const uint64_t n = o->manifold->n_vertices;
+  DevBuf<uint32_t> head, tail;
+  DevBuf<double> eps;
+  get_device_array(r, head, UINT64_MAX, s);
+  const uint64_t E = head.n;
+  get_device_array(r, tail, E, s);
+  get_device_array(r, eps, E, s);
+  o->n = r.get<uint64_t>();
+  o->dim = r.get<uint64_t>();
+  if (o->n != n || o->dim < 1 || o->dim > (1u << 20)) throw Error(FORMAT, "embedding shape mismatch");
+  {
+    DevBuf<float> e;
+    get_device_array(r, e, n * o->dim, s);
+    o->emb2.alloc(2 * n * o->dim, s);
+    d2d(o->emb2.p, e.p, n * o->dim, s);
+  }
+  for (int t = 0; t < 3; ++t) {  // schedule state: recomputed from epochs_per_sample
+    uint64_t c = r.count(8);
+    if (c != E) throw Error(FORMAT, "schedule array length mismatch");
+    r.off += c * 8;
+  }
+  o->current_epoch = r.get<uint64_t>();
+  o->total_epochs = r.get<uint64_t>();
+  o->gamma = r.get<float>();
+  o->initial_alpha = r.get<float>();
+  o->negative_sample_rate = (uint64_t)r.get<double>();
+  o->metric_type = (int)r.get<uint32_t>();
+  o->seed = r.get<uint64_t>();
+  o->max_val = r.get<float>();
+  o->threshold = r.get<float>();
+  o->max_w = r.get<float>();
+  if (r.off != len) throw Error(FORMAT, "trailing bytes after the optimizer");
+  if (o->current_epoch > o->total_epochs) throw Error(FORMAT, "current_epoch exceeds total_epochs");
+  if (o->metric_type != UMAP_METRIC_EUCLIDEAN) throw Error(UNSUPPORTED, "only Euclidean optimizers are supported");
+  // Validate the edge list (row-major by head, heads and tails < n) on the host.
+  std::vector<uint32_t> hh(E), tt(E);
+  d2h(hh.data(), head.p, E, s);
+  d2h(tt.data(), tail.p, E, s);
+  UB_CUDA(cudaStreamSynchronize(s));
+  for (uint64_t i = 0; i < E; ++i) {
+    if (hh[i] >= n || tt[i] >= n) throw Error(FORMAT, "edge index out of range");
+    if (i && hh[i] < hh[i - 1]) throw Error(FORMAT, "edges are not ordered by head");
+  }
+  DevBuf<uint64_t> ptr(n + 1, s);
+  segment_starts(head.p, E, n, ptr.p, s);
+  build_sgd_layout(ptr.p, tail.p, eps.p, n, 0, o->layout, s);
+  set_l2_window(*o, true);
+  UB_CUDA(cudaStreamSynchronize(s));
+  *out = o.release();
+  API_END
+}
+
+// FittedUmap fields (embedding.rs:438-443): embedding, manifold, config.
+int umap_fitted_serialize(const umap_fitted* f, uint8_t* buf, uint64_t cap, uint64_t* needed) {
+  API_BEGIN
+  need(f, "fitted");
+  f->manifold->stream->activate();
+  Writer w;
+  write_header(w, KIND_FITTED);
+  w.put<uint64_t>(f->n);
+  w.put<uint64_t>(f->dim);
+  put_device_array(w, f->embedding.p, f->n * f->dim, f->s());
+  write_manifold(w, *f->manifold);
+  write_config(w, f->config);
+  int rc = copy_out(w, buf, cap, needed);
+  if (rc) throw Error(rc, "buffer too small for the serialized fitted model");
+  API_END
+}
+
+int umap_fitted_deserialize(const uint8_t* buf, uint64_t len, umap_fitted** out) {
+  API_BEGIN
+  need(buf, "buf"); need(out, "out");
+  *out = nullptr;
+  Reader r{buf, len};
+  read_header(r, KIND_FITTED);
+  auto f = std::make_unique<umap_fitted>();
+  f->n = r.get<uint64_t>();
+  f->dim = r.get<uint64_t>();
+  if (f->dim > (1u << 20)) throw Error(FORMAT, "embedding shape mismatch");
+  // The embedding precedes the manifold (which owns the stream): stage it on the host.
+  uint64_t cnt = r.count(4);
+  if (cnt != f->n * f->dim) throw Error(FORMAT, "embedding length mismatch");
+  const float* host_emb = (const float*)(r.p + r.off);
+  r.off += cnt * 4;
+  f->manifold = read_manifold(r);
+  f->config = read_config(r);
+  if (r.off != len) throw Error(FORMAT, "trailing bytes after the fitted model");
+  if (f->manifold->n_vertices != f->n) throw Error(FORMAT, "embedding rows do not match the manifold");
+  f->embedding.alloc(cnt, f->s());
+  std::vector<float> tmp(host_emb, host_emb + cnt);
+  h2d(f->embedding.p, tmp.data(), cnt, f->s());
+  UB_CUDA(cudaStreamSynchronize(f->s()));
+  *out = f.release();
+  API_END
+}
+
+// ---- kernel-level entry points
+int umap_smooth_knn_dist_device(const float* dists, uint64_t n, uint64_t k, uint64_t n_iter,
+                                float local_connectivity, float bandwidth, float* sigmas, float* rhos) {
+  API_BEGIN
+  need(dists, "dists"); need(sigmas, "sigmas"); need(rhos, "rhos");
+  if (k < 1) throw Error(INVALID_ARGUMENT, "k must be >= 1");
+  cudaStream_t s;
+  UB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  struct SGuard { cudaStream_t s; ~SGuard() { (void)cudaStreamSynchronize(s); (void)cudaStreamDestroy(s); } } g{s};
+  UB_CUDA(cudaDeviceSynchronize());
+  GraphParams gp{};
+  gp.local_connectivity = local_connectivity;
+  const float lcf = floorf(local_connectivity);
+  gp.interpolation = local_connectivity - lcf;
+  gp.lc_usize = rust_f32_as_usize(local_connectivity);
+  gp.lc_index = rust_f32_as_usize(lcf);
+  gp.target = log2f((float)k) * bandwidth;
+  gp.n_iter = (int)std::min<uint64_t>(n_iter, 1u << 30);
+  smooth_knn(dists, n, k, gp, sigmas, rhos, s);
+  UB_CUDA(cudaStreamSynchronize(s));
+  API_END
+}
+
+int umap_radix_sort_pairs_device(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
+                                 uint32_t* vals_out, uint64_t n, int end_bit) {
+  API_BEGIN
+  need(keys_in, "keys_in"); need(keys_out, "keys_out"); need(vals_out, "values_out");
+  cudaStream_t s;
+  UB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  struct SGuard { cudaStream_t s; ~SGuard() { (void)cudaStreamSynchronize(s); (void)cudaStreamDestroy(s); } } g{s};
+  UB_CUDA(cudaDeviceSynchronize());
+  radix_sort_pairs(keys_in, vals_in, keys_out, vals_out, n, end_bit, s);
+  UB_CUDA(cudaStreamSynchronize(s));
+  API_END
+}
+
+}  // extern "C"

@@ -1,0 +1,691 @@
+// Edge pruning + task/slice layout (K5), init normalisation (K6) and the Hogwild SGD epoch
+// (K7).
+//
+// Layout.  The kept edges of the symmetric graph are grouped by head row and cut into tasks
+// of at most `chunk` edges (see SgdLayout).  A warp owns a slice of 32 tasks and a lane owns
+// one task, keeping the head row's live embedding in registers.  The reference writes a
+// head row only from edges whose head it is (optimize_layout_euclidean.rs:281-306, :338),
+// so a task that is a whole row reproduces the reference's sequential per-row order with
+// no lost head updates; the rare long rows (kNN hubs) are split so that one row cannot
+// serialise an epoch, and each partial task merges its head delta with an atomic add.
+// Tail moves and negative samples touch the per-call snapshot buffer with racy loads and
+// stores, as the reference does.
+//
+// Schedule.  The reference keeps four f64 arrays per edge (optimizer.rs:33-43).  Here one
+// u32 per edge holds Q = ceil(2^32 / epochs_per_sample) and the state is recomputed in
+// exact integer arithmetic: the edge has fired m(n) = (n*Q) >> 32 times by epoch n, so it
+// fires at n iff m(n) > m(n-1) (at most once per epoch, never at epoch 0; :277, :308), and
+// a firing with index m draws y(n) - y(p) negatives, y(x) = (x*neg*Q) >> 32 and p the epoch
+// of firing m-1 (y(n) - 1 for the first firing): the closed form of :310-311 / :343.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <cstdlib>
+#include <vector>
+
+#include "ub_internal.hpp"
+
+namespace ub {
+namespace {
+
+constexpr uint32_t PAD_ROW = 0xFFFFFFFFu;
+
+// ------------------------------------------------------------------------------ Philox
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as easy as 1, 2, 3",
+// SC'11): counter-based, so every (seed, entry, epoch, block) has its own stream.
+__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k) {
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    const uint32_t hi0 = __umulhi(0xD2511F53u, c.x), lo0 = 0xD2511F53u * c.x;
+    const uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u * c.z;
+    c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
+    k.x += 0x9E3779B9u;
+    k.y += 0xBB67AE85u;
+  }
+  return c;
+}
+
+// ------------------------------------------------------------------------------ schedule
+__host__ __device__ __forceinline__ uint32_t q_minus_1(double eps) {
+  if (!(eps > 0.0)) return 0u;
+  const double x = ceil(4294967296.0 / eps);
+  if (x >= 4294967296.0) return 0xFFFFFFFFu;
+  if (x < 1.0) return 0u;
+  return (uint32_t)x - 1u;
+}
+__device__ __forceinline__ uint64_t fires_by(uint64_t n, uint64_t Q) { return (n * Q) >> 32; }
+// Smallest epoch x with fires_by(x) >= m.
+__device__ __forceinline__ uint64_t fire_epoch(uint64_t m, uint64_t Q) {
+  const float est = (float)m * __fdividef(4294967296.0f, (float)Q);
+  uint64_t x = est > 0.0f ? (uint64_t)ceilf(est) : 0ull;
+  for (int t = 0; t < 8 && x > 0 && fires_by(x - 1, Q) >= m; ++t) --x;
+  for (int t = 0; t < 8 && fires_by(x, Q) < m; ++t) ++x;
+  return x;
+}
+// Negatives drawn by the firing at epoch n with index m >= 1.
+__device__ __forceinline__ uint32_t negatives_at(uint64_t n, uint64_t m, uint64_t Q, uint64_t negQ) {
+  const int64_t y = (int64_t)((n * negQ) >> 32);
+  const int64_t prev = m <= 1 ? 1 : (int64_t)((fire_epoch(m - 1, Q) * negQ) >> 32);
+  const int64_t d = y - prev;
+  return d > 0 ? (uint32_t)d : 0u;
+}
+// Negatives drawn in total after m firings.
+__device__ __forceinline__ uint64_t negatives_after(uint64_t m, uint64_t Q, uint64_t negQ) {
+  if (m == 0) return 0;
+  const int64_t t = (int64_t)((fire_epoch(m, Q) * negQ) >> 32) - 1;
+  return t > 0 ? (uint64_t)t : 0ull;
+}
+
+// Rust f32::clamp(-4, 4) (utils/clip.rs:13-15): NaN passes through.
+__device__ __forceinline__ float clip4(float v) {
+  float x = v;
+  if (x < -4.0f) x = -4.0f;
+  if (x > 4.0f) x = 4.0f;
+  return x;
+}
+
+// ------------------------------------------------------------------------------ K7
+constexpr int PF = 8;        // entries loaded per lane per batch (coalesced across the warp)
+constexpr int NEG_BATCH = 8; // negative-sample rows fetched together
+
+template <int DIM>
+__device__ __forceinline__ void load_row(float (&v)[DIM], const float* p) {
+  if constexpr (DIM == 2) {
+    const float2 t = *reinterpret_cast<const float2*>(p);
+    v[0] = t.x;
+    v[1] = t.y;
+  } else if constexpr (DIM == 4) {
+    const float4 t = *reinterpret_cast<const float4*>(p);
+    v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+  } else {
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) v[d] = p[d];
+  }
+}
+template <int DIM>
+__device__ __forceinline__ void store_row(float* p, const float (&v)[DIM]) {
+  if constexpr (DIM == 2) {
+    *reinterpret_cast<float2*>(p) = make_float2(v[0], v[1]);
+  } else if constexpr (DIM == 4) {
+    *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+  } else {
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) p[d] = v[d];
+  }
+}
+
+// Tail move (optimize_layout_euclidean.rs:303-305) as a fire-and-forget atomic add.  The
+// reference's racy read-modify-write rarely collides on a CPU (a vertex's few tail moves per
+// epoch come from rows processed at different times); with every row of an epoch in flight
+// at once, plain stores would drop most of them, so the add is atomic to keep the
+// reference's statistics.
+template <int DIM>
+__device__ __forceinline__ void sub_row(float* p, const float (&g)[DIM]) {
+  if constexpr (DIM == 2) {
+    atomicAdd(reinterpret_cast<float2*>(p), make_float2(-g[0], -g[1]));
+  } else if constexpr (DIM == 4) {
+    atomicAdd(reinterpret_cast<float4*>(p), make_float4(-g[0], -g[1], -g[2], -g[3]));
+  } else {
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) atomicAdd(p + d, -g[d]);
+  }
+}
+
+// One fired edge (optimize_layout_euclidean.rs:278-343): attractive step on (head, tail),
+// then `nneg` negative samples, all reading the snapshot buffer.  The tail row and a batch
+// of negative rows are fetched together before the (sequential) updates of `cur`.
+template <int DIM>
+__device__ __forceinline__ void fired_edge(float (&cur)[DIM], uint32_t r, uint32_t k, uint32_t nneg,
+                                           float* snap, const SgdParams& p, float alpha, uint64_t idx,
+                                           uint32_t epoch, uint2 key) {
+  const float a = p.a, b = p.b;
+  float* oth = snap + (uint64_t)k * DIM;
+  float o[DIM];
+  load_row<DIM>(o, oth);
+  uint32_t kk[NEG_BATCH];
+  float ob[NEG_BATCH][DIM];
+  const uint32_t first = nneg < NEG_BATCH ? nneg : NEG_BATCH;
+  {
+    const uint4 r0 = philox4x32_10(make_uint4((uint32_t)idx, (uint32_t)(idx >> 32), epoch, 0u), key);
+    const uint4 r1 = first > 4 ? philox4x32_10(make_uint4((uint32_t)idx, (uint32_t)(idx >> 32), epoch, 1u), key)
+                               : make_uint4(0, 0, 0, 0);
+    const uint32_t rv[8] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w};
+#pragma unroll
+    for (int q = 0; q < NEG_BATCH; ++q) {
+      kk[q] = __umulhi(rv[q], p.n_vertices);
+      if ((uint32_t)q < first) load_row<DIM>(ob[q], snap + (uint64_t)kk[q] * DIM);
+    }
+  }
+  // attractive step (:284-306)
+  float ds = 0.0f;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) { const float df = cur[d] - o[d]; ds += df * df; }
+  float gc = 0.0f;
+  if (ds > 0.0f) {
+    const float pb = __powf(ds, b);
+    gc = __fdividef(p.neg_attr * pb, ds * (a * pb * ds + 1.0f));
+  }
+  float g[DIM];
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) {
+    g[d] = clip4(gc * (cur[d] - o[d])) * alpha;
+    cur[d] += g[d];
+  }
+  sub_row<DIM>(oth, g);
+  // negative samples (:313-341)
+  for (uint32_t q0 = 0; q0 < nneg; q0 += NEG_BATCH) {
+    if (q0 > 0) {  // rare: more than NEG_BATCH negatives in one firing
+      const uint32_t blk = q0 / 4;
+      const uint4 r0 = philox4x32_10(make_uint4((uint32_t)idx, (uint32_t)(idx >> 32), epoch, blk), key);
+      const uint4 r1 = philox4x32_10(make_uint4((uint32_t)idx, (uint32_t)(idx >> 32), epoch, blk + 1), key);
+      const uint32_t rv[8] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w};
+#pragma unroll
+      for (int q = 0; q < NEG_BATCH; ++q) {
+        kk[q] = __umulhi(rv[q], p.n_vertices);
+        if (q0 + q < nneg) load_row<DIM>(ob[q], snap + (uint64_t)kk[q] * DIM);
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < NEG_BATCH; ++q) {
+      if (q0 + q >= nneg) break;
+      if (kk[q] == r) continue;
+      float dsn = 0.0f;
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) { const float df = cur[d] - ob[q][d]; dsn += df * df; }
+      float gr = 0.0f;
+      if (dsn > 0.0f) {
+        const float pb = __powf(dsn, b);
+        gr = __fdividef(p.pos_rep, (0.001f + dsn) * (a * pb * dsn + 1.0f));
+      }
+      if (gr > 0.0f) {
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) cur[d] += clip4(gr * (cur[d] - ob[q][d])) * alpha;
+      }
+    }
+  }
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(256) sgd_epoch_kernel(
+    const uint64_t* __restrict__ slice_base, const uint32_t* __restrict__ slice_width,
+    const uint32_t* __restrict__ split_mask, const uint32_t* __restrict__ rowid,
+    const uint2* __restrict__ entry, uint64_t n_slices, float* __restrict__ live, float* snap,
+    SgdParams p, uint32_t epoch, float alpha) {
+  const uint64_t slice = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t lane = threadIdx.x & 31;
+  if (slice >= n_slices) return;
+  const uint32_t r = rowid[slice * 32 + lane];
+  const uint32_t width = slice_width[slice];
+  const uint64_t base = slice_base[slice];
+  const bool split = (split_mask[slice] >> lane) & 1u;
+  const bool active = r != PAD_ROW;
+  float cur[DIM], start[DIM];
+  float* hrow = live + (uint64_t)(active ? r : 0) * DIM;
+  if (active) load_row<DIM>(cur, hrow);
+  else
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) cur[d] = 0.0f;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) start[d] = cur[d];
+  const uint64_t n = epoch;
+  const uint64_t negQf = p.neg_rate;
+  const uint2 key = make_uint2((uint32_t)p.seed, (uint32_t)(p.seed >> 32));
+
+  for (uint32_t e0 = 0; e0 < width; e0 += PF) {
+    uint2 ent[PF];
+    uint32_t mask = 0;
+#pragma unroll
+    for (int j = 0; j < PF; ++j) {
+      const uint32_t e = e0 + j;
+      ent[j] = e < width ? __ldcs(entry + base + (uint64_t)e * 32 + lane) : make_uint2(0u, 0u);
+      const uint64_t Q = (uint64_t)ent[j].y + 1ull;
+      if (n > 0 && fires_by(n, Q) > fires_by(n - 1, Q)) mask |= 1u << j;
+    }
+    while (mask) {
+      const int j = __ffs(mask) - 1;
+      mask &= mask - 1;
+      uint2 en = ent[0];
+#pragma unroll
+      for (int t = 1; t < PF; ++t)
+        if (t == j) en = ent[t];
+      const uint64_t Q = (uint64_t)en.y + 1ull;
+      const uint64_t m = fires_by(n, Q);
+      const uint32_t nneg = negatives_at(n, m, Q, negQf * Q);
+      const uint64_t idx = base + (uint64_t)(e0 + j) * 32 + lane;
+      fired_edge<DIM>(cur, r, en.x, nneg, snap, p, alpha, idx, epoch, key);
+    }
+  }
+  if (active) {
+    if (split) {
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) atomicAdd(hrow + d, cur[d] - start[d]);
+    } else {
+      store_row<DIM>(hrow, cur);
+    }
+  }
+}
+
+// Generic dimension (any n_components): same algorithm, head row in global memory (owned
+// by this lane for whole-row tasks; split tasks accumulate their delta in place with
+// atomics).
+__global__ void __launch_bounds__(256) sgd_epoch_generic(
+    const uint64_t* __restrict__ slice_base, const uint32_t* __restrict__ slice_width,
+    const uint32_t* __restrict__ split_mask, const uint32_t* __restrict__ rowid,
+    const uint2* __restrict__ entry, uint64_t n_slices, float* __restrict__ live, float* snap,
+    SgdParams p, uint32_t epoch, float alpha) {
+  const uint64_t slice = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t lane = threadIdx.x & 31;
+  if (slice >= n_slices) return;
+  const uint32_t r = rowid[slice * 32 + lane];
+  if (r == PAD_ROW) return;
+  const uint32_t width = slice_width[slice];
+  const uint64_t base = slice_base[slice];
+  const bool split = (split_mask[slice] >> lane) & 1u;
+  const uint32_t dim = p.dim;
+  float* cur = live + (uint64_t)r * dim;
+  const uint64_t n = epoch;
+  const uint2 key = make_uint2((uint32_t)p.seed, (uint32_t)(p.seed >> 32));
+  const float a = p.a, b = p.b;
+  auto add = [&](uint32_t d, float v) {
+    if (split) atomicAdd(cur + d, v);
+    else cur[d] += v;
+  };
+  for (uint32_t e = 0; e < width; ++e) {
+    const uint64_t idx = base + (uint64_t)e * 32 + lane;
+    const uint2 en = __ldcs(entry + idx);
+    const uint64_t Q = (uint64_t)en.y + 1ull;
+    if (!(n > 0 && fires_by(n, Q) > fires_by(n - 1, Q))) continue;
+    float* oth = snap + (uint64_t)en.x * dim;
+    float ds = 0.0f;
+    for (uint32_t d = 0; d < dim; ++d) { const float df = cur[d] - oth[d]; ds += df * df; }
+    float gc = 0.0f;
+    if (ds > 0.0f) {
+      const float pb = __powf(ds, b);
+      gc = __fdividef(p.neg_attr * pb, ds * (a * pb * ds + 1.0f));
+    }
+    for (uint32_t d = 0; d < dim; ++d) {
+      const float cd = cur[d], od = oth[d];
+      const float g = clip4(gc * (cd - od)) * alpha;
+      add(d, g);
+      atomicAdd(oth + d, -g);
+    }
+    const uint32_t nneg = negatives_at(n, fires_by(n, Q), Q, (uint64_t)p.neg_rate * Q);
+    uint4 rnd = make_uint4(0, 0, 0, 0);
+    for (uint32_t q = 0; q < nneg; ++q) {
+      if ((q & 3) == 0)
+        rnd = philox4x32_10(make_uint4((uint32_t)idx, (uint32_t)(idx >> 32), epoch, q >> 2), key);
+      const uint32_t rv = (q & 3) == 0 ? rnd.x : (q & 3) == 1 ? rnd.y : (q & 3) == 2 ? rnd.z : rnd.w;
+      const uint32_t kk = __umulhi(rv, p.n_vertices);
+      if (kk == r) continue;
+      const float* ob = snap + (uint64_t)kk * dim;
+      float dsn = 0.0f;
+      for (uint32_t d = 0; d < dim; ++d) { const float df = cur[d] - ob[d]; dsn += df * df; }
+      float gr = 0.0f;
+      if (dsn > 0.0f) {
+        const float pb = __powf(dsn, b);
+        gr = __fdividef(p.pos_rep, (0.001f + dsn) * (a * pb * dsn + 1.0f));
+      }
+      if (gr > 0.0f)
+        for (uint32_t d = 0; d < dim; ++d) add(d, clip4(gr * (cur[d] - ob[d])) * alpha);
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------ K5 pieces
+__global__ void kept_degree_kernel(const uint64_t* __restrict__ indptr, const float* __restrict__ data,
+                                   uint64_t n, float thr, uint32_t* __restrict__ deg) {
+  const uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  uint32_t c = 0;
+  for (uint64_t q = indptr[r]; q < indptr[r + 1]; ++q) c += data[q] >= thr ? 1u : 0u;
+  deg[r] = c;
+}
+
+__global__ void ptr_degree_kernel(const uint64_t* __restrict__ kptr, uint64_t n, uint32_t chunk,
+                                  uint32_t* __restrict__ deg, uint32_t* __restrict__ ntask) {
+  const uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  const uint32_t d = (uint32_t)(kptr[r + 1] - kptr[r]);
+  deg[r] = d;
+  ntask[r] = (d + chunk - 1) / chunk;
+}
+
+// One task per chunk of a row: row id, first kept-edge index, length, split flag.
+__global__ void task_fill_kernel(const uint64_t* __restrict__ kptr, const uint32_t* __restrict__ deg,
+                                 const uint64_t* __restrict__ tptr, uint64_t n, uint32_t chunk,
+                                 uint32_t* __restrict__ trow, uint64_t* __restrict__ tstart,
+                                 uint32_t* __restrict__ tkey) {
+  const uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  const uint32_t d = deg[r];
+  const uint64_t t0 = tptr[r], nt = tptr[r + 1] - t0;
+  for (uint64_t c = 0; c < nt; ++c) {
+    const uint32_t len = (uint32_t)min((uint64_t)chunk, (uint64_t)d - c * chunk);
+    trow[t0 + c] = (uint32_t)r | (nt > 1 ? 0x80000000u : 0u);   // high bit: partial row
+    tstart[t0 + c] = kptr[r] + c * chunk;
+    tkey[t0 + c] = chunk - len;  // ascending key = descending length
+  }
+}
+
+__global__ void slice_meta_kernel(const uint32_t* __restrict__ perm, const uint32_t* __restrict__ trow,
+                                  const uint32_t* __restrict__ skey, uint64_t T, uint64_t n_slices,
+                                  uint32_t chunk, uint32_t* __restrict__ width, uint32_t* __restrict__ rowid,
+                                  uint32_t* __restrict__ split_mask) {
+  const uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n_slices * 32) return;
+  const uint32_t tr = q < T ? trow[perm[q]] : PAD_ROW;
+  rowid[q] = tr == PAD_ROW ? PAD_ROW : (tr & 0x7FFFFFFFu);
+  const unsigned bits = __ballot_sync(0xFFFFFFFFu, tr != PAD_ROW && (tr & 0x80000000u));
+  if ((q & 31) == 0) {
+    width[q >> 5] = q < T ? chunk - skey[q] : 0u;
+    split_mask[q >> 5] = bits;
+  }
+}
+
+__global__ void slice_fill_kernel(const uint32_t* __restrict__ ktail, const double* __restrict__ keps,
+                                  const uint32_t* __restrict__ perm, const uint64_t* __restrict__ tstart,
+                                  const uint32_t* __restrict__ skey, uint64_t T, uint32_t chunk,
+                                  const uint64_t* __restrict__ wscan, const uint32_t* __restrict__ width,
+                                  uint64_t n_slices, uint2* __restrict__ entry) {
+  const uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n_slices * 32) return;
+  const uint64_t s = q >> 5;
+  const uint32_t lane = (uint32_t)(q & 31);
+  const uint64_t base = wscan[s] * 32;
+  const uint32_t wd = width[s];
+  uint32_t e = 0;
+  if (q < T) {
+    const uint64_t st = tstart[perm[q]];
+    const uint32_t len = chunk - skey[q];
+    for (; e < len; ++e)
+      entry[base + (uint64_t)e * 32 + lane] = make_uint2(ktail[st + e], q_minus_1(keps[st + e]));
+  }
+  for (; e < wd; ++e) entry[base + (uint64_t)e * 32 + lane] = make_uint2(0u, 0u);
+}
+
+__global__ void head_from_ptr_kernel(const uint64_t* __restrict__ kptr, uint64_t n, uint32_t* __restrict__ head) {
+  const uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  for (uint64_t j = kptr[r]; j < kptr[r + 1]; ++j) head[j] = (uint32_t)r;
+}
+
+// Schedule state of the reference at `cur` (optimizer.rs:41-43) from the closed form:
+// m = firings so far, T = negatives drawn so far;  eons = (m+1)*eps, epns = eps/neg,
+// eonns = epns*(1+T).
+__global__ void export_state_kernel(const double* __restrict__ eps, uint64_t E, uint64_t neg,
+                                    uint64_t cur, double* __restrict__ eons, double* __restrict__ eonns,
+                                    double* __restrict__ epns) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= E) return;
+  const double e = eps[i];
+  const uint64_t Q = (uint64_t)q_minus_1(e) + 1ull;
+  const uint64_t m = cur > 0 ? fires_by(cur - 1, Q) : 0ull;
+  const uint64_t t = negatives_after(m, Q, neg * Q);
+  const double pn = e / (double)neg;
+  if (eons) eons[i] = e * ((double)m + 1.0);
+  if (epns) epns[i] = pn;
+  if (eonns) eonns[i] = pn * (1.0 + (double)t);
+}
+
+// make_epochs_per_sample.rs:30-49 in f64.
+__device__ __forceinline__ double epochs_per_sample(float w, double max_w, double n_ep) {
+  const double n_samples = n_ep * ((double)w / max_w);
+  return n_samples > 0.0 ? n_ep / n_samples : -1.0;
+}
+
+__global__ void export_edges_kernel(const uint64_t* __restrict__ indptr, const uint32_t* __restrict__ indices,
+                                    const float* __restrict__ data, uint64_t n, float thr, double max_w,
+                                    double n_ep, const uint64_t* __restrict__ kept_ptr,
+                                    uint32_t* __restrict__ head, uint32_t* __restrict__ tail,
+                                    double* __restrict__ eps) {
+  const uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  uint64_t o = kept_ptr[r];
+  for (uint64_t j = indptr[r]; j < indptr[r + 1]; ++j) {
+    const float w = data[j];
+    if (w >= thr) {
+      if (head) head[o] = (uint32_t)r;
+      if (tail) tail[o] = indices[j];
+      if (eps) eps[o] = epochs_per_sample(w, max_w, n_ep);
+      ++o;
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------ K6
+// optimizer.rs:189-230.  f32::min / f32::max ignore NaN like fminf / fmaxf.
+__global__ void minmax_dim_kernel(const float* __restrict__ emb, uint64_t n, uint32_t dim,
+                                  float* __restrict__ mins, float* __restrict__ maxs) {
+  // one block per dimension
+  const uint32_t d = blockIdx.x;
+  float mn = INFINITY, mx = -INFINITY;
+  for (uint64_t i = threadIdx.x; i < n; i += blockDim.x) {
+    const float v = emb[i * dim + d];
+    mn = fminf(mn, v);
+    mx = fmaxf(mx, v);
+  }
+  __shared__ float s_mn[32], s_mx[32];
+  for (int o = 16; o > 0; o >>= 1) {
+    mn = fminf(mn, __shfl_xor_sync(0xFFFFFFFFu, mn, o));
+    mx = fmaxf(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, o));
+  }
+  if ((threadIdx.x & 31) == 0) { s_mn[threadIdx.x >> 5] = mn; s_mx[threadIdx.x >> 5] = mx; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (uint32_t w = 1; w < blockDim.x / 32; ++w) { mn = fminf(mn, s_mn[w]); mx = fmaxf(mx, s_mx[w]); }
+    const float range = __fsub_rn(mx, mn);
+    mins[d] = mn;
+    maxs[d] = range > 0.0f ? __fdiv_rn(10.0f, range) : 0.0f;  // scale
+  }
+}
+
+__global__ void normalize_kernel(float* __restrict__ emb, uint64_t total, uint32_t dim,
+                                 const float* __restrict__ mins, const float* __restrict__ scales) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= total) return;
+  const uint32_t d = (uint32_t)(i % dim);
+  const float sc = scales[d];
+  if (sc > 0.0f) emb[i] = __fmul_rn(__fsub_rn(emb[i], mins[d]), sc);
+}
+
+// ------------------------------------------------------------------------------ accounting
+__global__ void schedule_totals_kernel(const uint2* __restrict__ entry, uint64_t n_entries, uint64_t neg,
+                                       uint64_t start, uint64_t end, unsigned long long* __restrict__ fired,
+                                       unsigned long long* __restrict__ negs) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long f = 0, g = 0;
+  if (i < n_entries) {
+    const uint64_t Q = (uint64_t)entry[i].y + 1ull;
+    // firings in [start, end) = m(end-1) - m(start-1); negatives telescope the same way.
+    const uint64_t fe = end > 0 ? fires_by(end - 1, Q) : 0ull;
+    const uint64_t fs = start > 0 ? fires_by(start - 1, Q) : 0ull;
+    f = fe - fs;
+    g = negatives_after(fe, Q, neg * Q) - negatives_after(fs, Q, neg * Q);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    f += __shfl_xor_sync(0xFFFFFFFFu, f, o);
+    g += __shfl_xor_sync(0xFFFFFFFFu, g, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (f) atomicAdd(fired, f);
+    if (g) atomicAdd(negs, g);
+  }
+}
+
+__global__ void nan_rows_kernel(const uint64_t* __restrict__ indptr, uint64_t n, uint32_t dim,
+                                float* __restrict__ emb) {
+  const uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n || indptr[r + 1] != indptr[r]) return;
+  for (uint32_t d = 0; d < dim; ++d) emb[r * dim + d] = __int_as_float(0x7FC00000);
+}
+
+__global__ void scale32_kernel(uint64_t* __restrict__ x, uint64_t n) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) x[i] *= 32;
+}
+
+inline unsigned grid_for(uint64_t n, unsigned bt) { return (unsigned)((n + bt - 1) / bt); }
+
+}  // namespace
+
+void kept_degree(const uint64_t* indptr, const float* data, uint64_t n, float thr, uint32_t* deg,
+                 cudaStream_t s) {
+  if (n == 0) return;
+  kept_degree_kernel<<<grid_for(n, 256), 256, 0, s>>>(indptr, data, n, thr, deg);
+  UB_LAUNCH_CHECK();
+}
+
+void prune_edges(const uint64_t* indptr, const float* data, uint64_t n, float thr, uint64_t* kept_ptr,
+                 uint64_t* n_edges, cudaStream_t s) {
+  DevBuf<uint32_t> deg(n, s);
+  kept_degree(indptr, data, n, thr, deg.p, s);
+  scan_u32_to_u64(deg.p, kept_ptr, n, s);
+  UB_CUDA(cudaMemcpyAsync(n_edges, kept_ptr + n, 8, cudaMemcpyDeviceToHost, s));
+  UB_CUDA(cudaStreamSynchronize(s));
+}
+
+void head_from_ptr(const uint64_t* kept_ptr, uint64_t n, uint32_t* head, cudaStream_t s) {
+  if (n == 0) return;
+  head_from_ptr_kernel<<<grid_for(n, 256), 256, 0, s>>>(kept_ptr, n, head);
+  UB_LAUNCH_CHECK();
+}
+
+void export_state(const double* eps, uint64_t E, uint64_t neg_rate, uint64_t cur_epoch, double* eons,
+                  double* eonns, double* epns, cudaStream_t s) {
+  if (E == 0) return;
+  export_state_kernel<<<grid_for(E, 256), 256, 0, s>>>(eps, E, neg_rate, cur_epoch, eons, eonns, epns);
+  UB_LAUNCH_CHECK();
+}
+
+// Longest task (edges) so that no single lane's chain of updates outlasts roughly half an
+// epoch: an epoch streams E edges across the whole GPU, while one lane works through its
+// task sequentially, so the bound grows linearly with E (~E/135k for this kernel).
+uint32_t pick_chunk(uint64_t n_edges) {
+  if (const char* e = getenv("UMAP_B200_CHUNK")) {
+    long v = atol(e);
+    if (v >= 1 && v <= (1 << 30)) return (uint32_t)v;
+  }
+  uint64_t c = (n_edges / 135000 + 7) / 8 * 8;
+  return (uint32_t)std::min<uint64_t>(512, std::max<uint64_t>(32, c));
+}
+
+void build_sgd_layout(const uint64_t* kept_ptr, const uint32_t* ktail, const double* keps, uint64_t n,
+                      uint32_t chunk, SgdLayout& L, cudaStream_t s) {
+  L.n_vertices = n;
+  uint64_t n_edges = 0;
+  UB_CUDA(cudaMemcpyAsync(&n_edges, kept_ptr + n, 8, cudaMemcpyDeviceToHost, s));
+  UB_CUDA(cudaStreamSynchronize(s));
+  L.n_edges = n_edges;
+  L.chunk = chunk ? chunk : pick_chunk(n_edges);
+  DevBuf<uint32_t> deg(n, s), ntask(n, s);
+  if (n) {
+    ptr_degree_kernel<<<grid_for(n, 256), 256, 0, s>>>(kept_ptr, n, L.chunk, deg.p, ntask.p);
+    UB_LAUNCH_CHECK();
+  }
+  DevBuf<uint32_t> dmax(1, s);
+  reduce_max_u32(deg.p, n, dmax.p, s);
+  DevBuf<uint64_t> tptr(n + 1, s);
+  scan_u32_to_u64(ntask.p, tptr.p, n, s);
+  uint64_t T = 0;
+  UB_CUDA(cudaMemcpyAsync(&T, tptr.p + n, 8, cudaMemcpyDeviceToHost, s));
+  UB_CUDA(cudaMemcpyAsync(&L.max_degree, dmax.p, 4, cudaMemcpyDeviceToHost, s));
+  UB_CUDA(cudaStreamSynchronize(s));
+  if (T >= 0xFFFFFFFFull) throw Error(UNSUPPORTED, "too many SGD tasks (>= 2^32)");
+  L.n_tasks = T;
+  DevBuf<uint32_t> trow(T, s), tkey(T, s), skey(T, s), perm(T, s);
+  DevBuf<uint64_t> tstart(T, s);
+  if (n) {
+    task_fill_kernel<<<grid_for(n, 256), 256, 0, s>>>(kept_ptr, deg.p, tptr.p, n, L.chunk, trow.p, tstart.p,
+                                                      tkey.p);
+    UB_LAUNCH_CHECK();
+  }
+  if (T) radix_sort_pairs(tkey.p, nullptr, skey.p, perm.p, T, bits_for(L.chunk), s);
+  L.n_slices = (T + 31) / 32;
+  L.slice_width.alloc(L.n_slices, s);
+  L.split_mask.alloc(L.n_slices, s);
+  L.rowid.alloc(L.n_slices * 32, s);
+  L.slice_base.alloc(L.n_slices + 1, s);
+  if (L.n_slices) {
+    slice_meta_kernel<<<grid_for(L.n_slices * 32, 256), 256, 0, s>>>(perm.p, trow.p, skey.p, T, L.n_slices,
+                                                                        L.chunk, L.slice_width.p, L.rowid.p,
+                                                                        L.split_mask.p);
+    UB_LAUNCH_CHECK();
+  }
+  DevBuf<uint64_t> wscan(L.n_slices + 1, s);
+  scan_u32_to_u64(L.slice_width.p, wscan.p, L.n_slices, s);
+  uint64_t wtot = 0;
+  UB_CUDA(cudaMemcpyAsync(&wtot, wscan.p + L.n_slices, 8, cudaMemcpyDeviceToHost, s));
+  UB_CUDA(cudaStreamSynchronize(s));
+  L.n_entries = wtot * 32;
+  L.entry.alloc(L.n_entries, s);
+  if (L.n_slices) {
+    slice_fill_kernel<<<grid_for(L.n_slices * 32, 256), 256, 0, s>>>(ktail, keps, perm.p, tstart.p, skey.p, T,
+                                                                        L.chunk, wscan.p, L.slice_width.p,
+                                                                        L.n_slices, L.entry.p);
+    UB_LAUNCH_CHECK();
+  }
+  // slice_base = 32 * wscan (entries, not widths)
+  scale32_kernel<<<grid_for(L.n_slices + 1, 256), 256, 0, s>>>(wscan.p, L.n_slices + 1);
+  UB_LAUNCH_CHECK();
+  UB_CUDA(cudaMemcpyAsync(L.slice_base.p, wscan.p, (L.n_slices + 1) * 8, cudaMemcpyDeviceToDevice, s));
+  // count partial-row tasks (diagnostics)
+  std::vector<uint32_t> h(L.n_slices);
+  if (L.n_slices) UB_CUDA(cudaMemcpyAsync(h.data(), L.split_mask.p, L.n_slices * 4, cudaMemcpyDeviceToHost, s));
+  UB_CUDA(cudaStreamSynchronize(s));
+  L.split_tasks = 0;
+  for (uint32_t v : h) L.split_tasks += __builtin_popcount(v);
+}
+
+void export_edges(const uint64_t* indptr, const uint32_t* indices, const float* data, uint64_t n,
+                  float thr, float max_w, uint64_t total_epochs, const uint64_t* kept_ptr,
+                  uint32_t* head, uint32_t* tail, double* eps, cudaStream_t s) {
+  if (n == 0) return;
+  export_edges_kernel<<<grid_for(n, 256), 256, 0, s>>>(indptr, indices, data, n, thr, (double)max_w,
+                                                       (double)total_epochs, kept_ptr, head, tail, eps);
+  UB_LAUNCH_CHECK();
+}
+
+void normalize_init(float* emb, uint64_t n, uint32_t dim, cudaStream_t s) {
+  if (n == 0 || dim == 0) return;
+  DevBuf<float> mins(dim, s), scales(dim, s);
+  minmax_dim_kernel<<<dim, 1024, 0, s>>>(emb, n, dim, mins.p, scales.p);
+  UB_LAUNCH_CHECK();
+  normalize_kernel<<<grid_for(n * dim, 256), 256, 0, s>>>(emb, n * dim, dim, mins.p, scales.p);
+  UB_LAUNCH_CHECK();
+}
+
+void sgd_epoch(const SgdLayout& L, float* live, float* snap, const SgdParams& p, uint32_t epoch, float alpha,
+               cudaStream_t s) {
+  if (L.n_slices == 0) return;
+  const unsigned grid = grid_for(L.n_slices * 32, 256);
+#define UB_SGD_ARGS L.slice_base.p, L.slice_width.p, L.split_mask.p, L.rowid.p, L.entry.p, L.n_slices, live, snap, \
+                    p, epoch, alpha
+  switch (p.dim) {
+    case 1: sgd_epoch_kernel<1><<<grid, 256, 0, s>>>(UB_SGD_ARGS); break;
+    case 2: sgd_epoch_kernel<2><<<grid, 256, 0, s>>>(UB_SGD_ARGS); break;
+    case 3: sgd_epoch_kernel<3><<<grid, 256, 0, s>>>(UB_SGD_ARGS); break;
+    case 4: sgd_epoch_kernel<4><<<grid, 256, 0, s>>>(UB_SGD_ARGS); break;
+    default: sgd_epoch_generic<<<grid, 256, 0, s>>>(UB_SGD_ARGS); break;
+  }
+#undef UB_SGD_ARGS
+  UB_LAUNCH_CHECK();
+}
+
+void schedule_totals(const SgdLayout& L, uint32_t neg_rate, uint32_t start, uint32_t end,
+                     unsigned long long* d_fired, unsigned long long* d_negs, cudaStream_t s) {
+  UB_CUDA(cudaMemsetAsync(d_fired, 0, 8, s));
+  UB_CUDA(cudaMemsetAsync(d_negs, 0, 8, s));
+  if (L.n_entries == 0 || end <= start) return;
+  schedule_totals_kernel<<<grid_for(L.n_entries, 256), 256, 0, s>>>(L.entry.p, L.n_entries, neg_rate, start, end,
+                                                                   d_fired, d_negs);
+  UB_LAUNCH_CHECK();
+}
+
+void nan_empty_rows(const uint64_t* indptr, uint64_t n, uint32_t dim, float* emb, cudaStream_t s) {
+  if (n == 0) return;
+  nan_rows_kernel<<<grid_for(n, 256), 256, 0, s>>>(indptr, n, dim, emb);
+  UB_LAUNCH_CHECK();
+}
+
+}  // namespace ub

@@ -1,0 +1,208 @@
+// Internal declarations shared by the CUDA kernels (*.cu) and the C++ host (*.cpp).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <utility>
+
+namespace ub {
+
+// C-ABI status codes (mirrors include/umap_b200.h).
+enum Status : int {
+  OK = 0,
+  INVALID_ARGUMENT = 1,
+  OVERSTEP = 2,
+  CUDA = 3,
+  OUT_OF_MEMORY = 4,
+  FORMAT = 5,
+  IO = 6,
+  NULLPTR = 7,
+  UNSUPPORTED = 8,
+};
+
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+[[noreturn]] void throw_cuda(cudaError_t e, const char* what, const char* file, int line);
+inline void cuda_check(cudaError_t e, const char* what, const char* file, int line) {
+  if (e != cudaSuccess) throw_cuda(e, what, file, line);
+}
+#define UB_CUDA(x) ::ub::cuda_check((x), #x, __FILE__, __LINE__)
+// Every kernel launch site calls this right after its launch: it counts the launch (for
+// throughput accounting) and surfaces launch errors.
+void count_launch();
+#define UB_LAUNCH_CHECK() \
+  (::ub::count_launch(), ::ub::cuda_check(cudaGetLastError(), "kernel launch", __FILE__, __LINE__))
+
+// Stream-ordered device buffer (cudaMallocAsync / cudaFreeAsync on the owner stream).
+template <class T>
+struct DevBuf {
+  T* p = nullptr;
+  uint64_t n = 0;
+  cudaStream_t s = nullptr;
+
+  DevBuf() = default;
+  DevBuf(uint64_t count, cudaStream_t st) { alloc(count, st); }
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n), s(o.s) { o.p = nullptr; o.n = 0; }
+  DevBuf& operator=(DevBuf&& o) noexcept {
+    if (this != &o) {
+      reset();
+      p = o.p; n = o.n; s = o.s;
+      o.p = nullptr; o.n = 0;
+    }
+    return *this;
+  }
+  ~DevBuf() { reset(); }
+
+  void alloc(uint64_t count, cudaStream_t st) {
+    reset();
+    s = st;
+    n = count;
+    if (count == 0) return;
+    cudaError_t e = cudaMallocAsync((void**)&p, count * sizeof(T), st);
+    if (e == cudaErrorMemoryAllocation) {
+      (void)cudaGetLastError();
+      p = nullptr;
+      n = 0;
+      throw Error(OUT_OF_MEMORY, "device allocation of " + std::to_string(count * sizeof(T)) +
+                                     " bytes failed");
+    }
+    cuda_check(e, "cudaMallocAsync", __FILE__, __LINE__);
+  }
+  void reset() noexcept {
+    if (p) (void)cudaFreeAsync(p, s);
+    p = nullptr;
+    n = 0;
+  }
+  // Moves ownership to another stream's ordering (caller guarantees ordering).
+  void set_stream(cudaStream_t st) { s = st; }
+  uint64_t bytes() const { return n * sizeof(T); }
+  T* get() const { return p; }
+};
+
+// ---------------------------------------------------------------- primitives (prim.cu)
+// out[0..n] = exclusive prefix sum of in[0..n-1]; out[n] = total.
+void scan_u32_to_u64(const uint32_t* in, uint64_t* out, uint64_t n, cudaStream_t s);
+void scan_u64_to_u64(const uint64_t* in, uint64_t* out, uint64_t n, cudaStream_t s);
+// Stable LSD radix sort by key bits [0, end_bit).  vals_in == nullptr means 0..n-1.
+// keys_out/vals_out may not alias the inputs.  n must be < 2^32.
+void radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
+                      uint32_t* vals_out, uint64_t n, int end_bit, cudaStream_t s);
+// Reductions into a device scalar (*out).
+void reduce_max_f32(const float* x, uint64_t n, float init, float* out, cudaStream_t s);
+void reduce_max_u32(const uint32_t* x, uint64_t n, uint32_t* out, cudaStream_t s);
+void reduce_sum_u64(const uint64_t* x, uint64_t n, uint64_t* out, cudaStream_t s);
+int bits_for(uint64_t max_value);
+
+// ---------------------------------------------------------------- graph build (graph.cu)
+struct GraphParams {
+  float local_connectivity;
+  float interpolation;  // local_connectivity - floor(local_connectivity)
+  uint64_t lc_usize;    // `local_connectivity as usize` (saturating)
+  uint64_t lc_index;    // `local_connectivity.floor() as usize`
+  float target;         // log2f(k) * bandwidth, computed on the host with glibc log2f
+  float disc_thr;       // disconnection distance (+inf by default)
+  float mix;            // set_op_mix_ratio
+  float prod_coeff;     // 1 - 2*mix (f32, host-rounded)
+  int n_iter;           // 64
+};
+
+// K1: per-row rho and sigma (smooth_knn_dist.rs:60-198).  Uses a device scratch flag and
+// global-mean fixup for rows whose rho is not positive.
+void smooth_knn(const float* dist, uint64_t n, uint64_t k, const GraphParams& gp,
+                float* sigmas, float* rhos, cudaStream_t s);
+// K2: directed membership entries per row, kept ones sorted by column (stable) into the
+// padded [n][k] arrays pcol/pw; cnt[r] = kept count.  edges_removed (device u64) counts
+// dist >= disc_thr entries.
+void membership(const uint32_t* idx, const float* dist, uint64_t n, uint64_t k,
+                const GraphParams& gp, const float* sigmas, const float* rhos, uint32_t* pcol,
+                float* pw, uint32_t* cnt, unsigned long long* edges_removed, cudaStream_t s);
+// Compacts padded rows into CSR order: keys[q] = column, vals[q] = padded position r*k+e.
+void compact_directed(const uint32_t* pcol, const uint32_t* cnt, const uint64_t* dptr,
+                      uint64_t n, uint64_t k, uint32_t* keys, uint32_t* vals, cudaStream_t s);
+// data[q] = pw[vals[q]].
+void gather_weights(const float* pw, const uint32_t* vals, uint64_t nnz, float* data,
+                    cudaStream_t s);
+// tptr[c] = first index i with sorted_keys[i] >= c, for c in [0, n]; tptr[n] = nnz.
+void segment_starts(const uint32_t* sorted_keys, uint64_t nnz, uint64_t n, uint64_t* tptr,
+                    cudaStream_t s);
+// K4 fuzzy union, count pass (fill=false) and fill pass.
+void union_rows(const uint32_t* pcol, const float* pw, const uint32_t* cnt, uint64_t k,
+                const uint64_t* tptr, const uint32_t* tvals, uint64_t n, const GraphParams& gp,
+                uint32_t* out_cnt, const uint64_t* out_ptr, uint32_t* out_idx, float* out_w,
+                bool fill, cudaStream_t s);
+// Rows whose weights sum to zero (embedding.rs:216-223); returns count into *out.
+void count_empty_rows(const uint64_t* indptr, const float* data, uint64_t n,
+                      unsigned long long* out, cudaStream_t s);
+
+// ---------------------------------------------------------------- SGD layout (sgd.cu)
+// Schedule value per kept edge: Q = ceil(2^32 / epochs_per_sample), stored as Q - 1 in a
+// u32 (Q in [1, 2^32]).  Fires by epoch n: (n * Q) >> 32.  Q - 1 == 0 never fires in
+// any realistic run (padding).
+//
+// Tasks: each head row's kept edges are cut into chunks of at most `chunk` edges; a task is
+// one chunk.  Tasks are sorted by length (descending, stable) and packed 32 to a slice; a
+// warp owns a slice, a lane owns a task.  Entry (e, lane) of slice s lives at
+// slice_base[s] + e*32 + lane as uint2 {tail, Q - 1}.  Bit `lane` of split_mask[s] is set
+// when the lane's task is a partial row (its head update is merged with an atomic add).
+struct SgdLayout {
+  uint64_t n_vertices = 0, n_edges = 0, n_entries = 0, n_slices = 0, n_tasks = 0;
+  uint32_t max_degree = 0, chunk = 0;
+  uint64_t split_tasks = 0;
+  DevBuf<uint64_t> slice_base;   // [n_slices + 1]
+  DevBuf<uint32_t> slice_width;  // [n_slices]
+  DevBuf<uint32_t> split_mask;   // [n_slices]
+  DevBuf<uint32_t> rowid;        // [n_slices * 32]; 0xFFFFFFFF = padding lane
+  DevBuf<uint2> entry;           // [n_entries] {tail, Q - 1}
+};
+
+struct SgdParams {
+  float a, b, gamma;
+  float neg_attr;   // (-2 a) b
+  float pos_rep;    // (2 gamma) b
+  uint32_t neg_rate;  // negative_sample_rate
+  uint32_t n_vertices;
+  uint32_t dim;
+  uint64_t seed;
+};
+
+// Prune (optimizer.rs:85-167): keep w >= thr.  kept_ptr[n+1] = row pointers of the kept
+// edges in the reference's row-major order; *n_edges = kept count (host, synchronises).
+void prune_edges(const uint64_t* indptr, const float* data, uint64_t n, float thr,
+                 uint64_t* kept_ptr, uint64_t* n_edges, cudaStream_t s);
+// Kept edges in the reference order: head/tail u32 and epochs_per_sample f64
+// (make_epochs_per_sample.rs:21-52 with max weight max_w).  Any output may be null.
+void export_edges(const uint64_t* indptr, const uint32_t* indices, const float* data,
+                  uint64_t n, float thr, float max_w, uint64_t total_epochs,
+                  const uint64_t* kept_ptr, uint32_t* head, uint32_t* tail, double* eps,
+                  cudaStream_t s);
+void head_from_ptr(const uint64_t* kept_ptr, uint64_t n, uint32_t* head, cudaStream_t s);
+// Schedule state at cur_epoch in the reference's representation (optimizer.rs:41-43).
+void export_state(const double* eps, uint64_t E, uint64_t neg_rate, uint64_t cur_epoch,
+                  double* eons, double* eonns, double* epns, cudaStream_t s);
+// Slice layout from kept edges (kept_ptr, tail, eps).  chunk = 0 picks the task length
+// from the edge count.
+void build_sgd_layout(const uint64_t* kept_ptr, const uint32_t* tail, const double* eps,
+                      uint64_t n, uint32_t chunk, SgdLayout& L, cudaStream_t s);
+void kept_degree(const uint64_t* indptr, const float* data, uint64_t n, float thr,
+                 uint32_t* deg, cudaStream_t s);
+// K6 normalise init into [0, 10] per dimension (optimizer.rs:181-230), in place.
+void normalize_init(float* emb, uint64_t n, uint32_t dim, cudaStream_t s);
+// K7 one Hogwild epoch.
+void sgd_epoch(const SgdLayout& L, float* live, float* snap, const SgdParams& p,
+               uint32_t epoch, float alpha, cudaStream_t s);
+// Exact totals of fired edges / negatives over epochs [start, end).
+void schedule_totals(const SgdLayout& L, uint32_t neg_rate, uint32_t start, uint32_t end,
+                     unsigned long long* d_fired, unsigned long long* d_negs, cudaStream_t s);
+// Rows with an empty graph row -> NaN (embedding.rs:327-334).
+void nan_empty_rows(const uint64_t* indptr, uint64_t n, uint32_t dim, float* emb,
+                    cudaStream_t s);
+
+}  // namespace ub

@@ -1,0 +1,266 @@
+"""Seeded synthetic workloads for the UMAP fit path, and an exact kNN producer.
+
+No public dataset is used.  Each generator reproduces the shapes, sizes and value
+distributions of one benchmark configuration of the fit path:
+
+* ``gaussians_10k``   n=10,000, D=32, 10 isotropic Gaussians (centres ~N(0, 5^2 I), std 1,
+  equal weights), seed 0; 200 epochs.
+* ``gaussians_2m``    n=2,000,000, D=64, 50 anisotropic Gaussians (centres ~N(0, 8^2 I),
+  per-cluster diagonal std ~U[0.5, 2], Dirichlet(1) weights), seed 1; 500 epochs.
+* ``swiss_roll``      3-D noisy swiss roll (t~U[1.5pi, 4.5pi], height~U[0, 20], noise std
+  0.05), seed 2.
+* ``instances``       many independent datasets, sizes log-uniform in [500, 50,000], D=32,
+  5 Gaussians each (centres ~N(0, 5^2 I), std 1), per-instance seed.
+
+Every workload's kNN is exact (self first at distance 0): candidates come from a
+||x||^2 + ||y||^2 - 2 x.y distance matrix, then the final k distances are recomputed
+directly in f32 as sqrt(sum((x - y)^2)) and sorted by (distance, index).  A per-row
+certificate checks that no point outside the candidate list can beat the k-th
+neighbour; rows that fail it are redone by direct brute force.
+
+Init is uniform in [-10, 10]^dim (f32), like the reference's random-init examples.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+
+def _rng(seed: int) -> np.random.Generator:
+    return np.random.Generator(np.random.PCG64(seed))
+
+
+def gaussian_mixture(n: int, d: int, n_clusters: int, centre_std: float, seed: int,
+                     anisotropic: bool = False, dirichlet: bool = False):
+    """Returns (X f32[n, d], labels i32[n])."""
+    g = _rng(seed)
+    centres = g.normal(0.0, centre_std, size=(n_clusters, d))
+    if anisotropic:
+        stds = g.uniform(0.5, 2.0, size=(n_clusters, d))
+    else:
+        stds = np.ones((n_clusters, d))
+    if dirichlet:
+        w = g.dirichlet(np.ones(n_clusters))
+    else:
+        w = np.full(n_clusters, 1.0 / n_clusters)
+    labels = g.choice(n_clusters, size=n, p=w).astype(np.int32)
+    X = np.empty((n, d), np.float32)
+    chunk = 1 << 20
+    for s in range(0, n, chunk):
+        e = min(n, s + chunk)
+        lab = labels[s:e]
+        X[s:e] = (centres[lab] + g.standard_normal((e - s, d)) * stds[lab]).astype(np.float32)
+    return X, labels
+
+
+def gaussians_10k():
+    return gaussian_mixture(10_000, 32, 10, 5.0, seed=0)
+
+
+def gaussians_2m(n: int = 2_000_000):
+    return gaussian_mixture(n, 64, 50, 8.0, seed=1, anisotropic=True, dirichlet=True)
+
+
+def swiss_roll(n: int, seed: int = 2):
+    g = _rng(seed)
+    t = g.uniform(1.5 * math.pi, 4.5 * math.pi, size=n)
+    h = g.uniform(0.0, 20.0, size=n)
+    X = np.stack([t * np.cos(t), h, t * np.sin(t)], axis=1)
+    X += g.normal(0.0, 0.05, size=X.shape)
+    return X.astype(np.float32), t.astype(np.float32)
+
+
+def instance_sizes(count: int = 4096, lo: int = 500, hi: int = 50_000, seed: int = 4):
+    g = _rng(seed)
+    return np.exp(g.uniform(math.log(lo), math.log(hi), size=count)).astype(np.int64)
+
+
+def instance(i: int, n: int, seed_base: int = 1000):
+    return gaussian_mixture(int(n), 32, 5, 5.0, seed=seed_base + i)
+
+
+def uniform_init(n: int, dim: int = 2, seed: int = 0) -> np.ndarray:
+    g = _rng(10_000 + seed)
+    return g.uniform(-10.0, 10.0, size=(n, dim)).astype(np.float32)
+
+
+# ------------------------------------------------------------------ exact kNN
+def _finalize_rows(X, rows, cand, k):
+    """Exact f32 distances for candidate lists, sorted by (distance, index), k kept."""
+    xi = X[rows][:, None, :]
+    xc = X[cand]
+    d = np.sqrt(((xi - xc) ** 2).sum(axis=2, dtype=np.float32)).astype(np.float32)
+    o1 = np.argsort(cand, axis=1, kind="stable")
+    cand = np.take_along_axis(cand, o1, 1)
+    d = np.take_along_axis(d, o1, 1)
+    o2 = np.argsort(d, axis=1, kind="stable")
+    cand = np.take_along_axis(cand, o2, 1)
+    d = np.take_along_axis(d, o2, 1)
+    return cand[:, :k], d[:, :k]
+
+
+def knn_exact_numpy(X: np.ndarray, k: int, margin: int = 8, chunk: int = 1024):
+    """Exact kNN on the CPU (f64 distance matrix for candidates)."""
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    n = X.shape[0]
+    X64 = X.astype(np.float64)
+    sq = (X64 * X64).sum(1)
+    kc = min(n, k + margin)
+    idx = np.empty((n, k), np.uint32)
+    dst = np.empty((n, k), np.float32)
+    for s in range(0, n, chunk):
+        e = min(n, s + chunk)
+        D = sq[s:e, None] + sq[None, :] - 2.0 * (X64[s:e] @ X64.T)
+        D[np.arange(e - s), np.arange(s, e)] = -1.0  # self first
+        cand = np.argpartition(D, kc - 1, axis=1)[:, :kc]
+        ci, cd = _finalize_rows(X, np.arange(s, e), cand, k)
+        idx[s:e] = ci
+        dst[s:e] = cd
+    return idx, dst
+
+
+def knn_exact_torch(X: np.ndarray, k: int, device="cuda", margin: int = 8, chunk: int = 2048):
+    """Exact kNN with torch on the GPU (harness-side producer, not part of the fit path).
+
+    Candidates: top-(k+margin) of the fp32 (TF32 off) expansion distance.  Exactness
+    certificate per row: the (k+margin)-th candidate's approximate squared distance minus
+    an fp32 rounding bound must exceed the exact k-th squared distance; failing rows are
+    recomputed by direct brute force."""
+    import torch
+
+    torch.backends.cuda.matmul.allow_tf32 = False
+    X0 = torch.from_numpy(np.ascontiguousarray(X, dtype=np.float32)).to(device)
+    Xt = X0 - X0.mean(0, keepdim=True)   # centred copy: candidate search only
+    n, dim = Xt.shape
+    sq = (Xt * Xt).sum(1)
+    kc = min(n, k + margin)
+    idx = torch.empty((n, k), dtype=torch.int64, device=device)
+    dst = torch.empty((n, k), dtype=torch.float32, device=device)
+    bad_rows = []
+    eps = 4.0 * dim * 2.0 ** -23
+    for s in range(0, n, chunk):
+        e = min(n, s + chunk)
+        D = sq[s:e, None] + sq[None, :] - 2.0 * (Xt[s:e] @ Xt.T)
+        ar = torch.arange(e - s, device=device)
+        D[ar, ar + s] = -1.0
+        vals, cand = torch.topk(D, kc, dim=1, largest=False, sorted=True)
+        xc = X0[cand]                                   # [m, kc, dim]
+        ex = torch.sqrt(((X0[s:e, None, :] - xc) ** 2).sum(2))
+        # sort by (distance, index): stable sort on index first, then distance
+        o1 = torch.argsort(cand, dim=1, stable=True)
+        cand = torch.gather(cand, 1, o1)
+        ex = torch.gather(ex, 1, o1)
+        o2 = torch.argsort(ex, dim=1, stable=True)
+        cand = torch.gather(cand, 1, o2)
+        ex = torch.gather(ex, 1, o2)
+        idx[s:e] = cand[:, :k]
+        dst[s:e] = ex[:, :k]
+        if kc < n:
+            bound = eps * (sq[s:e] + sq[cand[:, kc - 1]] + 1.0)
+            kth = ex[:, k - 1] ** 2
+            bad = (vals[:, kc - 1] - bound) <= kth * (1.0 + 1e-6)
+            if bool(bad.any()):
+                bad_rows.extend((torch.nonzero(bad).flatten() + s).tolist())
+    for r in bad_rows:
+        d = torch.sqrt(((X0 - X0[r]) ** 2).sum(1))
+        d[r] = -1.0
+        v, c = torch.topk(d, kc, largest=False, sorted=True)
+        o1 = torch.argsort(c, stable=True)
+        c, v = c[o1], v[o1]
+        o2 = torch.argsort(v, stable=True)
+        c, v = c[o2], v[o2]
+        v[c == r] = 0.0
+        idx[r] = c[:k]
+        dst[r] = v[:k]
+    return idx.to(torch.int32).cpu().numpy().astype(np.uint32), dst.cpu().numpy(), len(bad_rows)
+
+
+def _torch_knn_block(torch, Xq0, Xq, Xc0, Xc, sqq, sqc, k, kc, self_offset):
+    """Top-(k) exact neighbours of query rows among candidate rows (both on the GPU).
+    X*0 are the original coordinates (exact distances), X* the centred copies (search)."""
+    D = sqq[:, None] + sqc[None, :] - 2.0 * (Xq @ Xc.T)
+    if self_offset is not None:
+        ar = torch.arange(Xq.shape[0], device=Xq.device)
+        D[ar, ar + self_offset] = -1.0
+    vals, cand = torch.topk(D, kc, dim=1, largest=False, sorted=True)
+    ex = torch.sqrt(((Xq0[:, None, :] - Xc0[cand]) ** 2).sum(2))
+    o1 = torch.argsort(cand, dim=1, stable=True)
+    cand = torch.gather(cand, 1, o1)
+    ex = torch.gather(ex, 1, o1)
+    o2 = torch.argsort(ex, dim=1, stable=True)
+    return torch.gather(cand, 1, o2)[:, :k], torch.gather(ex, 1, o2)[:, :k], vals[:, kc - 1]
+
+
+def knn_exact_clustered_torch(X: np.ndarray, labels: np.ndarray, k: int, device="cuda",
+                              margin: int = 8, chunk: int = 4096):
+    """Exact kNN for clustered data: search inside each cluster, then certify every row.
+
+    Certificate for row x in cluster A: for every other cluster B, ||x - c_B|| - R_B (c_B
+    the cluster mean, R_B its radius) must exceed the k-th neighbour distance found in A,
+    so no point outside A can be closer.  The in-cluster candidate list is certified like
+    knn_exact_torch.  Rows failing either test are recomputed by global brute force.
+    Returns (idx u32[n,k], dist f32[n,k], n_recomputed)."""
+    import torch
+
+    torch.backends.cuda.matmul.allow_tf32 = False
+    n, dim = X.shape
+    X0 = torch.from_numpy(np.ascontiguousarray(X, dtype=np.float32)).to(device)
+    lab = torch.from_numpy(np.ascontiguousarray(labels, dtype=np.int64)).to(device)
+    idx = torch.empty((n, k), dtype=torch.int64, device=device)
+    dst = torch.empty((n, k), dtype=torch.float32, device=device)
+    bad = torch.zeros(n, dtype=torch.bool, device=device)
+    eps = 4.0 * dim * 2.0 ** -23
+    C = int(labels.max()) + 1
+    centres = torch.zeros((C, dim), dtype=torch.float64, device=device)
+    radius = torch.zeros(C, dtype=torch.float64, device=device)
+    for c in range(C):
+        members = torch.nonzero(lab == c).flatten()
+        if members.numel() == 0:
+            continue
+        Xc0 = X0[members]
+        centres[c] = Xc0.double().mean(0)
+        radius[c] = torch.sqrt(((Xc0.double() - centres[c]) ** 2).sum(1)).max()
+        mu = Xc0.mean(0, keepdim=True)
+        Xc = Xc0 - mu
+        sq = (Xc * Xc).sum(1)
+        m = members.numel()
+        kc = min(m, k + margin)
+        for s in range(0, m, chunk):
+            e = min(m, s + chunk)
+            ci, cd, last = _torch_knn_block(torch, Xc0[s:e], Xc[s:e], Xc0, Xc, sq[s:e], sq, min(k, kc), kc, s)
+            gi = members[ci]
+            if ci.shape[1] < k:
+                bad[members[s:e]] = True
+                continue
+            idx[members[s:e]] = gi
+            dst[members[s:e]] = cd
+            if kc < m:
+                bound = eps * (sq[s:e] + sq.max() + 1.0)
+                bad[members[s:e]] |= (last - bound) <= cd[:, k - 1] ** 2 * (1.0 + 1e-6)
+            else:
+                pass
+    # cross-cluster certificate
+    for s in range(0, n, 1 << 18):
+        e = min(n, s + (1 << 18))
+        dc = torch.cdist(X0[s:e].double(), centres) - radius[None, :]
+        dc[torch.arange(e - s, device=device), lab[s:e]] = float("inf")
+        bad[s:e] |= dc.min(1).values <= dst[s:e, k - 1].double() * (1.0 + 1e-6) + 1e-6
+    bad_rows = torch.nonzero(bad).flatten()
+    Xg = X0 - X0.mean(0, keepdim=True)
+    sqg = (Xg * Xg).sum(1)
+    for s in range(0, bad_rows.numel(), 1024):
+        r = bad_rows[s:s + 1024]
+        D = sqg[r, None] + sqg[None, :] - 2.0 * (Xg[r] @ Xg.T)
+        D[torch.arange(r.numel(), device=device), r] = -1.0
+        kc = min(n, k + 64)
+        _, cand = torch.topk(D, kc, dim=1, largest=False, sorted=True)
+        ex = torch.sqrt(((X0[r][:, None, :] - X0[cand]) ** 2).sum(2))
+        o1 = torch.argsort(cand, dim=1, stable=True)
+        cand = torch.gather(cand, 1, o1)
+        ex = torch.gather(ex, 1, o1)
+        o2 = torch.argsort(ex, dim=1, stable=True)
+        idx[r] = torch.gather(cand, 1, o2)[:, :k]
+        dst[r] = torch.gather(ex, 1, o2)[:, :k]
+    return (idx.to(torch.int32).cpu().numpy().astype(np.uint32), dst.cpu().numpy(),
+            int(bad_rows.numel()))

@@ -31,12 +31,26 @@ namespace {
 
 constexpr uint32_t PAD_ROW = 0xFFFFFFFFu;
 
+// Tuning knobs (compile-time).
+#ifndef UB_SGD_PF
+#define UB_SGD_PF 8          // entries loaded per lane per batch
+#endif
+#ifndef UB_SGD_NEG_BATCH
+#define UB_SGD_NEG_BATCH 8   // negative-sample rows fetched together
+#endif
+#ifndef UB_SGD_MIN_BLOCKS
+#define UB_SGD_MIN_BLOCKS 2  // resident 256-thread blocks per SM the register budget targets
+#endif
+#ifndef UB_PHILOX_ROUNDS
+#define UB_PHILOX_ROUNDS 10
+#endif
+
 // ------------------------------------------------------------------------------ Philox
 // Philox4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as easy as 1, 2, 3",
 // SC'11): counter-based, so every (seed, entry, epoch, block) has its own stream.
 __device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k) {
 #pragma unroll
-  for (int r = 0; r < 10; ++r) {
+  for (int r = 0; r < UB_PHILOX_ROUNDS; ++r) {
     const uint32_t hi0 = __umulhi(0xD2511F53u, c.x), lo0 = 0xD2511F53u * c.x;
     const uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u * c.z;
     c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
@@ -86,8 +100,9 @@ __device__ __forceinline__ float clip4(float v) {
 }
 
 // ------------------------------------------------------------------------------ K7
-constexpr int PF = 8;        // entries loaded per lane per batch (coalesced across the warp)
-constexpr int NEG_BATCH = 8; // negative-sample rows fetched together
+constexpr int PF = UB_SGD_PF;               // entries per lane per batch (coalesced across the warp)
+constexpr int NEG_BATCH = UB_SGD_NEG_BATCH; // negative-sample rows fetched together
+static_assert(NEG_BATCH >= 1 && NEG_BATCH <= 8, "two Philox blocks feed one batch");
 
 template <int DIM>
 __device__ __forceinline__ void load_row(float (&v)[DIM], const float* p) {
@@ -176,7 +191,7 @@ __device__ __forceinline__ void fired_edge(float (&cur)[DIM], uint32_t r, uint32
   // negative samples (:313-341)
   for (uint32_t q0 = 0; q0 < nneg; q0 += NEG_BATCH) {
     if (q0 > 0) {  // rare: more than NEG_BATCH negatives in one firing
-      const uint32_t blk = q0 / 4;
+      const uint32_t blk = 2u * (q0 / NEG_BATCH);  // Philox blocks (2b, 2b+1) for batch b
       const uint4 r0 = philox4x32_10(make_uint4((uint32_t)idx, (uint32_t)(idx >> 32), epoch, blk), key);
       const uint4 r1 = philox4x32_10(make_uint4((uint32_t)idx, (uint32_t)(idx >> 32), epoch, blk + 1), key);
       const uint32_t rv[8] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w};
@@ -207,7 +222,7 @@ __device__ __forceinline__ void fired_edge(float (&cur)[DIM], uint32_t r, uint32
 }
 
 template <int DIM>
-__global__ void __launch_bounds__(256) sgd_epoch_kernel(
+__global__ void __launch_bounds__(256, UB_SGD_MIN_BLOCKS) sgd_epoch_kernel(
     const uint64_t* __restrict__ slice_base, const uint32_t* __restrict__ slice_width,
     const uint32_t* __restrict__ split_mask, const uint32_t* __restrict__ rowid,
     const uint2* __restrict__ entry, uint64_t n_slices, float* __restrict__ live, float* snap,

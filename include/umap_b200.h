@@ -199,6 +199,23 @@ int umap_radix_sort_pairs_device(const uint32_t* dev_keys_in, const uint32_t* de
                                  uint32_t* dev_keys_out, uint32_t* dev_values_out,
                                  uint64_t n, int end_bit);
 
+/* Allocation-free variant of umap_radix_sort_pairs_device (no counterpart in the
+ * reference; the reference has no device code).  For callers that cannot allocate device
+ * memory when they sort: a host application whose allocator owns the whole GPU heap, or a
+ * latency-critical loop that must not enter the CUDA allocator.  It performs no cudaMalloc
+ * / cudaFree and no allocating library call: its scratch is a static device array of about
+ * 9 MiB that every GPU loading this library holds until exit.  At most
+ * umap_radix_sort_noalloc_max_pairs() pairs (1,048,576); larger n returns
+ * UMAP_ERR_INVALID_ARGUMENT.  The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress) with that device current; make that first call before
+ * any stream capture.  Work is queued on `stream` (NULL = the default stream) and the call
+ * returns when it is done.  All calls share the array: calls whose GPU work overlaps (on
+ * different streams or threads) race on it and must be serialised by the caller. */
+int umap_radix_sort_pairs_device_noalloc(const uint32_t* dev_keys_in, const uint32_t* dev_values_in,
+                                         uint32_t* dev_keys_out, uint32_t* dev_values_out,
+                                         uint64_t n, int end_bit, void* stream);
+int umap_radix_sort_noalloc_max_pairs(uint64_t* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1238,4 +1238,21 @@ int umap_radix_sort_pairs_device(const uint32_t* keys_in, const uint32_t* vals_i
   API_END
 }
 
+int umap_radix_sort_pairs_device_noalloc(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
+                                         uint32_t* vals_out, uint64_t n, int end_bit, void* stream) {
+  API_BEGIN
+  need(keys_in, "keys_in"); need(keys_out, "keys_out"); need(vals_out, "values_out");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  radix_sort_pairs_noalloc(keys_in, vals_in, keys_out, vals_out, n, end_bit, s);
+  UB_CUDA(cudaStreamSynchronize(s));
+  API_END
+}
+
+int umap_radix_sort_noalloc_max_pairs(uint64_t* out) {
+  API_BEGIN
+  need(out, "out");
+  *out = radix_sort_noalloc_max_pairs();
+  API_END
+}
+
 }  // extern "C"

@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <mutex>
 
 #include "ub_internal.hpp"
 
@@ -337,6 +338,128 @@ void reduce_sum_u64(const uint64_t* x, uint64_t n, uint64_t* out, cudaStream_t s
     return;
   }
   reduce_impl<uint64_t, SumU64>(x, n, (uint64_t)0, out, SumU64{}, s);
+}
+
+// ------------------------------------------------------------------------------
+// Allocation-free variant of radix_sort_pairs.
+//
+// Some callers cannot allocate device memory at the moment they need this sort: a host
+// application whose allocator owns the whole GPU heap (it reserves the device memory up
+// front and a foreign cudaMalloc would fail or fragment it), or a latency-critical loop
+// that must not enter the CUDA allocator at all.  For them the scratch space lives in the
+// file-scope array below, sized for at most NOALLOC_MAX_PAIRS pairs; every GPU that loads
+// the library holds it (about 9 MiB) until the process exits.  In host code the array's
+// name is only a host-side stand-in, so its device address is looked up with
+// cudaGetSymbolAddress, once per device, with that device current.  Every call shares the
+// array and it keeps the previous call's contents: all of it is fully rewritten before it
+// is read (histograms, offsets and ping-pong buffers), so nothing needs clearing, but two
+// calls whose GPU work overlaps (e.g. on different streams) race on it.
+namespace {
+
+constexpr uint64_t NOALLOC_MAX_PAIRS = 1ull << 20;
+constexpr uint64_t NA_TILES = (NOALLOC_MAX_PAIRS + RS_TILE - 1) / RS_TILE;
+constexpr uint64_t NA_HIST = NA_TILES * RS_RADIX;
+constexpr uint64_t NA_SCAN_TILES = (NA_HIST + SCAN_TILE - 1) / SCAN_TILE;
+constexpr uint64_t align256(uint64_t b) { return (b + 255) / 256 * 256; }
+constexpr uint64_t NOALLOC_SCRATCH_BYTES =
+    2 * align256(NOALLOC_MAX_PAIRS * 4) +          // ping-pong keys / values
+    align256(NA_HIST * 4) + align256((NA_HIST + 1) * 4) +  // digit histograms / offsets
+    2 * align256((NA_SCAN_TILES + 1) * 4) +        // scan tile sums / offsets
+    4096;                                          // slack for the carving's alignment
+
+static __device__ __align__(256) unsigned char g_sort_scratch[NOALLOC_SCRATCH_BYTES];
+
+// Bump allocator over the scratch array (device address).
+struct Carve {
+  unsigned char* p;
+  uint64_t left;
+  template <class T>
+  T* take(uint64_t count) {
+    const uint64_t bytes = align256(count * sizeof(T));
+    if (bytes > left) throw Error(INVALID_ARGUMENT, "allocation-free sort: scratch exhausted");
+    T* r = reinterpret_cast<T*>(p);
+    p += bytes;
+    left -= bytes;
+    return r;
+  }
+};
+
+template <class TIn, class TOut>
+void scan_carved(const TIn* in, TOut* out, uint64_t n, cudaStream_t s, Carve& c) {
+  if (n == 0) {
+    UB_CUDA(cudaMemsetAsync(out, 0, sizeof(TOut), s));
+    return;
+  }
+  const uint64_t tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
+  if (tiles == 1) {
+    scan_tile_apply<TIn, TOut><<<1, SCAN_BT, 0, s>>>(in, n, nullptr, out);
+    UB_LAUNCH_CHECK();
+    return;
+  }
+  TOut* sums = c.take<TOut>(tiles);
+  TOut* offs = c.take<TOut>(tiles + 1);
+  scan_tile_sums<TIn, TOut><<<(unsigned)tiles, SCAN_BT, 0, s>>>(in, n, sums);
+  UB_LAUNCH_CHECK();
+  scan_carved<TOut, TOut>(sums, offs, tiles, s, c);
+  scan_tile_apply<TIn, TOut><<<(unsigned)tiles, SCAN_BT, 0, s>>>(in, n, offs, out);
+  UB_LAUNCH_CHECK();
+}
+
+// Device address of g_sort_scratch on the current device (looked up once per device).
+unsigned char* sort_scratch_address() {
+  static std::mutex mu;
+  static unsigned char* addr[256] = {};
+  int dev = 0;
+  UB_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 256) throw Error(UNSUPPORTED, "device ordinal out of range");
+  std::lock_guard<std::mutex> lock(mu);
+  if (!addr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_sort_scratch);
+    if (e != cudaSuccess || p == nullptr) {
+      (void)cudaGetLastError();
+      throw Error(CUDA, std::string("cudaGetSymbolAddress(sort scratch) failed: ") + cudaGetErrorString(e));
+    }
+    addr[dev] = static_cast<unsigned char*>(p);
+  }
+  return addr[dev];
+}
+
+}  // namespace
+
+uint64_t radix_sort_noalloc_max_pairs() { return NOALLOC_MAX_PAIRS; }
+
+void radix_sort_pairs_noalloc(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
+                              uint32_t* vals_out, uint64_t n, int end_bit, cudaStream_t s) {
+  if (n > NOALLOC_MAX_PAIRS)
+    throw Error(INVALID_ARGUMENT, "allocation-free radix sort takes at most " + std::to_string(NOALLOC_MAX_PAIRS) +
+                                      " pairs, got " + std::to_string(n));
+  unsigned char* base = sort_scratch_address();
+  if (n == 0) return;
+  if (end_bit < 1) end_bit = 1;
+  if (end_bit > 32) end_bit = 32;
+  Carve c{base, NOALLOC_SCRATCH_BYTES};
+  const int passes = (end_bit + 7) / 8;
+  const uint32_t tiles = (uint32_t)((n + RS_TILE - 1) / RS_TILE);
+  uint32_t* tk = c.take<uint32_t>(NOALLOC_MAX_PAIRS);
+  uint32_t* tv = c.take<uint32_t>(NOALLOC_MAX_PAIRS);
+  uint32_t* hist = c.take<uint32_t>((uint64_t)tiles * RS_RADIX);
+  uint32_t* offs = c.take<uint32_t>((uint64_t)tiles * RS_RADIX + 1);
+  const uint32_t* ck = keys_in;
+  const uint32_t* cv = vals_in;
+  for (int p = 0; p < passes; ++p) {
+    const bool to_out = ((passes - 1 - p) % 2) == 0;
+    uint32_t* nk = to_out ? keys_out : tk;
+    uint32_t* nv = to_out ? vals_out : tv;
+    radix_upsweep<<<tiles, RS_BT, 0, s>>>(ck, n, p * 8, hist, tiles);
+    UB_LAUNCH_CHECK();
+    Carve scan_ws = c;  // the scan's temporaries are reused by every pass
+    scan_carved<uint32_t, uint32_t>(hist, offs, (uint64_t)tiles * RS_RADIX, s, scan_ws);
+    radix_downsweep<<<tiles, RS_BT, 0, s>>>(ck, cv, nk, nv, n, p * 8, offs, tiles);
+    UB_LAUNCH_CHECK();
+    ck = nk;
+    cv = nv;
+  }
 }
 
 }  // namespace ub

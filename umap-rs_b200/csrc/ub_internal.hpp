@@ -95,6 +95,11 @@ void scan_u64_to_u64(const uint64_t* in, uint64_t* out, uint64_t n, cudaStream_t
 // keys_out/vals_out may not alias the inputs.  n must be < 2^32.
 void radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
                       uint32_t* vals_out, uint64_t n, int end_bit, cudaStream_t s);
+// Same sort with its scratch in a static device array instead of allocations; n must be
+// at most radix_sort_noalloc_max_pairs().  Calls whose GPU work overlaps race on the array.
+void radix_sort_pairs_noalloc(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
+                              uint32_t* vals_out, uint64_t n, int end_bit, cudaStream_t s);
+uint64_t radix_sort_noalloc_max_pairs();
 // Reductions into a device scalar (*out).
 void reduce_max_f32(const float* x, uint64_t n, float init, float* out, cudaStream_t s);
 void reduce_max_u32(const uint32_t* x, uint64_t n, uint32_t* out, cudaStream_t s);

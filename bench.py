@@ -295,7 +295,7 @@ def main():
         "sgd_edge_updates_per_s": F_tot / (float(np.median(sgd_ms)) / 1e3),
         "e2e": {"value": F_tot / (e2e_step / 1e3), "unit": "edge-updates/s", "ms_per_step": e2e_step,
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-        "roofline": {"bound": "hbm", "kernel": "sgd_epoch_kernel<2>", "achieved": achieved,
+        "roofline": {"bound": "hbm", "kernel": "sgd_epoch_kernel2<2>", "achieved": achieved,
                      "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "peak_source": peak_src,
                      "traffic": tr, "algorithmic_bytes_per_launch": alg_bytes / a.epochs,
                      "avg_launch_ms": sgd_kernel_ms},

@@ -154,6 +154,10 @@ int umap_optimizer_schedule_totals(const umap_optimizer* opt, uint64_t start, ui
 /* Extension: CUDA-event time (ms) of the epoch loop of the last step_epochs call, measured
  * on the optimizer's stream (the SGD kernels only; no host overhead). */
 int umap_optimizer_last_step_ms(const umap_optimizer* opt, float* ms);
+/* Extension: device memory freed by the library is cached for reuse by later calls (growing
+ * the device pool costs ~100 ms per large block).  This returns the cached blocks to the
+ * CUDA pool; *released_bytes (may be NULL) receives their total size. */
+int umap_release_cached_memory(uint64_t* released_bytes);
 /* Extension: number of this library's kernel launches so far in this process. */
 int umap_kernel_launches(uint64_t* out);
 

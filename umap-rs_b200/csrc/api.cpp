@@ -22,6 +22,13 @@ namespace ub {
 thread_local std::string g_last_error;
 static std::atomic<uint64_t> g_launches{0};
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+bool alloc_log_enabled() {
+  static const bool on = getenv("UMAP_B200_LOG") != nullptr;
+  return on;
+}
+void log_slow_alloc(uint64_t bytes, double ms) {
+  fprintf(stderr, "[umap_b200] slow device allocation: %llu bytes took %.1f ms\n", (unsigned long long)bytes, ms);
+}
 
 [[noreturn]] void throw_cuda(cudaError_t e, const char* what, const char* file, int line) {
   (void)cudaGetLastError();
@@ -361,6 +368,8 @@ std::unique_ptr<umap_optimizer> optimizer_new_impl(std::unique_ptr<umap_manifold
                                       std::to_string(man->n_vertices) + " samples");
   if (dims < 1) throw Error(INVALID_ARGUMENT, "n_components must be >= 1, got 0");
   if (man->n_vertices >= 0xFFFFFFFFull) throw Error(UNSUPPORTED, "n_vertices must be < 2^32");
+  if ((total_epochs + 1) * (c.negative_sample_rate + 1) >= 0xFFFFFFFFull)
+    throw Error(UNSUPPORTED, "total_epochs * negative_sample_rate must be < 2^32");
   auto o = std::make_unique<umap_optimizer>();
   o->manifold = std::move(man);
   cudaStream_t s = o->s();
@@ -957,6 +966,13 @@ int umap_optimizer_last_step_ms(const umap_optimizer* opt, float* ms) {
   API_BEGIN
   need(opt, "optimizer"); need(ms, "ms");
   *ms = opt->last_step_ms;
+  API_END
+}
+
+int umap_release_cached_memory(uint64_t* released_bytes) {
+  API_BEGIN
+  uint64_t b = release_cached_memory();
+  if (released_bytes) *released_bytes = b;
   API_END
 }
 

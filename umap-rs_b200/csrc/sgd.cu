@@ -36,10 +36,13 @@ constexpr uint32_t PAD_ROW = 0xFFFFFFFFu;
 #define UB_SGD_PF 8          // entries loaded per lane per batch
 #endif
 #ifndef UB_SGD_NEG_BATCH
-#define UB_SGD_NEG_BATCH 8   // negative-sample rows fetched together
+#define UB_SGD_NEG_BATCH 4   // negative-sample rows fetched together
 #endif
 #ifndef UB_SGD_MIN_BLOCKS
-#define UB_SGD_MIN_BLOCKS 2  // resident 256-thread blocks per SM the register budget targets
+#define UB_SGD_MIN_BLOCKS 4  // resident 256-thread blocks per SM the register budget targets
+#endif
+#ifndef UB_SGD_KERNEL
+#define UB_SGD_KERNEL 2      // 1: warp-batched entries, 2: independent lane progress
 #endif
 #ifndef UB_PHILOX_ROUNDS
 #define UB_PHILOX_ROUNDS 10
@@ -68,27 +71,35 @@ __host__ __device__ __forceinline__ uint32_t q_minus_1(double eps) {
   if (x < 1.0) return 0u;
   return (uint32_t)x - 1u;
 }
-__device__ __forceinline__ uint64_t fires_by(uint64_t n, uint64_t Q) { return (n * Q) >> 32; }
+// All schedule helpers take q = Q - 1 (the stored u32).  n*Q = n*q + n fits in 64 bits for
+// any u32 n, and the product is a single 32x32->64 multiply.
+__device__ __forceinline__ uint64_t fires_by(uint32_t n, uint32_t q) {
+  return ((uint64_t)n * q + n) >> 32;
+}
 // Smallest epoch x with fires_by(x) >= m.
-__device__ __forceinline__ uint64_t fire_epoch(uint64_t m, uint64_t Q) {
-  const float est = (float)m * __fdividef(4294967296.0f, (float)Q);
-  uint64_t x = est > 0.0f ? (uint64_t)ceilf(est) : 0ull;
-  for (int t = 0; t < 8 && x > 0 && fires_by(x - 1, Q) >= m; ++t) --x;
-  for (int t = 0; t < 8 && fires_by(x, Q) < m; ++t) ++x;
+__device__ __forceinline__ uint32_t fire_epoch(uint64_t m, uint32_t q) {
+  const float est = (float)m * __fdividef(4294967296.0f, (float)q + 1.0f);
+  uint32_t x = est > 0.0f ? (est < 4294967040.0f ? (uint32_t)ceilf(est) : 0xFFFFFF00u) : 0u;
+  for (int t = 0; t < 8 && x > 0 && fires_by(x - 1, q) >= m; ++t) --x;
+  for (int t = 0; t < 8 && fires_by(x, q) < m; ++t) ++x;
   return x;
 }
-// Negatives drawn by the firing at epoch n with index m >= 1.
-__device__ __forceinline__ uint32_t negatives_at(uint64_t n, uint64_t m, uint64_t Q, uint64_t negQ) {
-  const int64_t y = (int64_t)((n * negQ) >> 32);
-  const int64_t prev = m <= 1 ? 1 : (int64_t)((fire_epoch(m - 1, Q) * negQ) >> 32);
+// Negatives drawn by the firing at epoch n with index m >= 1 (n * neg < 2^32 is checked on
+// the host).
+__device__ __forceinline__ uint32_t negatives_at(uint32_t n, uint64_t m, uint32_t q, uint32_t neg) {
+  const int64_t y = (int64_t)fires_by(n * neg, q);
+  const int64_t prev = m <= 1 ? 1 : (int64_t)fires_by(fire_epoch(m - 1, q) * neg, q);
   const int64_t d = y - prev;
   return d > 0 ? (uint32_t)d : 0u;
 }
 // Negatives drawn in total after m firings.
-__device__ __forceinline__ uint64_t negatives_after(uint64_t m, uint64_t Q, uint64_t negQ) {
+__device__ __forceinline__ uint64_t negatives_after(uint64_t m, uint32_t q, uint32_t neg) {
   if (m == 0) return 0;
-  const int64_t t = (int64_t)((fire_epoch(m, Q) * negQ) >> 32) - 1;
+  const int64_t t = (int64_t)fires_by(fire_epoch(m, q) * neg, q) - 1;
   return t > 0 ? (uint64_t)t : 0ull;
+}
+__device__ __forceinline__ bool fires_at(uint32_t n, uint32_t q) {
+  return n > 0 && fires_by(n, q) > fires_by(n - 1, q);
 }
 
 // Rust f32::clamp(-4, 4) (utils/clip.rs:13-15): NaN passes through.
@@ -102,7 +113,7 @@ __device__ __forceinline__ float clip4(float v) {
 // ------------------------------------------------------------------------------ K7
 constexpr int PF = UB_SGD_PF;               // entries per lane per batch (coalesced across the warp)
 constexpr int NEG_BATCH = UB_SGD_NEG_BATCH; // negative-sample rows fetched together
-static_assert(NEG_BATCH >= 1 && NEG_BATCH <= 8, "two Philox blocks feed one batch");
+static_assert(NEG_BATCH >= 1 && NEG_BATCH <= 16, "negative batch size");
 
 template <int DIM>
 __device__ __forceinline__ void load_row(float (&v)[DIM], const float* p) {
@@ -158,20 +169,28 @@ __device__ __forceinline__ void fired_edge(float (&cur)[DIM], uint32_t r, uint32
   float* oth = snap + (uint64_t)k * DIM;
   float o[DIM];
   load_row<DIM>(o, oth);
+  // Negative q uses word (q & 3) of Philox block (q >> 2) for this (entry, epoch).
   uint32_t kk[NEG_BATCH];
   float ob[NEG_BATCH][DIM];
-  const uint32_t first = nneg < NEG_BATCH ? nneg : NEG_BATCH;
-  {
-    const uint4 r0 = philox4x32_10(make_uint4((uint32_t)idx, (uint32_t)(idx >> 32), epoch, 0u), key);
-    const uint4 r1 = first > 4 ? philox4x32_10(make_uint4((uint32_t)idx, (uint32_t)(idx >> 32), epoch, 1u), key)
-                               : make_uint4(0, 0, 0, 0);
-    const uint32_t rv[8] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w};
+  uint4 rnd = make_uint4(0, 0, 0, 0);
+  uint32_t rblk = 0xFFFFFFFFu;
+  auto fetch = [&](uint32_t q0) {
 #pragma unroll
     for (int q = 0; q < NEG_BATCH; ++q) {
-      kk[q] = __umulhi(rv[q], p.n_vertices);
-      if ((uint32_t)q < first) load_row<DIM>(ob[q], snap + (uint64_t)kk[q] * DIM);
+      const uint32_t qq = q0 + q;
+      if (qq < nneg) {
+        if ((qq >> 2) != rblk) {
+          rblk = qq >> 2;
+          rnd = philox4x32_10(make_uint4((uint32_t)idx, (uint32_t)(idx >> 32), epoch, rblk), key);
+        }
+        const uint32_t w = qq & 3;
+        const uint32_t rv = w == 0 ? rnd.x : w == 1 ? rnd.y : w == 2 ? rnd.z : rnd.w;
+        kk[q] = __umulhi(rv, p.n_vertices);
+        load_row<DIM>(ob[q], snap + (uint64_t)kk[q] * DIM);
+      }
     }
-  }
+  };
+  fetch(0);
   // attractive step (:284-306)
   float ds = 0.0f;
 #pragma unroll
@@ -190,17 +209,7 @@ __device__ __forceinline__ void fired_edge(float (&cur)[DIM], uint32_t r, uint32
   sub_row<DIM>(oth, g);
   // negative samples (:313-341)
   for (uint32_t q0 = 0; q0 < nneg; q0 += NEG_BATCH) {
-    if (q0 > 0) {  // rare: more than NEG_BATCH negatives in one firing
-      const uint32_t blk = 2u * (q0 / NEG_BATCH);  // Philox blocks (2b, 2b+1) for batch b
-      const uint4 r0 = philox4x32_10(make_uint4((uint32_t)idx, (uint32_t)(idx >> 32), epoch, blk), key);
-      const uint4 r1 = philox4x32_10(make_uint4((uint32_t)idx, (uint32_t)(idx >> 32), epoch, blk + 1), key);
-      const uint32_t rv[8] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w};
-#pragma unroll
-      for (int q = 0; q < NEG_BATCH; ++q) {
-        kk[q] = __umulhi(rv[q], p.n_vertices);
-        if (q0 + q < nneg) load_row<DIM>(ob[q], snap + (uint64_t)kk[q] * DIM);
-      }
-    }
+    if (q0 > 0) fetch(q0);  // more than NEG_BATCH negatives in this firing
 #pragma unroll
     for (int q = 0; q < NEG_BATCH; ++q) {
       if (q0 + q >= nneg) break;
@@ -243,8 +252,7 @@ __global__ void __launch_bounds__(256, UB_SGD_MIN_BLOCKS) sgd_epoch_kernel(
     for (int d = 0; d < DIM; ++d) cur[d] = 0.0f;
 #pragma unroll
   for (int d = 0; d < DIM; ++d) start[d] = cur[d];
-  const uint64_t n = epoch;
-  const uint64_t negQf = p.neg_rate;
+  const uint32_t n = epoch;
   const uint2 key = make_uint2((uint32_t)p.seed, (uint32_t)(p.seed >> 32));
 
   for (uint32_t e0 = 0; e0 < width; e0 += PF) {
@@ -254,8 +262,7 @@ __global__ void __launch_bounds__(256, UB_SGD_MIN_BLOCKS) sgd_epoch_kernel(
     for (int j = 0; j < PF; ++j) {
       const uint32_t e = e0 + j;
       ent[j] = e < width ? __ldcs(entry + base + (uint64_t)e * 32 + lane) : make_uint2(0u, 0u);
-      const uint64_t Q = (uint64_t)ent[j].y + 1ull;
-      if (n > 0 && fires_by(n, Q) > fires_by(n - 1, Q)) mask |= 1u << j;
+      if (fires_at(n, ent[j].y)) mask |= 1u << j;
     }
     while (mask) {
       const int j = __ffs(mask) - 1;
@@ -264,10 +271,77 @@ __global__ void __launch_bounds__(256, UB_SGD_MIN_BLOCKS) sgd_epoch_kernel(
 #pragma unroll
       for (int t = 1; t < PF; ++t)
         if (t == j) en = ent[t];
-      const uint64_t Q = (uint64_t)en.y + 1ull;
-      const uint64_t m = fires_by(n, Q);
-      const uint32_t nneg = negatives_at(n, m, Q, negQf * Q);
+      const uint32_t nneg = negatives_at(n, fires_by(n, en.y), en.y, p.neg_rate);
       const uint64_t idx = base + (uint64_t)(e0 + j) * 32 + lane;
+      fired_edge<DIM>(cur, r, en.x, nneg, snap, p, alpha, idx, epoch, key);
+    }
+  }
+  if (active) {
+    if (split) {
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) atomicAdd(hrow + d, cur[d] - start[d]);
+    } else {
+      store_row<DIM>(hrow, cur);
+    }
+  }
+}
+
+// Variant with independent lane progress: each lane walks its own task through a small
+// register window of entries (refilled on demand, W loads in flight), so a warp runs as long
+// as its busiest task rather than its busiest lane of every batch.
+#ifndef UB_SGD2_W
+#define UB_SGD2_W 4
+#endif
+template <int DIM>
+__global__ void __launch_bounds__(256, UB_SGD_MIN_BLOCKS) sgd_epoch_kernel2(
+    const uint64_t* __restrict__ slice_base, const uint32_t* __restrict__ slice_width,
+    const uint32_t* __restrict__ split_mask, const uint32_t* __restrict__ rowid,
+    const uint2* __restrict__ entry, uint64_t n_slices, float* __restrict__ live, float* snap,
+    SgdParams p, uint32_t epoch, float alpha) {
+  constexpr int W = UB_SGD2_W;
+  const uint64_t slice = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t lane = threadIdx.x & 31;
+  if (slice >= n_slices) return;
+  const uint32_t r = rowid[slice * 32 + lane];
+  const bool active = r != PAD_ROW;
+  const uint32_t width = active ? slice_width[slice] : 0u;
+  const uint64_t base = slice_base[slice];
+  const bool split = (split_mask[slice] >> lane) & 1u;
+  float cur[DIM], start[DIM];
+  float* hrow = live + (uint64_t)(active ? r : 0) * DIM;
+  if (active) load_row<DIM>(cur, hrow);
+  else
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) cur[d] = 0.0f;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) start[d] = cur[d];
+  const uint32_t n = epoch;
+  const uint2 key = make_uint2((uint32_t)p.seed, (uint32_t)(p.seed >> 32));
+  uint2 win[W];
+  uint32_t mask = 0, ew = 0, ebase = 0;
+  for (;;) {
+    while (mask == 0 && ew < width) {
+      ebase = ew;
+#pragma unroll
+      for (int j = 0; j < W; ++j) {
+        const uint32_t e = ew + j;
+        win[j] = e < width ? __ldg(entry + base + (uint64_t)e * 32 + lane) : make_uint2(0u, 0u);
+      }
+#pragma unroll
+      for (int j = 0; j < W; ++j)
+        if (fires_at(n, win[j].y)) mask |= 1u << j;
+      ew += W;
+    }
+    if (!__any_sync(0xFFFFFFFFu, mask != 0)) break;
+    if (mask) {
+      const int j = __ffs(mask) - 1;
+      mask &= mask - 1;
+      uint2 en = win[0];
+#pragma unroll
+      for (int t = 1; t < W; ++t)
+        if (t == j) en = win[t];
+      const uint32_t nneg = negatives_at(n, fires_by(n, en.y), en.y, p.neg_rate);
+      const uint64_t idx = base + (uint64_t)(ebase + j) * 32 + lane;
       fired_edge<DIM>(cur, r, en.x, nneg, snap, p, alpha, idx, epoch, key);
     }
   }
@@ -299,7 +373,7 @@ __global__ void __launch_bounds__(256) sgd_epoch_generic(
   const bool split = (split_mask[slice] >> lane) & 1u;
   const uint32_t dim = p.dim;
   float* cur = live + (uint64_t)r * dim;
-  const uint64_t n = epoch;
+  const uint32_t n = epoch;
   const uint2 key = make_uint2((uint32_t)p.seed, (uint32_t)(p.seed >> 32));
   const float a = p.a, b = p.b;
   auto add = [&](uint32_t d, float v) {
@@ -309,8 +383,7 @@ __global__ void __launch_bounds__(256) sgd_epoch_generic(
   for (uint32_t e = 0; e < width; ++e) {
     const uint64_t idx = base + (uint64_t)e * 32 + lane;
     const uint2 en = __ldcs(entry + idx);
-    const uint64_t Q = (uint64_t)en.y + 1ull;
-    if (!(n > 0 && fires_by(n, Q) > fires_by(n - 1, Q))) continue;
+    if (!fires_at(n, en.y)) continue;
     float* oth = snap + (uint64_t)en.x * dim;
     float ds = 0.0f;
     for (uint32_t d = 0; d < dim; ++d) { const float df = cur[d] - oth[d]; ds += df * df; }
@@ -325,7 +398,7 @@ __global__ void __launch_bounds__(256) sgd_epoch_generic(
       add(d, g);
       atomicAdd(oth + d, -g);
     }
-    const uint32_t nneg = negatives_at(n, fires_by(n, Q), Q, (uint64_t)p.neg_rate * Q);
+    const uint32_t nneg = negatives_at(n, fires_by(n, en.y), en.y, p.neg_rate);
     uint4 rnd = make_uint4(0, 0, 0, 0);
     for (uint32_t q = 0; q < nneg; ++q) {
       if ((q & 3) == 0)
@@ -434,9 +507,9 @@ __global__ void export_state_kernel(const double* __restrict__ eps, uint64_t E, 
   const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= E) return;
   const double e = eps[i];
-  const uint64_t Q = (uint64_t)q_minus_1(e) + 1ull;
-  const uint64_t m = cur > 0 ? fires_by(cur - 1, Q) : 0ull;
-  const uint64_t t = negatives_after(m, Q, neg * Q);
+  const uint32_t q = q_minus_1(e);
+  const uint64_t m = cur > 0 ? fires_by((uint32_t)(cur - 1), q) : 0ull;
+  const uint64_t t = negatives_after(m, q, (uint32_t)neg);
   const double pn = e / (double)neg;
   if (eons) eons[i] = e * ((double)m + 1.0);
   if (epns) epns[i] = pn;
@@ -511,12 +584,12 @@ __global__ void schedule_totals_kernel(const uint2* __restrict__ entry, uint64_t
   const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   unsigned long long f = 0, g = 0;
   if (i < n_entries) {
-    const uint64_t Q = (uint64_t)entry[i].y + 1ull;
+    const uint32_t q = entry[i].y;
     // firings in [start, end) = m(end-1) - m(start-1); negatives telescope the same way.
-    const uint64_t fe = end > 0 ? fires_by(end - 1, Q) : 0ull;
-    const uint64_t fs = start > 0 ? fires_by(start - 1, Q) : 0ull;
+    const uint64_t fe = end > 0 ? fires_by((uint32_t)(end - 1), q) : 0ull;
+    const uint64_t fs = start > 0 ? fires_by((uint32_t)(start - 1), q) : 0ull;
     f = fe - fs;
-    g = negatives_after(fe, Q, neg * Q) - negatives_after(fs, Q, neg * Q);
+    g = negatives_after(fe, q, (uint32_t)neg) - negatives_after(fs, q, (uint32_t)neg);
   }
   for (int o = 16; o > 0; o >>= 1) {
     f += __shfl_xor_sync(0xFFFFFFFFu, f, o);
@@ -676,14 +749,20 @@ void sgd_epoch(const SgdLayout& L, float* live, float* snap, const SgdParams& p,
   const unsigned grid = grid_for(L.n_slices * 32, 256);
 #define UB_SGD_ARGS L.slice_base.p, L.slice_width.p, L.split_mask.p, L.rowid.p, L.entry.p, L.n_slices, live, snap, \
                     p, epoch, alpha
+#if UB_SGD_KERNEL == 2
+#define UB_SGD_K sgd_epoch_kernel2
+#else
+#define UB_SGD_K sgd_epoch_kernel
+#endif
   switch (p.dim) {
-    case 1: sgd_epoch_kernel<1><<<grid, 256, 0, s>>>(UB_SGD_ARGS); break;
-    case 2: sgd_epoch_kernel<2><<<grid, 256, 0, s>>>(UB_SGD_ARGS); break;
-    case 3: sgd_epoch_kernel<3><<<grid, 256, 0, s>>>(UB_SGD_ARGS); break;
-    case 4: sgd_epoch_kernel<4><<<grid, 256, 0, s>>>(UB_SGD_ARGS); break;
+    case 1: UB_SGD_K<1><<<grid, 256, 0, s>>>(UB_SGD_ARGS); break;
+    case 2: UB_SGD_K<2><<<grid, 256, 0, s>>>(UB_SGD_ARGS); break;
+    case 3: UB_SGD_K<3><<<grid, 256, 0, s>>>(UB_SGD_ARGS); break;
+    case 4: UB_SGD_K<4><<<grid, 256, 0, s>>>(UB_SGD_ARGS); break;
     default: sgd_epoch_generic<<<grid, 256, 0, s>>>(UB_SGD_ARGS); break;
   }
 #undef UB_SGD_ARGS
+#undef UB_SGD_K
   UB_LAUNCH_CHECK();
 }
 

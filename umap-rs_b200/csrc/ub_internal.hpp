@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <chrono>
 #include <cstdint>
 #include <stdexcept>
 #include <string>
@@ -39,7 +40,18 @@ void count_launch();
 #define UB_LAUNCH_CHECK() \
   (::ub::count_launch(), ::ub::cuda_check(cudaGetLastError(), "kernel launch", __FILE__, __LINE__))
 
-// Stream-ordered device buffer (cudaMallocAsync / cudaFreeAsync on the owner stream).
+// Allocation diagnostics (UMAP_B200_LOG): reports device allocations whose host call took
+// longer than 1 ms.
+bool alloc_log_enabled();
+void log_slow_alloc(uint64_t bytes, double ms);
+
+// Device memory from the library's cache (alloc.cpp): stream-ordered, blocks reused across
+// calls.  dev_free orders the block's reuse after the work queued so far on `s`.
+void* dev_alloc(uint64_t bytes, cudaStream_t s);
+void dev_free(void* p, uint64_t bytes, cudaStream_t s) noexcept;
+uint64_t release_cached_memory();
+
+// Stream-ordered device buffer from the cache above, owned by one stream.
 template <class T>
 struct DevBuf {
   T* p = nullptr;
@@ -64,20 +76,12 @@ struct DevBuf {
   void alloc(uint64_t count, cudaStream_t st) {
     reset();
     s = st;
-    n = count;
     if (count == 0) return;
-    cudaError_t e = cudaMallocAsync((void**)&p, count * sizeof(T), st);
-    if (e == cudaErrorMemoryAllocation) {
-      (void)cudaGetLastError();
-      p = nullptr;
-      n = 0;
-      throw Error(OUT_OF_MEMORY, "device allocation of " + std::to_string(count * sizeof(T)) +
-                                     " bytes failed");
-    }
-    cuda_check(e, "cudaMallocAsync", __FILE__, __LINE__);
+    p = static_cast<T*>(dev_alloc(count * sizeof(T), st));
+    n = count;
   }
   void reset() noexcept {
-    if (p) (void)cudaFreeAsync(p, s);
+    if (p) dev_free(p, n * sizeof(T), s);
     p = nullptr;
     n = 0;
   }

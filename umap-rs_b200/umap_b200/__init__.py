@@ -158,6 +158,13 @@ def kernel_launches() -> int:
     return v.value
 
 
+def release_cached_memory() -> int:
+    """Return the library's cached device blocks to the CUDA pool; returns their bytes."""
+    v = C.c_uint64()
+    _check(_lib.load().umap_release_cached_memory(C.byref(v)))
+    return v.value
+
+
 def find_ab_params(spread: float, min_dist: float):
     """umap/find_ab_params.rs:9-82 (host code inside the library)."""
     a, b = C.c_float(), C.c_float()

@@ -62,6 +62,7 @@ SIGNATURES = {
     "umap_optimizer_schedule_totals": [P, u64, u64, C.POINTER(u64), C.POINTER(u64)],
     "umap_optimizer_last_step_ms": [P, C.POINTER(f32)],
     "umap_kernel_launches": [C.POINTER(u64)],
+    "umap_release_cached_memory": [C.POINTER(u64)],
     "umap_fitted_embedding": [P, P],
     "umap_fitted_dims": [P, C.POINTER(u64), C.POINTER(u64)],
     "umap_fitted_manifold": [P, PP],

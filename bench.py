@@ -45,6 +45,11 @@ def parse():
     ap.add_argument("--profile", action="store_true",
                     help="profiling run: build one optimizer, run --profile-epochs epochs, exit")
     ap.add_argument("--profile-epochs", type=int, default=24)
+    ap.add_argument("--workload", default="gaussians_2m", choices=["gaussians_2m", "batched"],
+                    help="batched: 4096 independent instances, 200 epochs, vs a per-instance loop")
+    ap.add_argument("--instances", type=int, default=4096)
+    ap.add_argument("--loop-sample", type=int, default=8,
+                    help="per-instance loop timed on every n-th instance, scaled by n")
     return ap.parse_args()
 
 
@@ -175,10 +180,63 @@ def run_reference(a):
     print(json.dumps(line), flush=True)
 
 
+def run_batched(a):
+    """Batched many-instance workload: one batched fit (one kernel launch per epoch over all
+    instances, graph-captured, autotuned) vs a per-instance loop of the plain fit."""
+    import torch
+    import umap_b200 as ub
+    from umap_b200 import workloads as W
+    torch.cuda.set_device(0)
+    t0 = time.time()
+    sizes, idx, dist, init = W.instances_torch(a.instances)
+    torch.cuda.synchronize()
+    gen_s = time.time() - t0
+    off = np.concatenate([[0], np.cumsum(sizes)]).astype(np.uint64)
+    cfg = ub.UmapConfig()
+    cfg.optimization.n_epochs = 200
+    opt = ub.Optimizer.batch(cfg, off, idx, dist, init, 200)
+    F, Nn = opt.schedule_totals(0, 200)
+    E = opt.n_edges()
+    chunk, bt = opt.tuning()
+    del opt
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(max(1, a.warmup)):
+        ub.batch_fit(cfg, off, idx, dist, init)
+    torch.cuda.synchronize()
+    launches0 = ub.kernel_launches()
+    with Clocks(0) as clk:
+        ev0.record()
+        for _ in range(a.steps):
+            ub.batch_fit(cfg, off, idx, dist, init)
+        ev1.record()
+        torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1) / a.steps
+    launches = (ub.kernel_launches() - launches0) // a.steps
+    # per-instance loop of the plain GPU path on every loop_sample-th instance
+    step = max(1, a.loop_sample)
+    t1 = time.perf_counter()
+    for i in range(0, len(sizes), step):
+        lo, hi = int(off[i]), int(off[i + 1])
+        ub.Umap(cfg).fit(hi - lo, idx[lo:hi], dist[lo:hi], init[lo:hi])
+    torch.cuda.synchronize()
+    loop_ms = (time.perf_counter() - t1) * 1e3 * step
+    line = {"metric": "SGD edge-updates/s (batched instances)", "value": F / (ms / 1e3), "unit": "edge-updates/s",
+            "n_gpus": 1, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"instances_{len(sizes)}_logu500-50000_d32_k15_200ep", "points": int(off[-1]),
+                       "kept_edges": E, "edge_updates_per_fit": F, "negatives_per_fit": Nn,
+                       "autotuned_chunk": chunk, "autotuned_block": bt, "generate_s": round(gen_s, 1)},
+            "per_instance_loop_ms": loop_ms, "loop_sample": f"every {step}-th instance, time x {step}",
+            "speedup_vs_loop": loop_ms / ms, "gpu_launches_per_fit": launches, "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     a = parse()
     if a.impl == "reference":
         return run_reference(a)
+    if a.workload == "batched":
+        return run_batched(a)
     import torch
     import umap_b200 as ub
     rank, world, local = dist_info()

@@ -180,6 +180,33 @@ int umap_fit_device(const umap_config* cfg, uint64_t n_samples, const uint32_t* 
                     const float* dev_init, uint64_t init_rows, uint64_t init_cols,
                     umap_fitted** out);
 
+/* ---- batched instances (no counterpart in the reference: a fit per dataset) --------
+ * n_instances independent fits in one problem.  Instance s owns points
+ * [offsets[s], offsets[s+1]) of the concatenated arrays (host offsets, u64[n_instances+1],
+ * offsets[0] = 0); its kNN ids are local to it (0..n_s-1).  Each instance is validated like
+ * learn_manifold (messages prefixed "instance s: ").  Every epoch is one kernel launch over
+ * all instances; the SGD task length and block shape are autotuned on the first batch of a
+ * given size.  The result is an ordinary optimizer handle (step_epochs, embedding,
+ * export_edges, schedule_totals, into_fitted work on it; checkpoints do not). */
+int umap_batch_optimizer_new(const umap_config* cfg, uint64_t n_instances, const uint64_t* host_offsets,
+                             const uint32_t* host_knn_indices, const float* host_knn_dists,
+                             uint64_t knn_cols, const float* host_init, uint64_t init_cols,
+                             uint64_t total_epochs, umap_optimizer** out);
+int umap_batch_optimizer_new_device(const umap_config* cfg, uint64_t n_instances,
+                                    const uint64_t* host_offsets, const uint32_t* dev_knn_indices,
+                                    const float* dev_knn_dists, uint64_t knn_cols, const float* dev_init,
+                                    uint64_t init_cols, uint64_t total_epochs, umap_optimizer** out);
+/* Umap::fit for every instance at once: n_epochs from cfg (or the shared default), rows
+ * with an empty graph row become NaN; writes f32[total points, init_cols]. */
+int umap_batch_fit(const umap_config* cfg, uint64_t n_instances, const uint64_t* host_offsets,
+                   const uint32_t* host_knn_indices, const float* host_knn_dists, uint64_t knn_cols,
+                   const float* host_init, uint64_t init_cols, float* host_embedding_out);
+int umap_batch_fit_device(const umap_config* cfg, uint64_t n_instances, const uint64_t* host_offsets,
+                          const uint32_t* dev_knn_indices, const float* dev_knn_dists, uint64_t knn_cols,
+                          const float* dev_init, uint64_t init_cols, float* dev_embedding_out);
+/* Extension: the SGD task length and threads per block in use (autotuned for batches). */
+int umap_optimizer_tuning(const umap_optimizer* opt, uint32_t* chunk, uint32_t* block_threads);
+
 /* ---- serde checkpoints (optimizer.rs:27, manifold.rs:14, embedding.rs:438) ---------
  * The byte format is this library's own little-endian layout carrying every field of the
  * reference struct (not bincode).  *_serialize writes at most `cap` bytes and sets

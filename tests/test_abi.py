@@ -129,3 +129,13 @@ def test_transform_is_todo_like_reference(ub):
     f = ub.FittedUmap(None)
     with pytest.raises(NotImplementedError, match="Transform not yet implemented"):
         f.transform(None, None, None)
+
+
+def test_batch_validation_names_the_instance(ub):
+    # checked on the host before any device work
+    off = np.array([0, 100, 110], np.uint64)
+    idx = np.zeros((110, 15), np.uint32)
+    dist = np.zeros((110, 15), np.float32)
+    init = np.zeros((110, 2), np.float32)
+    with pytest.raises(ub.UmapError, match=r"^instance 1: Number of samples \(10\) must be > n_neighbors \(15\)$"):
+        ub.Optimizer.batch(ub.UmapConfig(), off, idx, dist, init, 10)

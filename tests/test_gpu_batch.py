@@ -1,0 +1,86 @@
+"""Batched many-instance UMAP (no counterpart in the reference: one fit per dataset there).
+
+The batch must give every instance exactly what a plain fit of that instance gives for the
+deterministic stages (graph, pruned edges + schedule, normalised init), and embeddings of
+the same quality as plain per-instance fits.
+"""
+import numpy as np
+import pytest
+
+from conftest import small_gauss
+
+pytestmark = pytest.mark.gpu
+
+
+def make_batch(sizes, k=15, seed0=100):
+    idxs, dists, inits = [], [], []
+    for i, n in enumerate(sizes):
+        a, b, c = small_gauss(n, k, seed=seed0 + i, d=8, clusters=3)
+        idxs.append(a)
+        dists.append(b)
+        inits.append(c)
+    off = np.concatenate([[0], np.cumsum(sizes)]).astype(np.uint64)
+    return off, idxs, dists, inits
+
+
+def test_batch_matches_per_instance_plain_fits(ub):
+    sizes = [300, 1200, 57, 2500, 800]
+    off, idxs, dists, inits = make_batch(sizes)
+    idxs[1] = idxs[1].copy()
+    idxs[1][::7, -1] = 0xFFFFFFFF                     # sentinels stay sentinels
+    dists[3] = dists[3].copy()
+    dists[3][::11, 4] = np.inf                        # disconnected entries
+    cfg = ub.UmapConfig()
+    total = 120
+    bopt = ub.Optimizer.batch(cfg, off, np.vstack(idxs), np.vstack(dists), np.vstack(inits), total)
+    G = bopt.manifold().graph()
+    bs, br = bopt.manifold().sigmas_rhos()
+    bh, bt, be, _, _, _ = bopt.export_edges()
+    bemb = bopt.embedding()
+    for i, n in enumerate(sizes):
+        lo, hi = int(off[i]), int(off[i + 1])
+        m = ub.Umap(cfg).learn_manifold(n, idxs[i], dists[i])
+        g = m.graph()
+        s, r = m.sigmas_rhos()
+        assert np.array_equal(br[lo:hi], r) and np.array_equal(bs[lo:hi], s)
+        rows = G.indptr[lo:hi + 1]
+        assert np.array_equal(rows - rows[0], g.indptr)
+        assert np.array_equal(G.indices[rows[0]:rows[-1]], g.indices + lo)
+        assert np.array_equal(G.data[rows[0]:rows[-1]], g.data)
+        opt = ub.Optimizer(m, inits[i], total, cfg)
+        h, t, e, _, _, _ = opt.export_edges()
+        sel = (bh >= lo) & (bh < hi)
+        assert np.array_equal(bh[sel], h + lo) and np.array_equal(bt[sel], t + lo)
+        assert np.array_equal(be[sel], e)
+        assert np.array_equal(bemb[lo:hi], opt.embedding())   # per-instance normalisation
+    assert sum(ub.Optimizer(ub.Umap(cfg).learn_manifold(n, idxs[i], dists[i]), inits[i], total, cfg)
+               .schedule_totals(0, total)[0] for i, n in enumerate(sizes)) == bopt.schedule_totals(0, total)[0]
+
+
+def test_batch_fit_quality_matches_plain(ub):
+    from umap_b200 import quality as Q
+    sizes = [900, 2000, 1500, 3000]
+    off, idxs, dists, inits = make_batch(sizes, seed0=300)
+    cfg = ub.UmapConfig()
+    cfg.optimization.n_epochs = 200
+    emb = ub.batch_fit(cfg, off, np.vstack(idxs), np.vstack(dists), np.vstack(inits))
+    assert emb.shape == (int(off[-1]), 2) and np.isfinite(emb).all()
+    for i, n in enumerate(sizes):
+        lo, hi = int(off[i]), int(off[i + 1])
+        m = ub.Umap(cfg).learn_manifold(n, idxs[i], dists[i])
+        a, b = m.curve_params()
+        opt = ub.Optimizer(m, inits[i], 200, cfg)
+        h, t, _, _, _, _ = opt.export_edges()
+        G = opt.manifold().graph()
+        ip = G.indptr.astype(np.int64)
+        w = np.array([G.data[ip[x] + np.searchsorted(G.indices[ip[x]:ip[x + 1]], y)] for x, y in zip(h, t)])
+        ce_b = Q.fuzzy_cross_entropy(emb[lo:hi], h, t, w, a, b)
+        ces = []
+        for seed in (1, 2, 3):
+            o2 = ub.Optimizer(ub.Umap(cfg).learn_manifold(n, idxs[i], dists[i]), inits[i], 200, cfg)
+            o2.set_seed(seed)
+            o2.step_epochs(200)
+            ces.append(Q.fuzzy_cross_entropy(o2.embedding(), h, t, w, a, b))
+        spread = max(ces) - min(ces)
+        print(i, n, ce_b, ces)
+        assert abs(ce_b - np.mean(ces)) <= max(0.02 * np.mean(ces), 3 * spread)

@@ -8,7 +8,9 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -146,6 +148,11 @@ struct umap_optimizer {
   float max_val = 0, threshold = 0, max_w = 1;
   uint64_t seed = 0;
   float last_step_ms = 0;  // CUDA-event time of the last step_epochs epoch loop
+  // Batched instances (n_seg > 0): instance s owns rows [seg_off[s], seg_off[s+1]).
+  uint32_t n_seg = 0;
+  ub::DevBuf<uint64_t> seg_off;
+  ub::DevBuf<uint32_t> row_seg;
+  ub::DevBuf<float> seg_thr, seg_maxw;
   cudaStream_t s() const { return manifold->s(); }
 };
 
@@ -203,7 +210,8 @@ GraphParams graph_params(const umap_config& c) {
 // embedding.rs:149-240 on device arrays.
 std::unique_ptr<umap_manifold> learn_manifold_impl(const umap_config& c, uint64_t n_samples,
                                                    const uint32_t* idx, const float* dist,
-                                                   uint64_t rows, uint64_t cols) {
+                                                   uint64_t rows, uint64_t cols,
+                                                   const Segments* seg = nullptr) {
   std::string err = validate_parameters(c, n_samples, rows, cols);
   if (!err.empty()) throw Error(INVALID_ARGUMENT, err);
   const uint64_t n = n_samples, k = cols;
@@ -224,7 +232,7 @@ std::unique_ptr<umap_manifold> learn_manifold_impl(const umap_config& c, uint64_
 
   m->sigmas.alloc(n, s);
   m->rhos.alloc(n, s);
-  smooth_knn(dist, n, k, gp, m->sigmas.p, m->rhos.p, s);
+  smooth_knn(dist, n, k, gp, m->sigmas.p, m->rhos.p, s, seg);
   log.mark("smooth_knn_dist complete");
 
   DevBuf<uint32_t> pcol(n * k, s), cnt(n, s);
@@ -345,12 +353,19 @@ struct KeptEdges {
 void compute_kept_edges(const umap_optimizer& o, KeptEdges& K, bool want_tail, bool want_eps) {
   const umap_manifold& m = *o.manifold;
   cudaStream_t s = o.s();
+  SegmentPrune sp;
+  if (o.n_seg) {
+    sp.seg_thr = o.seg_thr.p;
+    sp.seg_maxw = o.seg_maxw.p;
+    sp.row_seg = o.row_seg.p;
+  }
+  const SegmentPrune* spp = o.n_seg ? &sp : nullptr;
   K.ptr.alloc(m.n_vertices + 1, s);
-  prune_edges(m.indptr.p, m.data.p, m.n_vertices, o.threshold, K.ptr.p, &K.E, s);
+  prune_edges(m.indptr.p, m.data.p, m.n_vertices, o.threshold, K.ptr.p, &K.E, s, spp);
   if (want_tail) K.tail.alloc(K.E, s);
   if (want_eps) K.eps.alloc(K.E, s);
   export_edges(m.indptr.p, m.indices.p, m.data.p, m.n_vertices, o.threshold, o.max_w, o.total_epochs,
-               K.ptr.p, nullptr, want_tail ? K.tail.p : nullptr, want_eps ? K.eps.p : nullptr, s);
+               K.ptr.p, nullptr, want_tail ? K.tail.p : nullptr, want_eps ? K.eps.p : nullptr, s, spp);
 }
 
 // optimizer.rs:74-290.  `init` is a device array of n*dim floats on stream `s` (or host).
@@ -432,6 +447,8 @@ SgdParams sgd_params(const umap_optimizer& o) {
   p.n_vertices = (uint32_t)o.manifold->n_vertices;
   p.dim = (uint32_t)o.dim;
   p.seed = o.seed;
+  p.row_seg = o.n_seg ? o.row_seg.p : nullptr;
+  p.seg_off = o.n_seg ? o.seg_off.p : nullptr;
   return p;
 }
 
@@ -450,13 +467,51 @@ void step_epochs_impl(umap_optimizer& o, uint64_t n_ep) {
   cudaEvent_t ev[2];
   UB_CUDA(cudaEventCreate(&ev[0]));
   UB_CUDA(cudaEventCreate(&ev[1]));
+  // The epoch loop is captured into a CUDA graph (one kernel node per epoch, each with its
+  // own epoch and learning rate) and launched once.
+  static const bool no_graph = [] {
+    const char* e = getenv("UMAP_B200_GRAPH");
+    return e && e[0] == '0';
+  }();
+  // Worth it where launches are a visible share of an epoch: batches and small graphs.
+  const bool use_graph = !no_graph && n_ep >= 2 && o.layout.n_slices > 0 &&
+                         (o.n_seg > 0 || o.layout.n_edges < (8ull << 20));
+  cudaGraphExec_t exec = nullptr;
+  if (use_graph) {
+    cudaGraph_t graph = nullptr;
+    UB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    try {
+      for (uint64_t epoch = o.current_epoch; epoch < o.current_epoch + n_ep; ++epoch) {
+        const float alpha = o.initial_alpha * (1.0f - ((float)epoch / (float)o.total_epochs));  // :317
+        sgd_epoch(o.layout, live, snap, p, (uint32_t)epoch, alpha, s);
+      }
+    } catch (...) {
+      cudaGraph_t g2 = nullptr;
+      (void)cudaStreamEndCapture(s, &g2);
+      if (g2) (void)cudaGraphDestroy(g2);
+      (void)cudaGetLastError();
+      throw;
+    }
+    UB_CUDA(cudaStreamEndCapture(s, &graph));
+    cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+    (void)cudaGraphDestroy(graph);
+    UB_CUDA(ie);
+  }
   UB_CUDA(cudaEventRecord(ev[0], s));
-  for (uint64_t epoch = o.current_epoch; epoch < o.current_epoch + n_ep; ++epoch) {
-    const float alpha = o.initial_alpha * (1.0f - ((float)epoch / (float)o.total_epochs));  // :317
-    sgd_epoch(o.layout, live, snap, p, (uint32_t)epoch, alpha, s);
+  if (use_graph) {
+    cudaError_t le = cudaGraphLaunch(exec, s);
+    if (le != cudaSuccess) (void)cudaGraphExecDestroy(exec);
+    UB_CUDA(le);
+  } else {
+    for (uint64_t epoch = o.current_epoch; epoch < o.current_epoch + n_ep; ++epoch) {
+      const float alpha = o.initial_alpha * (1.0f - ((float)epoch / (float)o.total_epochs));  // :317
+      sgd_epoch(o.layout, live, snap, p, (uint32_t)epoch, alpha, s);
+    }
   }
   UB_CUDA(cudaEventRecord(ev[1], s));
-  UB_CUDA(cudaStreamSynchronize(s));
+  cudaError_t se = cudaStreamSynchronize(s);
+  if (exec) (void)cudaGraphExecDestroy(exec);
+  UB_CUDA(se);
   float ms = 0.0f;
   (void)cudaEventElapsedTime(&ms, ev[0], ev[1]);
   (void)cudaEventDestroy(ev[0]);
@@ -519,6 +574,213 @@ std::unique_ptr<umap_fitted> fit_impl(const umap_config& c, uint64_t n_samples, 
   nan_empty_rows(f->manifold->indptr.p, f->n, (uint32_t)f->dim, f->embedding.p, f->s());  // :327-334
   UB_CUDA(cudaStreamSynchronize(f->s()));
   return f;
+}
+
+// ------------------------------------------------------------------ autotuning
+// Picks the SGD task length ("edges per thread") and the block shape by timing a few
+// epochs of each candidate on a scratch copy of the embedding.  Choices are cached per
+// problem size (vertices, edges in MiB units, dims) for the life of the process.
+struct TuneKey {
+  uint64_t n, e_mib, dim;
+  bool operator<(const TuneKey& o) const {
+    return n != o.n ? n < o.n : e_mib != o.e_mib ? e_mib < o.e_mib : dim < o.dim;
+  }
+};
+std::mutex& g_tune_mu = *new std::mutex;
+std::map<TuneKey, std::pair<uint32_t, uint32_t>>& g_tuned = *new std::map<TuneKey, std::pair<uint32_t, uint32_t>>;
+
+void tune_layout(umap_optimizer& o, const KeptEdges& K) {
+  cudaStream_t s = o.s();
+  const uint64_t n = o.manifold->n_vertices;
+  const TuneKey key{n, K.E >> 20, o.dim};
+  Segments sgs{o.n_seg, o.seg_off.p, o.row_seg.p};
+  const Segments* seg_ptr = o.n_seg ? &sgs : nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    auto it = g_tuned.find(key);
+    if (it != g_tuned.end()) {
+      build_sgd_layout(K.ptr.p, K.tail.p, K.eps.p, n, it->second.first, o.layout, s, seg_ptr);
+      o.layout.block_threads = it->second.second;
+      return;
+    }
+  }
+  const uint32_t chunks[] = {32, 64, 128, 256};
+  const uint32_t blocks[] = {128, 256};
+  const uint32_t mid = (uint32_t)std::max<uint64_t>(1, o.total_epochs / 2);
+  DevBuf<float> scratch(2 * n * o.dim, s);
+  d2d(scratch.p, o.emb2.p, n * o.dim, s);
+  d2d(scratch.p + n * o.dim, o.emb2.p, n * o.dim, s);
+  const SgdParams p = sgd_params(o);
+  cudaEvent_t e0, e1;
+  UB_CUDA(cudaEventCreate(&e0));
+  UB_CUDA(cudaEventCreate(&e1));
+  float best = 1e30f;
+  uint32_t best_chunk = 0, best_bt = 256;
+  for (uint32_t ch : chunks) {
+    SgdLayout L;
+    build_sgd_layout(K.ptr.p, K.tail.p, K.eps.p, n, ch, L, s, seg_ptr);
+    for (uint32_t bt : blocks) {
+      L.block_threads = bt;
+      sgd_epoch(L, scratch.p, scratch.p + n * o.dim, p, mid, 0.5f, s);  // warm-up
+      UB_CUDA(cudaEventRecord(e0, s));
+      for (int r = 0; r < 2; ++r) sgd_epoch(L, scratch.p, scratch.p + n * o.dim, p, mid + r, 0.5f, s);
+      UB_CUDA(cudaEventRecord(e1, s));
+      UB_CUDA(cudaEventSynchronize(e1));
+      float ms = 0;
+      UB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      if (ms < best) {
+        best = ms;
+        best_chunk = ch;
+        best_bt = bt;
+      }
+    }
+  }
+  (void)cudaEventDestroy(e0);
+  (void)cudaEventDestroy(e1);
+  build_sgd_layout(K.ptr.p, K.tail.p, K.eps.p, n, best_chunk, o.layout, s, seg_ptr);
+  o.layout.block_threads = best_bt;
+  if (getenv("UMAP_B200_LOG"))
+    fprintf(stderr, "[umap_b200] autotune: chunk=%u block=%u (%.3f ms / 2 epochs)\n", best_chunk, best_bt, best);
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  g_tuned[key] = {best_chunk, best_bt};
+}
+
+// ------------------------------------------------------------------ batched instances
+// Many independent UMAP fits in one problem: instance s owns points [off[s], off[s+1]) and
+// its kNN ids are local to it.  The graph of the batch is block diagonal, so every
+// row-local step (smooth-kNN, membership, transpose, union) is the plain one on global
+// ids; the per-instance steps (distance-mean fallback, prune threshold, max weight, init
+// normalisation, negative-sample range) use the instance tables.  Each epoch is one kernel
+// launch over all instances.
+std::unique_ptr<umap_optimizer> batch_new_impl(const umap_config& c, uint64_t n_inst, const uint64_t* h_off,
+                                               const uint32_t* idx, const float* dist, uint64_t k,
+                                               const float* init, uint64_t dims, uint64_t total_epochs,
+                                               bool host) {
+  if (n_inst == 0) throw Error(INVALID_ARGUMENT, "n_instances must be >= 1");
+  if (n_inst >= 0xFFFFFFFFull) throw Error(UNSUPPORTED, "too many instances");
+  if (h_off[0] != 0) throw Error(INVALID_ARGUMENT, "instance offsets must start at 0");
+  for (uint64_t i = 0; i < n_inst; ++i) {
+    if (h_off[i + 1] < h_off[i]) throw Error(INVALID_ARGUMENT, "instance offsets must be non-decreasing");
+    const uint64_t ns = h_off[i + 1] - h_off[i];
+    std::string err = validate_parameters(c, ns, ns, k);
+    if (!err.empty()) throw Error(INVALID_ARGUMENT, "instance " + std::to_string(i) + ": " + err);
+  }
+  if (dims < 1) throw Error(INVALID_ARGUMENT, "n_components must be >= 1, got 0");
+  const uint64_t N = h_off[n_inst];
+  if (N >= 0xFFFFFFFFull || N * k >= 0xFFFFFFFFull)
+    throw Error(UNSUPPORTED, "total points * n_neighbors must be < 2^32 on this build");
+  if ((total_epochs + 1) * (c.negative_sample_rate + 1) >= 0xFFFFFFFFull)
+    throw Error(UNSUPPORTED, "total_epochs * negative_sample_rate must be < 2^32");
+
+  cudaStream_t s0;
+  UB_CUDA(cudaStreamCreateWithFlags(&s0, cudaStreamNonBlocking));
+  struct SGuard { cudaStream_t s; ~SGuard() { (void)cudaStreamSynchronize(s); (void)cudaStreamDestroy(s); } } guard{s0};
+  DevBuf<uint64_t> seg_off(n_inst + 1, s0);
+  DevBuf<uint32_t> row_seg(N, s0);
+  h2d(seg_off.p, h_off, n_inst + 1, s0);
+  fill_row_segments(seg_off.p, (uint32_t)n_inst, row_seg.p, s0);
+  Segments sg{(uint32_t)n_inst, seg_off.p, row_seg.p};
+  DevBuf<uint32_t> gidx(N * k, s0), hidx;
+  DevBuf<float> hdist;
+  const float* ddist = dist;
+  if (host) {
+    hidx.alloc(N * k, s0);
+    hdist.alloc(N * k, s0);
+    h2d(hidx.p, idx, N * k, s0);
+    h2d(hdist.p, dist, N * k, s0);
+    ddist = hdist.p;
+    localize_knn(hidx.p, N, k, sg, gidx.p, s0);
+  } else {
+    localize_knn(idx, N, k, sg, gidx.p, s0);
+  }
+  UB_CUDA(cudaStreamSynchronize(s0));
+  auto man = learn_manifold_impl(c, N, gidx.p, ddist, N, k, &sg);
+  UB_CUDA(cudaStreamSynchronize(man->s()));
+
+  auto o = std::make_unique<umap_optimizer>();
+  o->manifold = std::move(man);
+  cudaStream_t s = o->s();
+  o->n_seg = (uint32_t)n_inst;
+  o->seg_off = std::move(seg_off);
+  o->seg_off.set_stream(s);
+  o->row_seg = std::move(row_seg);
+  o->row_seg.set_stream(s);
+  o->gamma = c.repulsion_strength;
+  o->initial_alpha = c.learning_rate;
+  o->negative_sample_rate = c.negative_sample_rate;
+  o->metric_type = UMAP_METRIC_EUCLIDEAN;
+  o->n = N;
+  o->dim = dims;
+  o->total_epochs = total_epochs;
+  o->current_epoch = 0;
+
+  // per-instance threshold and max weight (optimizer.rs:90-102, make_epochs_per_sample.rs:26-32)
+  DevBuf<float> smax(n_inst, s);
+  segment_max(o->manifold->indptr.p, o->manifold->data.p, o->seg_off.p, (uint32_t)n_inst, smax.p, s);
+  std::vector<float> hmax(n_inst), hthr(n_inst), hmw(n_inst);
+  d2h(hmax.data(), smax.p, n_inst, s);
+  UB_CUDA(cudaStreamSynchronize(s));
+  for (uint64_t i = 0; i < n_inst; ++i) {
+    const uint64_t ns = h_off[i + 1] - h_off[i];
+    const uint64_t default_epochs = ns <= 10000 ? 500 : 200;
+    const uint64_t threshold_epochs = total_epochs > 10 ? total_epochs : default_epochs;
+    hthr[i] = hmax[i] / (float)threshold_epochs;
+    hmw[i] = hmax[i] > 0.0f ? hmax[i] : 1.0f;
+    o->max_val = std::max(o->max_val, hmax[i]);
+  }
+  o->seg_thr.alloc(n_inst, s);
+  o->seg_maxw.alloc(n_inst, s);
+  h2d(o->seg_thr.p, hthr.data(), n_inst, s);
+  h2d(o->seg_maxw.p, hmw.data(), n_inst, s);
+  UB_CUDA(cudaStreamSynchronize(s));
+
+  o->emb2.alloc(2 * N * dims, s);
+  if (host) h2d(o->emb2.p, init, N * dims, s);
+  else d2d(o->emb2.p, init, N * dims, s);
+  Segments so{(uint32_t)n_inst, o->seg_off.p, o->row_seg.p};
+  normalize_init(o->emb2.p, N, (uint32_t)dims, s, &so);
+  {
+    KeptEdges K;
+    compute_kept_edges(*o, K, true, true);
+    static const bool no_tune = [] {
+      const char* e = getenv("UMAP_B200_AUTOTUNE");
+      return e && e[0] == '0';
+    }();
+    if (no_tune || total_epochs < 2) build_sgd_layout(K.ptr.p, K.tail.p, K.eps.p, N, 0, o->layout, s, &so);
+    else tune_layout(*o, K);
+  }
+  set_l2_window(*o, true);
+  UB_CUDA(cudaStreamSynchronize(s));
+  return o;
+}
+
+uint64_t batch_epochs(const umap_config& c, uint64_t n_inst, const uint64_t* h_off) {
+  if (c.has_n_epochs) return c.n_epochs;
+  uint64_t e = 0;
+  for (uint64_t i = 0; i < n_inst; ++i) {
+    const uint64_t ns = h_off[i + 1] - h_off[i];
+    const uint64_t d = ns <= 10000 ? 500 : 200;  // embedding.rs:304-308
+    if (e && d != e)
+      throw Error(UNSUPPORTED, "instances straddle 10,000 points, so their default epoch counts differ; "
+                               "set optimization.n_epochs for a batched fit");
+    e = d;
+  }
+  return e;
+}
+
+void batch_fit_impl(const umap_config& c, uint64_t n_inst, const uint64_t* h_off, const uint32_t* idx,
+                    const float* dist, uint64_t k, const float* init, uint64_t icols, float* out, bool host) {
+  if (icols != c.n_components)
+    throw Error(INVALID_ARGUMENT, "init has " + std::to_string(icols) + " components but n_components is " +
+                                      std::to_string(c.n_components));
+  const uint64_t total = batch_epochs(c, n_inst, h_off);
+  auto o = batch_new_impl(c, n_inst, h_off, idx, dist, k, init, icols, total, host);
+  step_epochs_impl(*o, total);
+  cudaStream_t s = o->s();
+  nan_empty_rows(o->manifold->indptr.p, o->n, (uint32_t)o->dim, o->emb2.p, s);  // embedding.rs:327-334
+  if (host) d2h(out, o->emb2.p, o->n * o->dim, s);
+  else d2d(out, o->emb2.p, o->n * o->dim, s);
+  UB_CUDA(cudaStreamSynchronize(s));
 }
 
 // ------------------------------------------------------------------ serialization
@@ -1073,6 +1335,7 @@ int umap_manifold_deserialize(const uint8_t* buf, uint64_t len, umap_manifold** 
 int umap_optimizer_serialize(const umap_optimizer* o, uint8_t* buf, uint64_t cap, uint64_t* needed) {
   API_BEGIN
   need(o, "optimizer");
+  if (o->n_seg) throw Error(UNSUPPORTED, "checkpoints of batched optimizers are not supported");
   o->manifold->stream->activate();
   cudaStream_t s = o->s();
   Writer w;
@@ -1215,6 +1478,60 @@ int umap_fitted_deserialize(const uint8_t* buf, uint64_t len, umap_fitted** out)
   h2d(f->embedding.p, tmp.data(), cnt, f->s());
   UB_CUDA(cudaStreamSynchronize(f->s()));
   *out = f.release();
+  API_END
+}
+
+// ---- batched instances
+int umap_batch_optimizer_new(const umap_config* cfg, uint64_t n_instances, const uint64_t* offsets,
+                             const uint32_t* idx, const float* dist, uint64_t knn_cols, const float* init,
+                             uint64_t init_cols, uint64_t total_epochs, umap_optimizer** out) {
+  API_BEGIN
+  need(cfg, "cfg"); need(offsets, "offsets"); need(idx, "knn_indices"); need(dist, "knn_dists");
+  need(init, "init"); need(out, "out");
+  *out = nullptr;
+  *out = batch_new_impl(*cfg, n_instances, offsets, idx, dist, knn_cols, init, init_cols, total_epochs, true)
+             .release();
+  API_END
+}
+
+int umap_batch_optimizer_new_device(const umap_config* cfg, uint64_t n_instances, const uint64_t* offsets,
+                                    const uint32_t* idx, const float* dist, uint64_t knn_cols, const float* init,
+                                    uint64_t init_cols, uint64_t total_epochs, umap_optimizer** out) {
+  API_BEGIN
+  need(cfg, "cfg"); need(offsets, "offsets"); need(idx, "knn_indices"); need(dist, "knn_dists");
+  need(init, "init"); need(out, "out");
+  *out = nullptr;
+  UB_CUDA(cudaDeviceSynchronize());
+  *out = batch_new_impl(*cfg, n_instances, offsets, idx, dist, knn_cols, init, init_cols, total_epochs, false)
+             .release();
+  API_END
+}
+
+int umap_batch_fit(const umap_config* cfg, uint64_t n_instances, const uint64_t* offsets, const uint32_t* idx,
+                   const float* dist, uint64_t knn_cols, const float* init, uint64_t init_cols, float* out) {
+  API_BEGIN
+  need(cfg, "cfg"); need(offsets, "offsets"); need(idx, "knn_indices"); need(dist, "knn_dists");
+  need(init, "init"); need(out, "out");
+  batch_fit_impl(*cfg, n_instances, offsets, idx, dist, knn_cols, init, init_cols, out, true);
+  API_END
+}
+
+int umap_batch_fit_device(const umap_config* cfg, uint64_t n_instances, const uint64_t* offsets,
+                          const uint32_t* idx, const float* dist, uint64_t knn_cols, const float* init,
+                          uint64_t init_cols, float* out) {
+  API_BEGIN
+  need(cfg, "cfg"); need(offsets, "offsets"); need(idx, "knn_indices"); need(dist, "knn_dists");
+  need(init, "init"); need(out, "out");
+  UB_CUDA(cudaDeviceSynchronize());
+  batch_fit_impl(*cfg, n_instances, offsets, idx, dist, knn_cols, init, init_cols, out, false);
+  API_END
+}
+
+int umap_optimizer_tuning(const umap_optimizer* opt, uint32_t* chunk, uint32_t* block_threads) {
+  API_BEGIN
+  need(opt, "optimizer");
+  if (chunk) *chunk = opt->layout.chunk;
+  if (block_threads) *block_threads = opt->layout.block_threads;
   API_END
 }
 

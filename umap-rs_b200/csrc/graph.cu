@@ -140,18 +140,24 @@ __global__ void __launch_bounds__(BT) smooth_knn_kernel(const float* __restrict_
   rhos[i] = rho;
 }
 
-// distances.mean() over the whole contiguous [n, k] array (smooth_knn_dist.rs:74), in the
-// exact order of ndarray's unrolled fold: 8 sequential partial sums.  One warp, lanes 0-7
-// each own one partial sum; only runs when some row needs it.
-__global__ void global_mean_kernel(const float* __restrict__ dist, uint64_t total,
-                                   const unsigned* __restrict__ need, float* __restrict__ out) {
+// distances.mean() over a contiguous [rows, k] array (smooth_knn_dist.rs:74), in the exact
+// order of ndarray's unrolled fold: 8 sequential partial sums.  One warp per segment (a
+// batch instance; a plain fit is one segment), lanes 0-7 each own one partial sum; only
+// runs when some row needs it.
+__global__ void segment_mean_kernel(const float* __restrict__ dist, uint32_t k,
+                                    const uint64_t* __restrict__ seg_off, uint64_t n,
+                                    const unsigned* __restrict__ need, float* __restrict__ out) {
   if (*need == 0) return;
+  const uint32_t sgm = blockIdx.x;
+  const uint64_t r0 = seg_off ? seg_off[sgm] : 0, r1 = seg_off ? seg_off[sgm + 1] : n;
+  const uint64_t total = (r1 - r0) * k;
+  const float* x0 = dist + r0 * k;
   const int lane = threadIdx.x;
   __shared__ float s_p[8];
   const uint64_t chunks = total / 8;
   if (lane < 8) {
     float p = 0.0f;
-    const float* x = dist + lane;
+    const float* x = x0 + lane;
     uint64_t c = 0;
     for (; c + 8 <= chunks; c += 8) {
       float v[8];
@@ -171,21 +177,42 @@ __global__ void global_mean_kernel(const float* __restrict__ dist, uint64_t tota
     acc = __fadd_rn(acc, __fadd_rn(s_p[2], s_p[6]));
     acc = __fadd_rn(acc, __fadd_rn(s_p[3], s_p[7]));
     const uint64_t rem = total - chunks * 8;
-    for (uint64_t t = 0; t < rem && t < 7; ++t) acc = __fadd_rn(acc, dist[chunks * 8 + t]);
-    *out = __fdiv_rn(acc, __ull2float_rn(total));
+    for (uint64_t t = 0; t < rem && t < 7; ++t) acc = __fadd_rn(acc, x0[chunks * 8 + t]);
+    out[sgm] = total ? __fdiv_rn(acc, __ull2float_rn(total)) : 0.0f;
   }
 }
 
 __global__ void global_mean_fixup(float* __restrict__ sigmas, const float* __restrict__ rhos,
                                   uint64_t n, const unsigned* __restrict__ need,
-                                  const float* __restrict__ gmean) {
+                                  const float* __restrict__ gmean, const uint32_t* __restrict__ row_seg) {
   if (*need == 0) return;
   const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   if (!(rhos[i] > 0.0f)) {
-    float lim = __fmul_rn(MIN_K_DIST_SCALE, *gmean);
+    float lim = __fmul_rn(MIN_K_DIST_SCALE, gmean[row_seg ? row_seg[i] : 0]);
     if (sigmas[i] < lim) sigmas[i] = lim;
   }
+}
+
+// Batched instances: local kNN ids (0..n_s-1 within instance s) -> global vertex ids; ids
+// outside the instance become the sentinel 0xFFFFFFFF (skipped like the reference's
+// `knn_idx >= n_samples`, fuzzy_simplicial_set.rs:192).
+__global__ void localize_kernel(const uint32_t* __restrict__ idx, uint64_t n, uint32_t k,
+                                const uint32_t* __restrict__ row_seg, const uint64_t* __restrict__ seg_off,
+                                uint32_t* __restrict__ out) {
+  const uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n * k) return;
+  const uint32_t sgm = row_seg[p / k];
+  const uint64_t off = seg_off[sgm], ns = seg_off[sgm + 1] - off;
+  const uint32_t v = idx[p];
+  out[p] = (uint64_t)v < ns ? (uint32_t)(off + v) : 0xFFFFFFFFu;
+}
+
+__global__ void row_segment_kernel(const uint64_t* __restrict__ seg_off, uint32_t n_seg,
+                                   uint32_t* __restrict__ row_seg) {
+  const uint32_t sgm = blockIdx.x;
+  if (sgm >= n_seg) return;
+  for (uint64_t r = seg_off[sgm] + threadIdx.x; r < seg_off[sgm + 1]; r += blockDim.x) row_seg[r] = sgm;
 }
 
 // ------------------------------------------------------------------------------ K2
@@ -360,10 +387,11 @@ inline unsigned grid_for(uint64_t n, unsigned bt) { return (unsigned)((n + bt - 
 }  // namespace
 
 void smooth_knn(const float* dist, uint64_t n, uint64_t k, const GraphParams& gp, float* sigmas,
-                float* rhos, cudaStream_t s) {
+                float* rhos, cudaStream_t s, const Segments* seg) {
   if (n == 0) return;
+  const uint32_t n_seg = seg ? seg->n_seg : 1u;
   DevBuf<unsigned> need(1, s);
-  DevBuf<float> gmean(1, s);
+  DevBuf<float> gmean(n_seg, s);
   UB_CUDA(cudaMemsetAsync(need.p, 0, sizeof(unsigned), s));
   const uint32_t stride = (uint32_t)k | 1u;
   const size_t smem = (size_t)BT * stride * sizeof(float);
@@ -374,9 +402,10 @@ void smooth_knn(const float* dist, uint64_t n, uint64_t k, const GraphParams& gp
     smooth_knn_kernel<false><<<grid, BT, 0, s>>>(dist, n, (uint32_t)k, gp, sigmas, rhos, need.p);
   }
   UB_LAUNCH_CHECK();
-  global_mean_kernel<<<1, 32, 0, s>>>(dist, n * k, need.p, gmean.p);
+  segment_mean_kernel<<<n_seg, 32, 0, s>>>(dist, (uint32_t)k, seg ? seg->seg_off : nullptr, n, need.p, gmean.p);
   UB_LAUNCH_CHECK();
-  global_mean_fixup<<<grid_for(n, 256), 256, 0, s>>>(sigmas, rhos, n, need.p, gmean.p);
+  global_mean_fixup<<<grid_for(n, 256), 256, 0, s>>>(sigmas, rhos, n, need.p, gmean.p,
+                                                     seg ? seg->row_seg : nullptr);
   UB_LAUNCH_CHECK();
 }
 
@@ -420,6 +449,19 @@ void union_rows(const uint32_t* pcol, const float* pw, const uint32_t* cnt, uint
   if (n == 0) return;
   union_kernel<<<grid_for(n, BT), BT, 0, s>>>(pcol, pw, cnt, (uint32_t)k, tptr, tvals, n, gp.mix,
                                               gp.prod_coeff, out_cnt, out_ptr, out_idx, out_w, fill);
+  UB_LAUNCH_CHECK();
+}
+
+void localize_knn(const uint32_t* idx, uint64_t n, uint64_t k, const Segments& seg, uint32_t* out,
+                  cudaStream_t s) {
+  if (n * k == 0) return;
+  localize_kernel<<<grid_for(n * k, 256), 256, 0, s>>>(idx, n, (uint32_t)k, seg.row_seg, seg.seg_off, out);
+  UB_LAUNCH_CHECK();
+}
+
+void fill_row_segments(const uint64_t* seg_off, uint32_t n_seg, uint32_t* row_seg, cudaStream_t s) {
+  if (n_seg == 0) return;
+  row_segment_kernel<<<n_seg, 256, 0, s>>>(seg_off, n_seg, row_seg);
   UB_LAUNCH_CHECK();
 }
 

@@ -164,7 +164,7 @@ __device__ __forceinline__ void sub_row(float* p, const float (&g)[DIM]) {
 template <int DIM>
 __device__ __forceinline__ void fired_edge(float (&cur)[DIM], uint32_t r, uint32_t k, uint32_t nneg,
                                            float* snap, const SgdParams& p, float alpha, uint64_t idx,
-                                           uint32_t epoch, uint2 key) {
+                                           uint32_t epoch, uint2 key, uint32_t seg_lo, uint32_t seg_n) {
   const float a = p.a, b = p.b;
   float* oth = snap + (uint64_t)k * DIM;
   float o[DIM];
@@ -185,7 +185,7 @@ __device__ __forceinline__ void fired_edge(float (&cur)[DIM], uint32_t r, uint32
         }
         const uint32_t w = qq & 3;
         const uint32_t rv = w == 0 ? rnd.x : w == 1 ? rnd.y : w == 2 ? rnd.z : rnd.w;
-        kk[q] = __umulhi(rv, p.n_vertices);
+        kk[q] = seg_lo + __umulhi(rv, seg_n);
         load_row<DIM>(ob[q], snap + (uint64_t)kk[q] * DIM);
       }
     }
@@ -244,6 +244,12 @@ __global__ void __launch_bounds__(256, UB_SGD_MIN_BLOCKS) sgd_epoch_kernel(
   const uint64_t base = slice_base[slice];
   const bool split = (split_mask[slice] >> lane) & 1u;
   const bool active = r != PAD_ROW;
+  uint32_t seg_lo = 0, seg_n = p.n_vertices;
+  if (p.row_seg && active) {
+    const uint32_t sg = p.row_seg[r];
+    seg_lo = (uint32_t)p.seg_off[sg];
+    seg_n = (uint32_t)(p.seg_off[sg + 1] - p.seg_off[sg]);
+  }
   float cur[DIM], start[DIM];
   float* hrow = live + (uint64_t)(active ? r : 0) * DIM;
   if (active) load_row<DIM>(cur, hrow);
@@ -273,7 +279,7 @@ __global__ void __launch_bounds__(256, UB_SGD_MIN_BLOCKS) sgd_epoch_kernel(
         if (t == j) en = ent[t];
       const uint32_t nneg = negatives_at(n, fires_by(n, en.y), en.y, p.neg_rate);
       const uint64_t idx = base + (uint64_t)(e0 + j) * 32 + lane;
-      fired_edge<DIM>(cur, r, en.x, nneg, snap, p, alpha, idx, epoch, key);
+      fired_edge<DIM>(cur, r, en.x, nneg, snap, p, alpha, idx, epoch, key, seg_lo, seg_n);
     }
   }
   if (active) {
@@ -307,6 +313,12 @@ __global__ void __launch_bounds__(256, UB_SGD_MIN_BLOCKS) sgd_epoch_kernel2(
   const uint32_t width = active ? slice_width[slice] : 0u;
   const uint64_t base = slice_base[slice];
   const bool split = (split_mask[slice] >> lane) & 1u;
+  uint32_t seg_lo = 0, seg_n = p.n_vertices;
+  if (p.row_seg && active) {
+    const uint32_t sg = p.row_seg[r];
+    seg_lo = (uint32_t)p.seg_off[sg];
+    seg_n = (uint32_t)(p.seg_off[sg + 1] - p.seg_off[sg]);
+  }
   float cur[DIM], start[DIM];
   float* hrow = live + (uint64_t)(active ? r : 0) * DIM;
   if (active) load_row<DIM>(cur, hrow);
@@ -342,7 +354,7 @@ __global__ void __launch_bounds__(256, UB_SGD_MIN_BLOCKS) sgd_epoch_kernel2(
         if (t == j) en = win[t];
       const uint32_t nneg = negatives_at(n, fires_by(n, en.y), en.y, p.neg_rate);
       const uint64_t idx = base + (uint64_t)(ebase + j) * 32 + lane;
-      fired_edge<DIM>(cur, r, en.x, nneg, snap, p, alpha, idx, epoch, key);
+      fired_edge<DIM>(cur, r, en.x, nneg, snap, p, alpha, idx, epoch, key, seg_lo, seg_n);
     }
   }
   if (active) {
@@ -371,6 +383,12 @@ __global__ void __launch_bounds__(256) sgd_epoch_generic(
   const uint32_t width = slice_width[slice];
   const uint64_t base = slice_base[slice];
   const bool split = (split_mask[slice] >> lane) & 1u;
+  uint32_t seg_lo = 0, seg_n = p.n_vertices;
+  if (p.row_seg) {
+    const uint32_t sg = p.row_seg[r];
+    seg_lo = (uint32_t)p.seg_off[sg];
+    seg_n = (uint32_t)(p.seg_off[sg + 1] - p.seg_off[sg]);
+  }
   const uint32_t dim = p.dim;
   float* cur = live + (uint64_t)r * dim;
   const uint32_t n = epoch;
@@ -404,7 +422,7 @@ __global__ void __launch_bounds__(256) sgd_epoch_generic(
       if ((q & 3) == 0)
         rnd = philox4x32_10(make_uint4((uint32_t)idx, (uint32_t)(idx >> 32), epoch, q >> 2), key);
       const uint32_t rv = (q & 3) == 0 ? rnd.x : (q & 3) == 1 ? rnd.y : (q & 3) == 2 ? rnd.z : rnd.w;
-      const uint32_t kk = __umulhi(rv, p.n_vertices);
+      const uint32_t kk = seg_lo + __umulhi(rv, seg_n);
       if (kk == r) continue;
       const float* ob = snap + (uint64_t)kk * dim;
       float dsn = 0.0f;
@@ -422,12 +440,31 @@ __global__ void __launch_bounds__(256) sgd_epoch_generic(
 
 // ------------------------------------------------------------------------------ K5 pieces
 __global__ void kept_degree_kernel(const uint64_t* __restrict__ indptr, const float* __restrict__ data,
-                                   uint64_t n, float thr, uint32_t* __restrict__ deg) {
+                                   uint64_t n, float thr, const float* __restrict__ seg_thr,
+                                   const uint32_t* __restrict__ row_seg, uint32_t* __restrict__ deg) {
   const uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= n) return;
+  const float t = seg_thr ? seg_thr[row_seg[r]] : thr;
   uint32_t c = 0;
-  for (uint64_t q = indptr[r]; q < indptr[r + 1]; ++q) c += data[q] >= thr ? 1u : 0u;
+  for (uint64_t q = indptr[r]; q < indptr[r + 1]; ++q) c += data[q] >= t ? 1u : 0u;
   deg[r] = c;
+}
+
+// Batched instances: max graph weight of each instance (optimizer.rs:90-94 per instance).
+__global__ void segment_max_kernel(const uint64_t* __restrict__ indptr, const float* __restrict__ data,
+                                   const uint64_t* __restrict__ seg_off, float* __restrict__ out) {
+  const uint32_t sgm = blockIdx.x;
+  const uint64_t q0 = indptr[seg_off[sgm]], q1 = indptr[seg_off[sgm + 1]];
+  float m = 0.0f;
+  for (uint64_t q = q0 + threadIdx.x; q < q1; q += blockDim.x) m = fmaxf(m, data[q]);
+  __shared__ float s_m[32];
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xFFFFFFFFu, m, o));
+  if ((threadIdx.x & 31) == 0) s_m[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (uint32_t w = 1; w < blockDim.x / 32; ++w) m = fmaxf(m, s_m[w]);
+    out[sgm] = m;
+  }
 }
 
 __global__ void ptr_degree_kernel(const uint64_t* __restrict__ kptr, uint64_t n, uint32_t chunk,
@@ -442,6 +479,7 @@ __global__ void ptr_degree_kernel(const uint64_t* __restrict__ kptr, uint64_t n,
 // One task per chunk of a row: row id, first kept-edge index, length, split flag.
 __global__ void task_fill_kernel(const uint64_t* __restrict__ kptr, const uint32_t* __restrict__ deg,
                                  const uint64_t* __restrict__ tptr, uint64_t n, uint32_t chunk,
+                                 const uint32_t* __restrict__ row_seg, int len_bits,
                                  uint32_t* __restrict__ trow, uint64_t* __restrict__ tstart,
                                  uint32_t* __restrict__ tkey) {
   const uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -452,21 +490,25 @@ __global__ void task_fill_kernel(const uint64_t* __restrict__ kptr, const uint32
     const uint32_t len = (uint32_t)min((uint64_t)chunk, (uint64_t)d - c * chunk);
     trow[t0 + c] = (uint32_t)r | (nt > 1 ? 0x80000000u : 0u);   // high bit: partial row
     tstart[t0 + c] = kptr[r] + c * chunk;
-    tkey[t0 + c] = chunk - len;  // ascending key = descending length
+    // ascending key = descending length; batched instances sort instance-major first
+    tkey[t0 + c] = (row_seg ? (row_seg[r] << len_bits) : 0u) | (chunk - len);
   }
 }
 
 __global__ void slice_meta_kernel(const uint32_t* __restrict__ perm, const uint32_t* __restrict__ trow,
                                   const uint32_t* __restrict__ skey, uint64_t T, uint64_t n_slices,
-                                  uint32_t chunk, uint32_t* __restrict__ width, uint32_t* __restrict__ rowid,
-                                  uint32_t* __restrict__ split_mask) {
+                                  uint32_t chunk, uint32_t len_mask, uint32_t* __restrict__ width,
+                                  uint32_t* __restrict__ rowid, uint32_t* __restrict__ split_mask) {
   const uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= n_slices * 32) return;
   const uint32_t tr = q < T ? trow[perm[q]] : PAD_ROW;
   rowid[q] = tr == PAD_ROW ? PAD_ROW : (tr & 0x7FFFFFFFu);
   const unsigned bits = __ballot_sync(0xFFFFFFFFu, tr != PAD_ROW && (tr & 0x80000000u));
+  // slice width = longest task of the slice (instance-major order: the max over lanes)
+  uint32_t len = q < T ? chunk - (skey[q] & len_mask) : 0u;
+  for (int o = 16; o > 0; o >>= 1) len = max(len, __shfl_xor_sync(0xFFFFFFFFu, len, o));
   if ((q & 31) == 0) {
-    width[q >> 5] = q < T ? chunk - skey[q] : 0u;
+    width[q >> 5] = len;
     split_mask[q >> 5] = bits;
   }
 }
@@ -474,8 +516,9 @@ __global__ void slice_meta_kernel(const uint32_t* __restrict__ perm, const uint3
 __global__ void slice_fill_kernel(const uint32_t* __restrict__ ktail, const double* __restrict__ keps,
                                   const uint32_t* __restrict__ perm, const uint64_t* __restrict__ tstart,
                                   const uint32_t* __restrict__ skey, uint64_t T, uint32_t chunk,
-                                  const uint64_t* __restrict__ wscan, const uint32_t* __restrict__ width,
-                                  uint64_t n_slices, uint2* __restrict__ entry) {
+                                  uint32_t len_mask, const uint64_t* __restrict__ wscan,
+                                  const uint32_t* __restrict__ width, uint64_t n_slices,
+                                  uint2* __restrict__ entry) {
   const uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= n_slices * 32) return;
   const uint64_t s = q >> 5;
@@ -485,7 +528,7 @@ __global__ void slice_fill_kernel(const uint32_t* __restrict__ ktail, const doub
   uint32_t e = 0;
   if (q < T) {
     const uint64_t st = tstart[perm[q]];
-    const uint32_t len = chunk - skey[q];
+    const uint32_t len = chunk - (skey[q] & len_mask);
     for (; e < len; ++e)
       entry[base + (uint64_t)e * 32 + lane] = make_uint2(ktail[st + e], q_minus_1(keps[st + e]));
   }
@@ -524,18 +567,26 @@ __device__ __forceinline__ double epochs_per_sample(float w, double max_w, doubl
 
 __global__ void export_edges_kernel(const uint64_t* __restrict__ indptr, const uint32_t* __restrict__ indices,
                                     const float* __restrict__ data, uint64_t n, float thr, double max_w,
-                                    double n_ep, const uint64_t* __restrict__ kept_ptr,
-                                    uint32_t* __restrict__ head, uint32_t* __restrict__ tail,
-                                    double* __restrict__ eps) {
+                                    double n_ep, const float* __restrict__ seg_thr,
+                                    const float* __restrict__ seg_maxw, const uint32_t* __restrict__ row_seg,
+                                    const uint64_t* __restrict__ kept_ptr, uint32_t* __restrict__ head,
+                                    uint32_t* __restrict__ tail, double* __restrict__ eps) {
   const uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= n) return;
+  float t = thr;
+  double mw = max_w;
+  if (seg_thr) {
+    const uint32_t sg = row_seg[r];
+    t = seg_thr[sg];
+    mw = (double)seg_maxw[sg];
+  }
   uint64_t o = kept_ptr[r];
   for (uint64_t j = indptr[r]; j < indptr[r + 1]; ++j) {
     const float w = data[j];
-    if (w >= thr) {
+    if (w >= t) {
       if (head) head[o] = (uint32_t)r;
       if (tail) tail[o] = indices[j];
-      if (eps) eps[o] = epochs_per_sample(w, max_w, n_ep);
+      if (eps) eps[o] = epochs_per_sample(w, mw, n_ep);
       ++o;
     }
   }
@@ -544,11 +595,13 @@ __global__ void export_edges_kernel(const uint64_t* __restrict__ indptr, const u
 // ------------------------------------------------------------------------------ K6
 // optimizer.rs:189-230.  f32::min / f32::max ignore NaN like fminf / fmaxf.
 __global__ void minmax_dim_kernel(const float* __restrict__ emb, uint64_t n, uint32_t dim,
-                                  float* __restrict__ mins, float* __restrict__ maxs) {
-  // one block per dimension
-  const uint32_t d = blockIdx.x;
+                                  const uint64_t* __restrict__ seg_off, float* __restrict__ mins,
+                                  float* __restrict__ scales) {
+  // one block per (dimension, instance)
+  const uint32_t d = blockIdx.x, sg = blockIdx.y;
+  const uint64_t r0 = seg_off ? seg_off[sg] : 0, r1 = seg_off ? seg_off[sg + 1] : n;
   float mn = INFINITY, mx = -INFINITY;
-  for (uint64_t i = threadIdx.x; i < n; i += blockDim.x) {
+  for (uint64_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
     const float v = emb[i * dim + d];
     mn = fminf(mn, v);
     mx = fmaxf(mx, v);
@@ -563,18 +616,21 @@ __global__ void minmax_dim_kernel(const float* __restrict__ emb, uint64_t n, uin
   if (threadIdx.x == 0) {
     for (uint32_t w = 1; w < blockDim.x / 32; ++w) { mn = fminf(mn, s_mn[w]); mx = fmaxf(mx, s_mx[w]); }
     const float range = __fsub_rn(mx, mn);
-    mins[d] = mn;
-    maxs[d] = range > 0.0f ? __fdiv_rn(10.0f, range) : 0.0f;  // scale
+    mins[sg * dim + d] = mn;
+    scales[sg * dim + d] = range > 0.0f ? __fdiv_rn(10.0f, range) : 0.0f;
   }
 }
 
 __global__ void normalize_kernel(float* __restrict__ emb, uint64_t total, uint32_t dim,
-                                 const float* __restrict__ mins, const float* __restrict__ scales) {
+                                 const float* __restrict__ mins, const float* __restrict__ scales,
+                                 const uint32_t* __restrict__ row_seg) {
   const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= total) return;
-  const uint32_t d = (uint32_t)(i % dim);
-  const float sc = scales[d];
-  if (sc > 0.0f) emb[i] = __fmul_rn(__fsub_rn(emb[i], mins[d]), sc);
+  const uint64_t r = i / dim;
+  const uint32_t d = (uint32_t)(i - r * dim);
+  const uint64_t c = (uint64_t)(row_seg ? row_seg[r] : 0) * dim + d;
+  const float sc = scales[c];
+  if (sc > 0.0f) emb[i] = __fmul_rn(__fsub_rn(emb[i], mins[c]), sc);
 }
 
 // ------------------------------------------------------------------------------ accounting
@@ -618,16 +674,24 @@ inline unsigned grid_for(uint64_t n, unsigned bt) { return (unsigned)((n + bt - 
 }  // namespace
 
 void kept_degree(const uint64_t* indptr, const float* data, uint64_t n, float thr, uint32_t* deg,
-                 cudaStream_t s) {
+                 cudaStream_t s, const SegmentPrune* sp) {
   if (n == 0) return;
-  kept_degree_kernel<<<grid_for(n, 256), 256, 0, s>>>(indptr, data, n, thr, deg);
+  kept_degree_kernel<<<grid_for(n, 256), 256, 0, s>>>(indptr, data, n, thr, sp ? sp->seg_thr : nullptr,
+                                                      sp ? sp->row_seg : nullptr, deg);
+  UB_LAUNCH_CHECK();
+}
+
+void segment_max(const uint64_t* indptr, const float* data, const uint64_t* seg_off, uint32_t n_seg,
+                 float* out, cudaStream_t s) {
+  if (n_seg == 0) return;
+  segment_max_kernel<<<n_seg, 256, 0, s>>>(indptr, data, seg_off, out);
   UB_LAUNCH_CHECK();
 }
 
 void prune_edges(const uint64_t* indptr, const float* data, uint64_t n, float thr, uint64_t* kept_ptr,
-                 uint64_t* n_edges, cudaStream_t s) {
+                 uint64_t* n_edges, cudaStream_t s, const SegmentPrune* sp) {
   DevBuf<uint32_t> deg(n, s);
-  kept_degree(indptr, data, n, thr, deg.p, s);
+  kept_degree(indptr, data, n, thr, deg.p, s, sp);
   scan_u32_to_u64(deg.p, kept_ptr, n, s);
   UB_CUDA(cudaMemcpyAsync(n_edges, kept_ptr + n, 8, cudaMemcpyDeviceToHost, s));
   UB_CUDA(cudaStreamSynchronize(s));
@@ -659,7 +723,7 @@ uint32_t pick_chunk(uint64_t n_edges) {
 }
 
 void build_sgd_layout(const uint64_t* kept_ptr, const uint32_t* ktail, const double* keps, uint64_t n,
-                      uint32_t chunk, SgdLayout& L, cudaStream_t s) {
+                      uint32_t chunk, SgdLayout& L, cudaStream_t s, const Segments* seg) {
   L.n_vertices = n;
   uint64_t n_edges = 0;
   UB_CUDA(cudaMemcpyAsync(&n_edges, kept_ptr + n, 8, cudaMemcpyDeviceToHost, s));
@@ -683,12 +747,17 @@ void build_sgd_layout(const uint64_t* kept_ptr, const uint32_t* ktail, const dou
   L.n_tasks = T;
   DevBuf<uint32_t> trow(T, s), tkey(T, s), skey(T, s), perm(T, s);
   DevBuf<uint64_t> tstart(T, s);
+  const int len_bits = bits_for(L.chunk);
+  const uint32_t len_mask = (1u << len_bits) - 1u;
+  const uint32_t n_seg = seg ? seg->n_seg : 0u;
+  if ((uint64_t)n_seg << len_bits >= (1ull << 32)) throw Error(UNSUPPORTED, "too many instances for the task sort key");
   if (n) {
-    task_fill_kernel<<<grid_for(n, 256), 256, 0, s>>>(kept_ptr, deg.p, tptr.p, n, L.chunk, trow.p, tstart.p,
-                                                      tkey.p);
+    task_fill_kernel<<<grid_for(n, 256), 256, 0, s>>>(kept_ptr, deg.p, tptr.p, n, L.chunk,
+                                                      seg ? seg->row_seg : nullptr, len_bits, trow.p,
+                                                      tstart.p, tkey.p);
     UB_LAUNCH_CHECK();
   }
-  if (T) radix_sort_pairs(tkey.p, nullptr, skey.p, perm.p, T, bits_for(L.chunk), s);
+  if (T) radix_sort_pairs(tkey.p, nullptr, skey.p, perm.p, T, len_bits + (n_seg ? bits_for(n_seg) : 0), s);
   L.n_slices = (T + 31) / 32;
   L.slice_width.alloc(L.n_slices, s);
   L.split_mask.alloc(L.n_slices, s);
@@ -696,8 +765,8 @@ void build_sgd_layout(const uint64_t* kept_ptr, const uint32_t* ktail, const dou
   L.slice_base.alloc(L.n_slices + 1, s);
   if (L.n_slices) {
     slice_meta_kernel<<<grid_for(L.n_slices * 32, 256), 256, 0, s>>>(perm.p, trow.p, skey.p, T, L.n_slices,
-                                                                        L.chunk, L.slice_width.p, L.rowid.p,
-                                                                        L.split_mask.p);
+                                                                        L.chunk, len_mask, L.slice_width.p,
+                                                                        L.rowid.p, L.split_mask.p);
     UB_LAUNCH_CHECK();
   }
   DevBuf<uint64_t> wscan(L.n_slices + 1, s);
@@ -709,8 +778,8 @@ void build_sgd_layout(const uint64_t* kept_ptr, const uint32_t* ktail, const dou
   L.entry.alloc(L.n_entries, s);
   if (L.n_slices) {
     slice_fill_kernel<<<grid_for(L.n_slices * 32, 256), 256, 0, s>>>(ktail, keps, perm.p, tstart.p, skey.p, T,
-                                                                        L.chunk, wscan.p, L.slice_width.p,
-                                                                        L.n_slices, L.entry.p);
+                                                                        L.chunk, len_mask, wscan.p,
+                                                                        L.slice_width.p, L.n_slices, L.entry.p);
     UB_LAUNCH_CHECK();
   }
   // slice_base = 32 * wscan (entries, not widths)
@@ -727,26 +796,30 @@ void build_sgd_layout(const uint64_t* kept_ptr, const uint32_t* ktail, const dou
 
 void export_edges(const uint64_t* indptr, const uint32_t* indices, const float* data, uint64_t n,
                   float thr, float max_w, uint64_t total_epochs, const uint64_t* kept_ptr,
-                  uint32_t* head, uint32_t* tail, double* eps, cudaStream_t s) {
+                  uint32_t* head, uint32_t* tail, double* eps, cudaStream_t s, const SegmentPrune* sp) {
   if (n == 0) return;
-  export_edges_kernel<<<grid_for(n, 256), 256, 0, s>>>(indptr, indices, data, n, thr, (double)max_w,
-                                                       (double)total_epochs, kept_ptr, head, tail, eps);
+  export_edges_kernel<<<grid_for(n, 256), 256, 0, s>>>(
+      indptr, indices, data, n, thr, (double)max_w, (double)total_epochs, sp ? sp->seg_thr : nullptr,
+      sp ? sp->seg_maxw : nullptr, sp ? sp->row_seg : nullptr, kept_ptr, head, tail, eps);
   UB_LAUNCH_CHECK();
 }
 
-void normalize_init(float* emb, uint64_t n, uint32_t dim, cudaStream_t s) {
+void normalize_init(float* emb, uint64_t n, uint32_t dim, cudaStream_t s, const Segments* seg) {
   if (n == 0 || dim == 0) return;
-  DevBuf<float> mins(dim, s), scales(dim, s);
-  minmax_dim_kernel<<<dim, 1024, 0, s>>>(emb, n, dim, mins.p, scales.p);
+  const uint32_t n_seg = seg ? seg->n_seg : 1u;
+  DevBuf<float> mins((uint64_t)dim * n_seg, s), scales((uint64_t)dim * n_seg, s);
+  minmax_dim_kernel<<<dim3(dim, n_seg), 1024, 0, s>>>(emb, n, dim, seg ? seg->seg_off : nullptr, mins.p, scales.p);
   UB_LAUNCH_CHECK();
-  normalize_kernel<<<grid_for(n * dim, 256), 256, 0, s>>>(emb, n * dim, dim, mins.p, scales.p);
+  normalize_kernel<<<grid_for(n * dim, 256), 256, 0, s>>>(emb, n * dim, dim, mins.p, scales.p,
+                                                          seg ? seg->row_seg : nullptr);
   UB_LAUNCH_CHECK();
 }
 
 void sgd_epoch(const SgdLayout& L, float* live, float* snap, const SgdParams& p, uint32_t epoch, float alpha,
                cudaStream_t s) {
   if (L.n_slices == 0) return;
-  const unsigned grid = grid_for(L.n_slices * 32, 256);
+  const unsigned bt = L.block_threads ? L.block_threads : 256;
+  const unsigned grid = grid_for(L.n_slices * 32, bt);
 #define UB_SGD_ARGS L.slice_base.p, L.slice_width.p, L.split_mask.p, L.rowid.p, L.entry.p, L.n_slices, live, snap, \
                     p, epoch, alpha
 #if UB_SGD_KERNEL == 2
@@ -755,11 +828,11 @@ void sgd_epoch(const SgdLayout& L, float* live, float* snap, const SgdParams& p,
 #define UB_SGD_K sgd_epoch_kernel
 #endif
   switch (p.dim) {
-    case 1: UB_SGD_K<1><<<grid, 256, 0, s>>>(UB_SGD_ARGS); break;
-    case 2: UB_SGD_K<2><<<grid, 256, 0, s>>>(UB_SGD_ARGS); break;
-    case 3: UB_SGD_K<3><<<grid, 256, 0, s>>>(UB_SGD_ARGS); break;
-    case 4: UB_SGD_K<4><<<grid, 256, 0, s>>>(UB_SGD_ARGS); break;
-    default: sgd_epoch_generic<<<grid, 256, 0, s>>>(UB_SGD_ARGS); break;
+    case 1: UB_SGD_K<1><<<grid, bt, 0, s>>>(UB_SGD_ARGS); break;
+    case 2: UB_SGD_K<2><<<grid, bt, 0, s>>>(UB_SGD_ARGS); break;
+    case 3: UB_SGD_K<3><<<grid, bt, 0, s>>>(UB_SGD_ARGS); break;
+    case 4: UB_SGD_K<4><<<grid, bt, 0, s>>>(UB_SGD_ARGS); break;
+    default: sgd_epoch_generic<<<grid, bt, 0, s>>>(UB_SGD_ARGS); break;
   }
 #undef UB_SGD_ARGS
 #undef UB_SGD_K

@@ -123,10 +123,21 @@ struct GraphParams {
   int n_iter;           // 64
 };
 
-// K1: per-row rho and sigma (smooth_knn_dist.rs:60-198).  Uses a device scratch flag and
-// global-mean fixup for rows whose rho is not positive.
+// Batched instances: rows [seg_off[s], seg_off[s+1]) belong to instance s (device arrays).
+struct Segments {
+  uint32_t n_seg = 0;
+  const uint64_t* seg_off = nullptr;  // [n_seg + 1] row offsets
+  const uint32_t* row_seg = nullptr;  // [n_rows] instance of each row
+};
+
+// K1: per-row rho and sigma (smooth_knn_dist.rs:60-198).  Rows whose rho is not positive
+// fall back on the mean of all distances of their instance (seg == nullptr: one instance).
 void smooth_knn(const float* dist, uint64_t n, uint64_t k, const GraphParams& gp,
-                float* sigmas, float* rhos, cudaStream_t s);
+                float* sigmas, float* rhos, cudaStream_t s, const Segments* seg = nullptr);
+// Batched instances: local kNN ids -> global ids (out-of-instance ids -> 0xFFFFFFFF).
+void localize_knn(const uint32_t* idx, uint64_t n, uint64_t k, const Segments& seg, uint32_t* out,
+                  cudaStream_t s);
+void fill_row_segments(const uint64_t* seg_off, uint32_t n_seg, uint32_t* row_seg, cudaStream_t s);
 // K2: directed membership entries per row, kept ones sorted by column (stable) into the
 // padded [n][k] arrays pcol/pw; cnt[r] = kept count.  edges_removed (device u64) counts
 // dist >= disc_thr entries.
@@ -164,6 +175,7 @@ void count_empty_rows(const uint64_t* indptr, const float* data, uint64_t n,
 struct SgdLayout {
   uint64_t n_vertices = 0, n_edges = 0, n_entries = 0, n_slices = 0, n_tasks = 0;
   uint32_t max_degree = 0, chunk = 0;
+  uint32_t block_threads = 256;  // threads per block of the epoch kernel (multiple of 32)
   uint64_t split_tasks = 0;
   DevBuf<uint64_t> slice_base;   // [n_slices + 1]
   DevBuf<uint32_t> slice_width;  // [n_slices]
@@ -178,20 +190,35 @@ struct SgdParams {
   float pos_rep;    // (2 gamma) b
   uint32_t neg_rate;  // negative_sample_rate
   uint32_t n_vertices;
+  // Batched instances (null for a plain fit): negatives of a row of instance s are drawn
+  // from [seg_off[s], seg_off[s+1]).
+  const uint32_t* row_seg;
+  const uint64_t* seg_off;
   uint32_t dim;
   uint64_t seed;
+};
+
+// Batched instances: per-instance prune threshold and max kept weight (device arrays).
+struct SegmentPrune {
+  const float* seg_thr = nullptr;
+  const float* seg_maxw = nullptr;
+  const uint32_t* row_seg = nullptr;
 };
 
 // Prune (optimizer.rs:85-167): keep w >= thr.  kept_ptr[n+1] = row pointers of the kept
 // edges in the reference's row-major order; *n_edges = kept count (host, synchronises).
 void prune_edges(const uint64_t* indptr, const float* data, uint64_t n, float thr,
-                 uint64_t* kept_ptr, uint64_t* n_edges, cudaStream_t s);
+                 uint64_t* kept_ptr, uint64_t* n_edges, cudaStream_t s,
+                 const SegmentPrune* sp = nullptr);
+// Batched instances: max weight per instance.
+void segment_max(const uint64_t* indptr, const float* data, const uint64_t* seg_off, uint32_t n_seg,
+                 float* out, cudaStream_t s);
 // Kept edges in the reference order: head/tail u32 and epochs_per_sample f64
 // (make_epochs_per_sample.rs:21-52 with max weight max_w).  Any output may be null.
 void export_edges(const uint64_t* indptr, const uint32_t* indices, const float* data,
                   uint64_t n, float thr, float max_w, uint64_t total_epochs,
                   const uint64_t* kept_ptr, uint32_t* head, uint32_t* tail, double* eps,
-                  cudaStream_t s);
+                  cudaStream_t s, const SegmentPrune* sp = nullptr);
 void head_from_ptr(const uint64_t* kept_ptr, uint64_t n, uint32_t* head, cudaStream_t s);
 // Schedule state at cur_epoch in the reference's representation (optimizer.rs:41-43).
 void export_state(const double* eps, uint64_t E, uint64_t neg_rate, uint64_t cur_epoch,
@@ -199,11 +226,13 @@ void export_state(const double* eps, uint64_t E, uint64_t neg_rate, uint64_t cur
 // Slice layout from kept edges (kept_ptr, tail, eps).  chunk = 0 picks the task length
 // from the edge count.
 void build_sgd_layout(const uint64_t* kept_ptr, const uint32_t* tail, const double* eps,
-                      uint64_t n, uint32_t chunk, SgdLayout& L, cudaStream_t s);
+                      uint64_t n, uint32_t chunk, SgdLayout& L, cudaStream_t s,
+                      const Segments* seg = nullptr);
 void kept_degree(const uint64_t* indptr, const float* data, uint64_t n, float thr,
-                 uint32_t* deg, cudaStream_t s);
+                 uint32_t* deg, cudaStream_t s, const SegmentPrune* sp = nullptr);
 // K6 normalise init into [0, 10] per dimension (optimizer.rs:181-230), in place.
-void normalize_init(float* emb, uint64_t n, uint32_t dim, cudaStream_t s);
+void normalize_init(float* emb, uint64_t n, uint32_t dim, cudaStream_t s,
+                    const Segments* seg = nullptr);
 // K7 one Hogwild epoch.
 void sgd_epoch(const SgdLayout& L, float* live, float* snap, const SgdParams& p,
                uint32_t epoch, float alpha, cudaStream_t s);

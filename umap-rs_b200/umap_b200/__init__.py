@@ -158,6 +158,34 @@ def kernel_launches() -> int:
     return v.value
 
 
+def batch_fit(config: UmapConfig, offsets, knn_indices, knn_dists, init):
+    """Umap::fit for many independent instances at once (no counterpart in the reference).
+    Returns f32[total points, n_components] (host) or writes into a CUDA tensor when the
+    inputs are CUDA tensors (returned)."""
+    L = _lib.load()
+    off = np.ascontiguousarray(offsets, dtype=np.uint64)
+    n_inst = len(off) - 1
+    cfg = config.to_c()
+    k = int(knn_dists.shape[1])
+    d = int(init.shape[1])
+    if _is_cuda_tensor(knn_dists):
+        import torch
+        ti, pi = _device(knn_indices, torch.int32)
+        td, pd = _device(knn_dists, torch.float32)
+        tn, pn = _device(init, torch.float32)
+        out = torch.empty((int(off[-1]), d), dtype=torch.float32, device=knn_dists.device)
+        _check(L.umap_batch_fit_device(C.byref(cfg), n_inst, off.ctypes.data_as(C.c_void_p), pi, pd, k, pn, d,
+                                       C.c_void_p(out.data_ptr())))
+        return out
+    ai, pi = _host(knn_indices, np.uint32)
+    ad, pd = _host(knn_dists, np.float32)
+    an, pn = _host(init, np.float32)
+    out = np.empty((int(off[-1]), d), np.float32)
+    _check(L.umap_batch_fit(C.byref(cfg), n_inst, off.ctypes.data_as(C.c_void_p), pi, pd, k, pn, d,
+                            out.ctypes.data_as(C.c_void_p)))
+    return out
+
+
 def release_cached_memory() -> int:
     """Return the library's cached device blocks to the CUDA pool; returns their bytes."""
     v = C.c_uint64()
@@ -481,6 +509,39 @@ class Optimizer(_Handle):
         f, g = C.c_uint64(), C.c_uint64()
         _check(_lib.load().umap_optimizer_schedule_totals(self._get(), start, end, C.byref(f), C.byref(g)))
         return f.value, g.value
+
+    @staticmethod
+    def batch(config: UmapConfig, offsets, knn_indices, knn_dists, init, total_epochs: int) -> "Optimizer":
+        """Batched instances (no counterpart in the reference): instance s owns points
+        [offsets[s], offsets[s+1]) of the concatenated arrays; kNN ids are local to each
+        instance.  Returns one optimizer over all instances (one kernel launch per epoch)."""
+        L = _lib.load()
+        off = np.ascontiguousarray(offsets, dtype=np.uint64)
+        n_inst = len(off) - 1
+        cfg = config.to_c()
+        out = C.c_void_p()
+        k = int(knn_dists.shape[1])
+        d = int(init.shape[1])
+        if _is_cuda_tensor(knn_dists):
+            import torch
+            ti, pi = _device(knn_indices, torch.int32)
+            td, pd = _device(knn_dists, torch.float32)
+            tn, pn = _device(init, torch.float32)
+            _check(L.umap_batch_optimizer_new_device(C.byref(cfg), n_inst, off.ctypes.data_as(C.c_void_p),
+                                                     pi, pd, k, pn, d, total_epochs, C.byref(out)))
+        else:
+            ai, pi = _host(knn_indices, np.uint32)
+            ad, pd = _host(knn_dists, np.float32)
+            an, pn = _host(init, np.float32)
+            _check(L.umap_batch_optimizer_new(C.byref(cfg), n_inst, off.ctypes.data_as(C.c_void_p),
+                                              pi, pd, k, pn, d, total_epochs, C.byref(out)))
+        return Optimizer(None, _handle=out.value)
+
+    def tuning(self):
+        """(task length, threads per block) of the SGD kernel in use."""
+        c, b = C.c_uint32(), C.c_uint32()
+        _check(_lib.load().umap_optimizer_tuning(self._get(), C.byref(c), C.byref(b)))
+        return c.value, b.value
 
     def into_fitted(self, config: UmapConfig | None = None) -> "FittedUmap":
         """optimizer.rs:397-403.  Consumes the optimizer."""

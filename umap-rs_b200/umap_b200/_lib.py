@@ -70,6 +70,11 @@ SIGNATURES = {
     "umap_fitted_free": [P],
     "umap_fit": [C.POINTER(UmapConfigC), u64, P, P, u64, u64, P, u64, u64, PP],
     "umap_fit_device": [C.POINTER(UmapConfigC), u64, P, P, u64, u64, P, u64, u64, PP],
+    "umap_batch_optimizer_new": [C.POINTER(UmapConfigC), u64, P, P, P, u64, P, u64, u64, PP],
+    "umap_batch_optimizer_new_device": [C.POINTER(UmapConfigC), u64, P, P, P, u64, P, u64, u64, PP],
+    "umap_batch_fit": [C.POINTER(UmapConfigC), u64, P, P, P, u64, P, u64, P],
+    "umap_batch_fit_device": [C.POINTER(UmapConfigC), u64, P, P, P, u64, P, u64, P],
+    "umap_optimizer_tuning": [P, C.POINTER(u32), C.POINTER(u32)],
     "umap_manifold_serialize": [P, P, u64, C.POINTER(u64)],
     "umap_manifold_deserialize": [P, u64, PP],
     "umap_optimizer_serialize": [P, P, u64, C.POINTER(u64)],

@@ -264,3 +264,35 @@ def knn_exact_clustered_torch(X: np.ndarray, labels: np.ndarray, k: int, device=
         dst[r] = torch.gather(ex, 1, o2)[:, :k]
     return (idx.to(torch.int32).cpu().numpy().astype(np.uint32), dst.cpu().numpy(),
             int(bad_rows.numel()))
+
+
+def instances_torch(count: int = 4096, k: int = 15, seed: int = 4, device="cuda", lo=500, hi=50_000):
+    """The batched workload on the GPU: `count` datasets with sizes log-uniform in [lo, hi],
+    each D=32, 5 Gaussians (centres ~N(0, 5^2 I), std 1), per-instance seed; exact kNN k
+    (self first, local ids) by brute force per instance; init U[-10, 10]^2.
+    Returns (sizes i64[count], idx i32 CUDA [N, k], dist f32 CUDA [N, k], init f32 CUDA [N, 2])."""
+    import torch
+
+    torch.backends.cuda.matmul.allow_tf32 = False
+    sizes = instance_sizes(count, lo, hi, seed)
+    N = int(sizes.sum())
+    idx = torch.empty((N, k), dtype=torch.int32, device=device)
+    dst = torch.empty((N, k), dtype=torch.float32, device=device)
+    off = 0
+    for i, n in enumerate(sizes.tolist()):
+        g = torch.Generator(device=device).manual_seed(1000 + i)
+        centres = torch.randn((5, 32), generator=g, device=device) * 5.0
+        lab = torch.randint(0, 5, (n,), generator=g, device=device)
+        X0 = centres[lab] + torch.randn((n, 32), generator=g, device=device)
+        Xc = X0 - X0.mean(0, keepdim=True)
+        sq = (Xc * Xc).sum(1)
+        kc = min(n, k + 8)
+        for s in range(0, n, 4096):
+            e = min(n, s + 4096)
+            ci, cd, _ = _torch_knn_block(torch, X0[s:e], Xc[s:e], X0, Xc, sq[s:e], sq, k, kc, s)
+            idx[off + s:off + e] = ci.to(torch.int32)
+            dst[off + s:off + e] = cd
+        off += n
+    g = torch.Generator(device=device).manual_seed(77)
+    init = torch.rand((N, 2), generator=g, device=device) * 20.0 - 10.0
+    return sizes, idx, dst, init

@@ -45,8 +45,12 @@ def parse():
     ap.add_argument("--profile", action="store_true",
                     help="profiling run: build one optimizer, run --profile-epochs epochs, exit")
     ap.add_argument("--profile-epochs", type=int, default=24)
-    ap.add_argument("--workload", default="gaussians_2m", choices=["gaussians_2m", "batched"],
-                    help="batched: 4096 independent instances, 200 epochs, vs a per-instance loop")
+    ap.add_argument("--workload", default="gaussians_2m", choices=["gaussians_2m", "batched", "warm_start"],
+                    help="batched: 4096 independent instances, 200 epochs, vs a per-instance loop; "
+                         "warm_start: learned initial embedding + a shortened fit vs the plain fit")
+    ap.add_argument("--sub", type=int, default=100_000, help="warm_start: subsample size")
+    ap.add_argument("--warm-epochs", type=int, default=100, help="warm_start: epochs of the refining fit")
+    ap.add_argument("--warm-lr", type=float, default=None, help="warm_start: learning rate of the refining fit")
     ap.add_argument("--instances", type=int, default=4096)
     ap.add_argument("--loop-sample", type=int, default=8,
                     help="per-instance loop timed on every n-th instance, scaled by n")
@@ -231,12 +235,119 @@ def run_batched(a):
     print(json.dumps(line), flush=True)
 
 
+def run_warm_start(a):
+    """Learned warm start on the 2M workload: a 100k subsample fitted plainly for 500 epochs
+    gives the targets; the MLP (64->256->256->2, bf16, Adam 1e-3, batch 4096, 20 epochs)
+    predicts every point's initial embedding; a 100-epoch fit refines it.  Compared by wall
+    time and 15-NN recall (fixed 100k-point sample) with the plain 500-epoch fit and with a
+    100-epoch fit from the uniform random init.  kNN of the full set and of the subsample are
+    harness inputs (cached / timed separately), as for the plain workload."""
+    import torch
+    import umap_b200 as ub
+    from umap_b200 import quality, workloads as W
+    torch.cuda.set_device(0)
+    n = a.n
+    X, lab = W.gaussians_2m() if n == 2_000_000 else W.gaussian_mixture(n, 64, 50, 8.0, seed=1, anisotropic=True,
+                                                                         dirichlet=True)
+    idx, dist, _ = W.knn_exact_clustered_torch(X, lab, 15)
+    init = W.uniform_init(n)
+    n_sub = min(a.sub, n)
+    sub = np.sort(np.random.Generator(np.random.PCG64(3)).choice(n, n_sub, replace=False))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    sidx, sdist, _ = W.knn_exact_clustered_torch(X[sub], lab[sub], 15)
+    torch.cuda.synchronize()
+    sub_knn_ms = (time.perf_counter() - t0) * 1e3
+    x = torch.from_numpy(X).cuda()
+    d_idx, d_dist = torch.from_numpy(idx.view(np.int32)).cuda(), torch.from_numpy(dist).cuda()
+    d_init = torch.from_numpy(init).cuda()
+    d_sub = torch.from_numpy(sub.astype(np.int64)).cuda()
+    d_sidx, d_sdist = torch.from_numpy(sidx.view(np.int32)).cuda(), torch.from_numpy(sdist).cuda()
+
+    def cfg_epochs(e, lr=None):
+        c = ub.UmapConfig()
+        c.optimization.n_epochs = e
+        if lr is not None:
+            c.optimization.learning_rate = lr
+        return c
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        r = fn()
+        torch.cuda.synchronize()
+        return r, (time.perf_counter() - t) * 1e3
+
+    plain = lambda: ub.Umap(cfg_epochs(a.epochs)).fit(x, d_idx, d_dist, d_init)  # noqa: E731
+    short = lambda: ub.Umap(cfg_epochs(a.warm_epochs)).fit(x, d_idx, d_dist, d_init)  # noqa: E731
+    infos = []
+
+    def warm():
+        info = {}
+        f = ub.warm_start_fit(ub.UmapConfig(), x, d_idx, d_dist, d_sub, d_sidx, d_sdist, sub_epochs=a.epochs,
+                              epochs=a.warm_epochs, mlp_epochs=20, batch=4096, mlp_lr=1e-3,
+                              learning_rate=a.warm_lr, seed=0, info=info)
+        infos.append(info)
+        return f
+
+    res, embs = {}, {}
+    launches0 = ub.kernel_launches()
+    with Clocks(0) as clk:
+        for name, fn in (("plain", plain), ("warm", warm), ("random_short", short)):
+            ms = []
+            for it in range(max(1, a.warmup) + a.steps):
+                f, t = timed(fn)
+                if it >= max(1, a.warmup):
+                    ms.append(t)
+            embs[name] = f.embedding()
+            if name == "plain":
+                ab = f.manifold().curve_params()
+                edges = quality.pruned_edges(f.manifold(), a.epochs)
+            res[name] = {"ms": float(np.median(ms))}
+            del f
+    launches = ub.kernel_launches() - launches0
+    for name, emb in embs.items():
+        res[name]["recall"] = quality.knn_recall(emb, idx, sample=100_000, seed=0)
+        res[name]["ce"] = quality.fuzzy_cross_entropy_torch(emb, *edges, *ab)
+    info = infos[-1]
+    steps_per_epoch = n_sub // 4096
+    flop_step = 2 * 4096 * (64 * 256 + 256 * 256 + 256 * 2) * 3 - 2 * 4096 * 64 * 256  # fwd + bwd (no dX)
+    train_ms = info["ms"]["mlp_train"]
+    train_tflops = flop_step * 20 * steps_per_epoch / (train_ms / 1e3) / 1e12
+    pred_tflops = 2 * n * (64 * 256 + 256 * 256 + 256 * 2) / (info["ms"]["mlp_predict"] / 1e3) / 1e12
+    pk = peaks()
+    tc = pk.get("bf16_tflops")
+    line = {"metric": "warm-start fit wall time at equal 15-NN recall", "value": res["warm"]["ms"], "unit": "ms",
+            "higher_is_better": False, "n_gpus": 1, "steps": a.steps, "warmup": a.warmup, "dtype": "bf16+f32",
+            "data": "synthetic",
+            "config": {"workload": f"gaussians_{n}_d64_k15: sub {n_sub} x {a.epochs}ep -> mlp 64-256-256-2 "
+                                   f"x20ep b4096 -> {a.warm_epochs}ep",
+                       "warm_learning_rate": a.warm_lr if a.warm_lr is not None else 1.0,
+                       "subsample_knn_ms_harness": round(sub_knn_ms, 1)},
+            "plain_ms": res["plain"]["ms"], "plain_recall": res["plain"]["recall"], "plain_ce": res["plain"]["ce"],
+            "warm_recall": res["warm"]["recall"], "warm_ce": res["warm"]["ce"],
+            "random_short_ms": res["random_short"]["ms"], "random_short_recall": res["random_short"]["recall"],
+            "random_short_ce": res["random_short"]["ce"],
+            "ce_scored_on": f"{len(edges[0])} edges of the plain fit's {a.epochs}-epoch pruned graph + 5x random pairs",
+            "time_ratio_warm_over_plain": res["warm"]["ms"] / res["plain"]["ms"],
+            "recall_gap_plain_minus_warm": res["plain"]["recall"] - res["warm"]["recall"],
+            "warm_phase_ms": info["ms"], "mlp_losses": [info["mlp_losses"][0], info["mlp_losses"][-1]],
+            "mlp": {"train_steps": 20 * steps_per_epoch, "train_tflops": train_tflops,
+                    "predict_tflops": pred_tflops, "bf16_peak_tflops": tc,
+                    "train_frac": train_tflops / tc if tc else None,
+                    "predict_frac": pred_tflops / tc if tc else None},
+            "gpu_launches": launches, "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     a = parse()
     if a.impl == "reference":
         return run_reference(a)
     if a.workload == "batched":
         return run_batched(a)
+    if a.workload == "warm_start":
+        return run_warm_start(a)
     import torch
     import umap_b200 as ub
     rank, world, local = dist_info()

@@ -76,6 +76,11 @@ typedef struct umap_optimizer umap_optimizer; /* Optimizer, optimizer.rs:27-56  
 typedef struct umap_fitted umap_fitted;       /* FittedUmap, embedding.rs:438-443    */
 
 /* ---- library ---------------------------------------------------------------------- */
+/* Device pointers (the *_device calls, dev_* arguments): a call first waits for the work
+ * queued so far on the legacy default stream (stream 0, where PyTorch queues by default),
+ * then works on its handle's own stream and returns when its results are complete.  Inputs
+ * produced on any other stream must be complete before the call.  Calls on different
+ * handles may run concurrently from different host threads. */
 /* Message of the last failed call on this thread ("" if none). */
 const char* umap_last_error(void);
 int umap_abi_version(void);
@@ -179,6 +184,13 @@ int umap_fit_device(const umap_config* cfg, uint64_t n_samples, const uint32_t* 
                     const float* dev_knn_dists, uint64_t knn_rows, uint64_t knn_cols,
                     const float* dev_init, uint64_t init_rows, uint64_t init_cols,
                     umap_fitted** out);
+/* The rest of Umap::fit once the manifold is learned (embedding.rs:299-337): optimise for
+ * n_epochs (or the 500 / 200 default), then NaN rows for vertices with an empty graph row.
+ * Consumes `manifold`.  Lets a caller build the graph while it prepares `init`. */
+int umap_fit_manifold(umap_manifold* manifold, const umap_config* cfg, const float* host_init,
+                      uint64_t init_rows, uint64_t init_cols, umap_fitted** out);
+int umap_fit_manifold_device(umap_manifold* manifold, const umap_config* cfg, const float* dev_init,
+                             uint64_t init_rows, uint64_t init_cols, umap_fitted** out);
 
 /* ---- batched instances (no counterpart in the reference: a fit per dataset) --------
  * n_instances independent fits in one problem.  Instance s owns points
@@ -246,6 +258,44 @@ int umap_radix_sort_pairs_device_noalloc(const uint32_t* dev_keys_in, const uint
                                          uint32_t* dev_keys_out, uint32_t* dev_values_out,
                                          uint64_t n, int end_bit, void* stream);
 int umap_radix_sort_noalloc_max_pairs(uint64_t* out);
+
+/* ---- Learned warm start (no counterpart in the reference: its caller supplies `init`) ----
+ * An MLP in_dim -> 256 -> 256 -> out_dim with exact-erf GELU, bf16 weights and activations,
+ * fp32 accumulation on the tensor cores, trained with Adam (beta 0.9 / 0.999, eps 1e-8) on
+ * the mean squared error to target embeddings; its predictions initialise a shortened fit.
+ * Parameters are one flat fp32 array of umap_mlp_param_count() values in the order
+ * W1 [256][in_dim], b1 [256], W2 [256][256], b2 [256], W3 [out_dim][256], b3 [out_dim]
+ * (weights row-major, one row per output unit).  in_dim: a multiple of 64 up to 4096;
+ * out_dim: 1..4.  dev_* pointers are device memory (row-major rows of in_dim / out_dim
+ * floats); the others are host memory. */
+typedef struct umap_mlp umap_mlp;
+int umap_mlp_param_count(uint64_t in_dim, uint64_t out_dim, uint64_t* out);
+int umap_mlp_new(uint64_t in_dim, uint64_t out_dim, const float* params, umap_mlp** out);
+int umap_mlp_dims(const umap_mlp* m, uint64_t* in_dim, uint64_t* out_dim);
+int umap_mlp_get_params(const umap_mlp* m, float* params);
+int umap_mlp_set_params(umap_mlp* m, const float* params);
+/* Input standardisation x' = (x - shift) * scale (per input column) applied before the first
+ * layer; fit_input_norm sets shift = column mean and scale = 1 / column std of dev_x. */
+int umap_mlp_fit_input_norm_device(umap_mlp* m, const float* dev_x, uint64_t rows);
+int umap_mlp_input_norm(const umap_mlp* m, float* shift, float* scale);
+int umap_mlp_set_input_norm(umap_mlp* m, const float* shift, const float* scale);
+/* One forward + backward over `rows` rows (a multiple of 128) without an update: gradients of
+ * the mean squared error in the flat parameter order into `grads`, the loss into *loss. */
+int umap_mlp_gradients_device(umap_mlp* m, const float* dev_x, const float* dev_y, uint64_t rows,
+                              float* grads, float* loss);
+/* Adam over `epochs` shuffled passes of mini-batches of `batch` rows (a multiple of 128; the
+ * last partial batch of each pass is dropped).  losses (may be NULL) receives each epoch's
+ * mean batch loss. */
+int umap_mlp_train_device(umap_mlp* m, const float* dev_x, const float* dev_y, uint64_t rows,
+                          uint64_t epochs, uint64_t batch, float learning_rate, uint64_t seed,
+                          float* losses);
+int umap_mlp_predict_device(umap_mlp* m, const float* dev_x, uint64_t rows, float* dev_y);
+int umap_mlp_free(umap_mlp* m);
+/* The tensor-core GEMM the MLP is built from: dev_c [m][n] (fp32) = A [m][k] * B [n][k]^T with
+ * bf16 A and B (both K contiguous).  m % 128 == 0, n % 32 == 0, k % (64 * k_splits) == 0;
+ * k_splits > 1 adds the split partial sums into dev_c with atomics (zero it first). */
+int umap_gemm_bf16_device(const void* dev_a, const void* dev_b, float* dev_c, uint64_t m, uint64_t n,
+                          uint64_t k, uint64_t k_splits);
 
 #ifdef __cplusplus
 }

@@ -213,6 +213,14 @@ def test_nan_rows_for_disconnected_vertices(ub, oracle):
     assert np.isnan(e[7]).all() and not np.isnan(np.delete(e, 7, 0)).any()
     eo, _, _ = oracle.fit(idx, dist, init, oracle.OracleConfig(n_neighbors=10, n_epochs=20))
     assert np.array_equal(np.isnan(eo), np.isnan(e))
+    # fit split into learn_manifold + fit_manifold keeps the NaN rows and the graph
+    u = ub.Umap(cfg)
+    f2 = u.fit_manifold(u.learn_manifold(500, idx, dist), init)
+    assert np.array_equal(np.isnan(f2.embedding()), np.isnan(e))
+    g1, g2 = f.manifold().graph(), f2.manifold().graph()
+    assert np.array_equal(g1.indptr, g2.indptr) and np.array_equal(g1.indices, g2.indices)
+    with pytest.raises(ub.UmapError, match=r"^init has 499 samples but data has 500 samples$"):
+        u.fit_manifold(u.learn_manifold(500, idx, dist), init[:499])
 
 
 # ---------------------------------------------------------------- embedding quality

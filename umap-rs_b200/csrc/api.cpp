@@ -164,6 +164,11 @@ struct umap_fitted {
   cudaStream_t s() const { return manifold->s(); }
 };
 
+struct umap_mlp {
+  std::unique_ptr<ub::Stream> stream;  // declared first: destroyed last
+  std::unique_ptr<ub::Mlp> net;
+};
+
 namespace ub {
 namespace {
 
@@ -186,6 +191,10 @@ void set_error(const std::string& m) { g_last_error = m; }
   }                                                              \
   ub::set_error("");                                             \
   return UMAP_OK;
+
+// Device inputs are produced by the caller on the legacy default stream (PyTorch's default):
+// order after that work only, so calls on other handles (other streams) keep running.
+void wait_for_inputs() { UB_CUDA(cudaStreamSynchronize(cudaStreamLegacy)); }
 
 void need(const void* p, const char* what) {
   if (!p) throw Error(NULLPTR, std::string(what) + " is NULL");
@@ -539,6 +548,25 @@ std::unique_ptr<umap_fitted> into_fitted_impl(std::unique_ptr<umap_optimizer> o,
   return f;
 }
 
+// embedding.rs:299-337: the rest of Umap::fit once the manifold is learned.
+std::unique_ptr<umap_fitted> fit_manifold_impl(const umap_config& c, std::unique_ptr<umap_manifold> m,
+                                               const float* init, uint64_t irows, uint64_t icols, bool host) {
+  const uint64_t n_samples = m->n_vertices;
+  if (icols != c.n_components)
+    throw Error(INVALID_ARGUMENT, "init has " + std::to_string(icols) + " components but n_components is " +
+                                      std::to_string(c.n_components));
+  if (irows != n_samples)
+    throw Error(INVALID_ARGUMENT, "init has " + std::to_string(irows) + " samples but data has " +
+                                      std::to_string(n_samples) + " samples");
+  const uint64_t total = c.has_n_epochs ? c.n_epochs : (n_samples <= 10000 ? 500 : 200);  // :304-308
+  auto o = optimizer_new_impl(std::move(m), init, host, irows, icols, total, c, UMAP_METRIC_EUCLIDEAN);
+  step_epochs_impl(*o, total);  // :321
+  auto f = into_fitted_impl(std::move(o), c);
+  nan_empty_rows(f->manifold->indptr.p, f->n, (uint32_t)f->dim, f->embedding.p, f->s());  // :327-334
+  UB_CUDA(cudaStreamSynchronize(f->s()));
+  return f;
+}
+
 std::unique_ptr<umap_fitted> fit_impl(const umap_config& c, uint64_t n_samples, const uint32_t* idx,
                                       const float* dist, uint64_t rows, uint64_t cols, const float* init,
                                       uint64_t irows, uint64_t icols, bool host) {
@@ -567,13 +595,7 @@ std::unique_ptr<umap_fitted> fit_impl(const umap_config& c, uint64_t n_samples, 
   } else {
     m = learn_manifold_impl(c, n_samples, idx, dist, rows, cols);
   }
-  const uint64_t total = c.has_n_epochs ? c.n_epochs : (n_samples <= 10000 ? 500 : 200);  // :304-308
-  auto o = optimizer_new_impl(std::move(m), init, host, irows, icols, total, c, UMAP_METRIC_EUCLIDEAN);
-  step_epochs_impl(*o, total);  // :321
-  auto f = into_fitted_impl(std::move(o), c);
-  nan_empty_rows(f->manifold->indptr.p, f->n, (uint32_t)f->dim, f->embedding.p, f->s());  // :327-334
-  UB_CUDA(cudaStreamSynchronize(f->s()));
-  return f;
+  return fit_manifold_impl(c, std::move(m), init, irows, icols, host);
 }
 
 // ------------------------------------------------------------------ autotuning
@@ -985,7 +1007,7 @@ int umap_learn_manifold_device(const umap_config* cfg, uint64_t n_samples, const
   API_BEGIN
   need(cfg, "cfg"); need(idx, "knn_indices"); need(dist, "knn_dists"); need(out, "out");
   *out = nullptr;
-  UB_CUDA(cudaDeviceSynchronize());
+  wait_for_inputs();
   auto m = learn_manifold_impl(*cfg, n_samples, idx, dist, rows, cols);
   *out = m.release();
   API_END
@@ -1080,7 +1102,7 @@ int umap_optimizer_new_device(umap_manifold* manifold, const float* init, uint64
   need(manifold, "manifold"); need(init, "init"); need(cfg, "cfg"); need(out, "out");
   *out = nullptr;
   owned->stream->activate();
-  UB_CUDA(cudaDeviceSynchronize());
+  wait_for_inputs();
   *out = optimizer_new_impl(std::move(owned), init, false, rows, dims, total_epochs, *cfg, metric_type).release();
   API_END
 }
@@ -1300,8 +1322,31 @@ int umap_fit_device(const umap_config* cfg, uint64_t n_samples, const uint32_t* 
   API_BEGIN
   need(cfg, "cfg"); need(idx, "knn_indices"); need(dist, "knn_dists"); need(init, "init"); need(out, "out");
   *out = nullptr;
-  UB_CUDA(cudaDeviceSynchronize());
+  wait_for_inputs();
   *out = fit_impl(*cfg, n_samples, idx, dist, rows, cols, init, irows, icols, false).release();
+  API_END
+}
+
+int umap_fit_manifold(umap_manifold* manifold, const umap_config* cfg, const float* init, uint64_t irows,
+                      uint64_t icols, umap_fitted** out) {
+  std::unique_ptr<umap_manifold> owned(manifold);
+  API_BEGIN
+  need(manifold, "manifold"); need(cfg, "cfg"); need(init, "init"); need(out, "out");
+  *out = nullptr;
+  owned->stream->activate();
+  *out = fit_manifold_impl(*cfg, std::move(owned), init, irows, icols, true).release();
+  API_END
+}
+
+int umap_fit_manifold_device(umap_manifold* manifold, const umap_config* cfg, const float* init, uint64_t irows,
+                             uint64_t icols, umap_fitted** out) {
+  std::unique_ptr<umap_manifold> owned(manifold);
+  API_BEGIN
+  need(manifold, "manifold"); need(cfg, "cfg"); need(init, "init"); need(out, "out");
+  *out = nullptr;
+  owned->stream->activate();
+  wait_for_inputs();
+  *out = fit_manifold_impl(*cfg, std::move(owned), init, irows, icols, false).release();
   API_END
 }
 
@@ -1501,7 +1546,7 @@ int umap_batch_optimizer_new_device(const umap_config* cfg, uint64_t n_instances
   need(cfg, "cfg"); need(offsets, "offsets"); need(idx, "knn_indices"); need(dist, "knn_dists");
   need(init, "init"); need(out, "out");
   *out = nullptr;
-  UB_CUDA(cudaDeviceSynchronize());
+  wait_for_inputs();
   *out = batch_new_impl(*cfg, n_instances, offsets, idx, dist, knn_cols, init, init_cols, total_epochs, false)
              .release();
   API_END
@@ -1522,7 +1567,7 @@ int umap_batch_fit_device(const umap_config* cfg, uint64_t n_instances, const ui
   API_BEGIN
   need(cfg, "cfg"); need(offsets, "offsets"); need(idx, "knn_indices"); need(dist, "knn_dists");
   need(init, "init"); need(out, "out");
-  UB_CUDA(cudaDeviceSynchronize());
+  wait_for_inputs();
   batch_fit_impl(*cfg, n_instances, offsets, idx, dist, knn_cols, init, init_cols, out, false);
   API_END
 }
@@ -1544,7 +1589,7 @@ int umap_smooth_knn_dist_device(const float* dists, uint64_t n, uint64_t k, uint
   cudaStream_t s;
   UB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
   struct SGuard { cudaStream_t s; ~SGuard() { (void)cudaStreamSynchronize(s); (void)cudaStreamDestroy(s); } } g{s};
-  UB_CUDA(cudaDeviceSynchronize());
+  wait_for_inputs();
   GraphParams gp{};
   gp.local_connectivity = local_connectivity;
   const float lcf = floorf(local_connectivity);
@@ -1565,7 +1610,7 @@ int umap_radix_sort_pairs_device(const uint32_t* keys_in, const uint32_t* vals_i
   cudaStream_t s;
   UB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
   struct SGuard { cudaStream_t s; ~SGuard() { (void)cudaStreamSynchronize(s); (void)cudaStreamDestroy(s); } } g{s};
-  UB_CUDA(cudaDeviceSynchronize());
+  wait_for_inputs();
   radix_sort_pairs(keys_in, vals_in, keys_out, vals_out, n, end_bit, s);
   UB_CUDA(cudaStreamSynchronize(s));
   API_END
@@ -1585,6 +1630,130 @@ int umap_radix_sort_noalloc_max_pairs(uint64_t* out) {
   API_BEGIN
   need(out, "out");
   *out = radix_sort_noalloc_max_pairs();
+  API_END
+}
+
+// ---------------------------------------------------------------- learned warm start
+int umap_mlp_param_count(uint64_t in_dim, uint64_t out_dim, uint64_t* out) {
+  API_BEGIN
+  need(out, "out");
+  if (in_dim > 4096 || out_dim > 4) throw Error(INVALID_ARGUMENT, "in_dim must be <= 4096 and out_dim <= 4");
+  *out = (uint64_t)Mlp::param_count((int)in_dim, (int)out_dim);
+  API_END
+}
+
+int umap_mlp_new(uint64_t in_dim, uint64_t out_dim, const float* params, umap_mlp** out) {
+  API_BEGIN
+  need(params, "params"); need(out, "out");
+  *out = nullptr;
+  if (in_dim > 4096 || out_dim > 4)
+    throw Error(INVALID_ARGUMENT, "MLP input width must be a positive multiple of 64 (at most 4096) and output width 1..4");
+  auto m = std::make_unique<umap_mlp>();
+  m->stream = std::make_unique<Stream>();
+  m->net = std::make_unique<Mlp>((int)in_dim, (int)out_dim, params, m->stream->s);
+  *out = m.release();
+  API_END
+}
+
+int umap_mlp_dims(const umap_mlp* m, uint64_t* in_dim, uint64_t* out_dim) {
+  API_BEGIN
+  need(m, "mlp"); need(in_dim, "in_dim"); need(out_dim, "out_dim");
+  *in_dim = (uint64_t)m->net->in_dim();
+  *out_dim = (uint64_t)m->net->out_dim();
+  API_END
+}
+
+int umap_mlp_get_params(const umap_mlp* m, float* params) {
+  API_BEGIN
+  need(m, "mlp"); need(params, "params");
+  m->stream->activate();
+  m->net->get_params(params);
+  API_END
+}
+
+int umap_mlp_set_params(umap_mlp* m, const float* params) {
+  API_BEGIN
+  need(m, "mlp"); need(params, "params");
+  m->stream->activate();
+  m->net->set_params(params);
+  API_END
+}
+
+int umap_mlp_fit_input_norm_device(umap_mlp* m, const float* x, uint64_t rows) {
+  API_BEGIN
+  need(m, "mlp"); need(x, "x");
+  m->stream->activate();
+  wait_for_inputs();
+  m->net->fit_input_norm(x, (int64_t)rows);
+  API_END
+}
+
+int umap_mlp_input_norm(const umap_mlp* m, float* shift, float* scale) {
+  API_BEGIN
+  need(m, "mlp"); need(shift, "shift"); need(scale, "scale");
+  m->stream->activate();
+  m->net->get_input_norm(shift, scale);
+  API_END
+}
+
+int umap_mlp_set_input_norm(umap_mlp* m, const float* shift, const float* scale) {
+  API_BEGIN
+  need(m, "mlp"); need(shift, "shift"); need(scale, "scale");
+  m->stream->activate();
+  m->net->set_input_norm(shift, scale);
+  API_END
+}
+
+int umap_mlp_gradients_device(umap_mlp* m, const float* x, const float* y, uint64_t rows, float* grads,
+                              float* loss) {
+  API_BEGIN
+  need(m, "mlp"); need(x, "x"); need(y, "y"); need(grads, "grads"); need(loss, "loss");
+  m->stream->activate();
+  wait_for_inputs();
+  m->net->gradients(x, y, (int64_t)rows, grads, loss);
+  API_END
+}
+
+int umap_mlp_train_device(umap_mlp* m, const float* x, const float* y, uint64_t rows, uint64_t epochs,
+                          uint64_t batch, float learning_rate, uint64_t seed, float* losses) {
+  API_BEGIN
+  need(m, "mlp"); need(x, "x"); need(y, "y");
+  if (epochs > (1u << 20)) throw Error(INVALID_ARGUMENT, "epochs must be <= 1048576");
+  if (!(learning_rate > 0.0f)) throw Error(INVALID_ARGUMENT, "learning_rate must be positive, got " + rust_f32(learning_rate));
+  m->stream->activate();
+  wait_for_inputs();
+  m->net->train(x, y, (int64_t)std::min<uint64_t>(rows, 1ull << 40), (int)epochs,
+                (int64_t)std::min<uint64_t>(batch, 1ull << 40), learning_rate, seed, losses);
+  API_END
+}
+
+int umap_mlp_predict_device(umap_mlp* m, const float* x, uint64_t rows, float* y) {
+  API_BEGIN
+  need(m, "mlp"); need(x, "x"); need(y, "y");
+  m->stream->activate();
+  wait_for_inputs();
+  m->net->predict(x, (int64_t)std::min<uint64_t>(rows, 1ull << 40), y);
+  API_END
+}
+
+int umap_mlp_free(umap_mlp* m) {
+  API_BEGIN
+  if (m) {
+    m->stream->activate();
+    delete m;
+  }
+  API_END
+}
+
+int umap_gemm_bf16_device(const void* a, const void* b, float* c, uint64_t m, uint64_t n, uint64_t k,
+                          uint64_t k_splits) {
+  API_BEGIN
+  need(a, "a"); need(b, "b"); need(c, "c");
+  if (m > (1ull << 40) || n > (1ull << 30) || k > (1ull << 30) || k_splits < 1 || k_splits > 65535)
+    throw Error(INVALID_ARGUMENT, "GEMM dimensions out of range");
+  Stream st;
+  wait_for_inputs();
+  umma_gemm_f32(a, b, c, (int64_t)m, (int64_t)n, (int64_t)k, (int)k_splits, st.s);
   API_END
 }
 

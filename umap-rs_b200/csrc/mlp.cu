@@ -1,0 +1,985 @@
+// Learned warm start: a small MLP (in -> 256 -> 256 -> out, exact-erf GELU) with BF16 weights
+// and activations and FP32 accumulation, trained with Adam on the mean squared error to 2-D
+// targets.  The reference has no counterpart (its caller supplies the initial embedding);
+// this produces that initial embedding from the input features.
+//
+// Tensor-core GEMM.  C[M,N] = A[M,K] * B[N,K]^T with A and B BF16, both K-major (row-major,
+// K contiguous), FP32 accumulation in tensor memory.  One CTA (4 warps) owns a 128 x BN
+// output tile and a K range (blockIdx.z splits K; split partial sums are added with
+// atomics).  Warp 0 allocates BN tensor-memory columns.  K is staged 64 at a time into shared
+// memory in the canonical no-swizzle K-major layout: 8-row x 16-byte core matrices, element
+// (r, k) of a 64-wide chunk at byte (r/8)*1024 + (k/8)*128 + (r%8)*16 + (k%8)*2, so the
+// descriptor of MMA step s (k = 16s..16s+15) starts at +256*s with leading byte offset 128
+// (the next 8 k) and stride byte offset 1024 (the next 8 rows).  One thread issues the four
+// tcgen05.mma (M=128, N=BN, K=16) of a chunk and commits them to an mbarrier; all threads
+// wait on it (bounded by a timer) before the chunk buffer is refilled.  The epilogue reads
+// the accumulator with tcgen05.ld (warp w owns rows 32w..32w+31, thread = row) and fuses
+// bias, GELU, the GELU derivative, column sums and transposed copies.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <cstdlib>
+#include <mutex>
+#include <vector>
+
+#include "ub_internal.hpp"
+
+namespace ub {
+namespace {
+
+using bf16 = __nv_bfloat16;
+
+constexpr int GM = 128;   // tile rows (UMMA M)
+constexpr int KC = 64;    // K staged per chunk
+constexpr int GT = 128;   // threads per GEMM CTA
+constexpr int HID = 256;  // hidden width
+
+enum Epi : int {
+  EPI_F32 = 0,         // out_f32 = acc (+ bias)
+  EPI_F32_ATOMIC = 1,  // out_f32 += acc (split-K partial sums)
+  EPI_BIAS_GELU = 2,   // z = acc + bias -> out_f32 (if set); h = gelu(z) -> out_bf16 (+ out_t)
+  EPI_GELU_GRAD = 3,   // d = acc * gelu'(z_in) -> out_bf16 / out_t (if set); colsum += sum_rows d
+};
+
+struct EpiArgs {
+  const float* bias;
+  float* out_f32;
+  const float* z_in;
+  bf16* out_bf16;
+  bf16* out_t;   // transposed copy [N, ldt]
+  float* colsum;
+  int ldo, ldt;
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// Shared-memory matrix descriptor: K-major, no swizzle (layout type 0), descriptor version 1.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1u << 46;
+  return d;
+}
+
+// Instruction descriptor, kind::f16: D F32 (bits 4-5 = 1), A and B BF16 (bits 7-9 and 10-12
+// = 1), both K-major (bits 15, 16 = 0), N >> 3 at bit 17, M >> 4 at bit 24.
+__host__ __device__ constexpr uint32_t instr_desc(int M, int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
+__device__ __forceinline__ float gelu_grad(float x) {
+  const float cdf = 0.5f * (1.0f + erff(x * 0.70710678118654752f));
+  const float pdf = 0.39894228040143268f * expf(-0.5f * x * x);
+  return cdf + x * pdf;
+}
+
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Waits for an mbarrier phase; gives up after about two seconds.
+__device__ __forceinline__ bool mbar_wait(uint32_t addr, uint32_t phase) {
+  const uint64_t t0 = global_ns();
+  for (uint32_t it = 0; it < (1u << 30); ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred P;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, P;\n\t}"
+        : "=r"(done)
+        : "r"(addr), "r"(phase)
+        : "memory");
+    if (done) return true;
+    if ((it & 255u) == 255u && global_ns() - t0 > 2000000000ull) return false;
+  }
+  return false;
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
+  const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+  return *reinterpret_cast<const uint32_t*>(&h);
+}
+
+template <int BN, int EPI>
+__global__ void __launch_bounds__(GT) umma_gemm_kernel(const bf16* __restrict__ A, int lda,
+                                                       const bf16* __restrict__ B, int ldb, int k_per_cta,
+                                                       EpiArgs ep, unsigned* __restrict__ err) {
+  // UMMA with M=128 takes N % 16 == 0 up to 256; the epilogue reads 32 columns at a time.
+  static_assert(BN % 32 == 0 && BN >= 32 && BN <= 256, "tile width");
+  constexpr uint32_t TCOLS = BN <= 32 ? 32 : BN <= 64 ? 64 : BN <= 128 ? 128 : 256;
+  constexpr int STAGE = (GM + BN) * KC * 2;  // bytes of one K chunk of A and B
+  extern __shared__ __align__(1024) uint8_t smem[];  // two stages: [A | B] [A | B]
+  __shared__ __align__(8) uint64_t mbar[2];          // MMA completion, one per stage
+  __shared__ uint32_t tmem_base;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int64_t m0 = (int64_t)blockIdx.x * GM, n0 = (int64_t)blockIdx.y * BN;
+  const int64_t k_begin = (int64_t)blockIdx.z * k_per_cta;
+  const int n_chunks = k_per_cta / KC;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                 :: "r"(smem_u32(&tmem_base)), "r"(TCOLS) : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(&mbar[0])), "r"(1) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(&mbar[1])), "r"(1) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t taddr = tmem_base;
+
+  // A[m0:m0+128, k:k+64] and B[n0:n0+BN, k:k+64] of chunk c into stage `st`, 16-byte vectors.
+  auto stage_chunk = [&](int c, int st) {
+    const int64_t kg = k_begin + (int64_t)c * KC;
+    uint8_t* sA = smem + st * STAGE;
+    uint8_t* sB = sA + GM * KC * 2;
+#pragma unroll 4
+    for (int v = tid; v < GM * (KC / 8); v += GT) {
+      const int r = v >> 3, c8 = v & 7;
+      const uint4 x = __ldg(reinterpret_cast<const uint4*>(A + (m0 + r) * lda + kg + c8 * 8));
+      *reinterpret_cast<uint4*>(sA + (r >> 3) * (KC * 16) + c8 * 128 + (r & 7) * 16) = x;
+    }
+#pragma unroll 4
+    for (int v = tid; v < BN * (KC / 8); v += GT) {
+      const int r = v >> 3, c8 = v & 7;
+      const uint4 x = __ldg(reinterpret_cast<const uint4*>(B + (n0 + r) * ldb + kg + c8 * 8));
+      *reinterpret_cast<uint4*>(sB + (r >> 3) * (KC * 16) + c8 * 128 + (r & 7) * 16) = x;
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  };
+  // The j-th completion of a stage's barrier (j = chunk / 2) has phase parity j & 1.
+  auto wait_chunk = [&](int c) { return mbar_wait(smem_u32(&mbar[c & 1]), (uint32_t)((c >> 1) & 1)); };
+
+  bool ok = true;
+  int last_issued = -1;
+  if (n_chunks > 0) stage_chunk(0, 0);
+  for (int c = 0; c < n_chunks; ++c) {
+    __syncthreads();  // stage c & 1 holds chunk c
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t a0 = smem_u32(smem + (c & 1) * STAGE);
+      const uint32_t b0 = a0 + GM * KC * 2;
+      constexpr uint32_t idesc = instr_desc(GM, BN);
+#pragma unroll
+      for (int s = 0; s < KC / 16; ++s) {
+        const uint64_t ad = smem_desc(a0 + s * 256, 128, KC * 16);
+        const uint64_t bd = smem_desc(b0 + s * 256, 128, KC * 16);
+        const uint32_t acc = (c > 0 || s > 0) ? 1u : 0u;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+            :: "r"(taddr), "l"(ad), "l"(bd), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+            : "memory");
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                   :: "r"(smem_u32(&mbar[c & 1])) : "memory");
+    }
+    last_issued = c;
+    if (c + 1 < n_chunks) {
+      // the other stage was last read by chunk c - 1: wait for it, then refill it while
+      // the MMAs of chunk c run
+      bool free_ok = true;
+      if (c >= 1) free_ok = wait_chunk(c - 1);
+      if (!__syncthreads_and(free_ok)) {
+        ok = false;
+        break;
+      }
+      stage_chunk(c + 1, (c + 1) & 1);
+    }
+  }
+  if (ok && last_issued >= 0) ok = __syncthreads_and(wait_chunk(last_issued));
+  if (!ok) {
+    // MMAs did not complete in time: record it, give the last ones one more bounded wait,
+    // release tensor memory and leave the tile unwritten.
+    if (tid == 0) atomicOr(err, 1u);
+    if (last_issued >= 0) (void)wait_chunk(last_issued);
+  }
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+
+  if (ok) {
+    const int64_t row = m0 + warp * 32 + lane;
+#pragma unroll 1
+    for (int c0 = 0; c0 < BN; c0 += 32) {
+      uint32_t r[32];
+      const uint32_t ta = taddr + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+          "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+          "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+            "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+            "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+            "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+          : "r"(ta));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      const int64_t cb = n0 + c0;  // first column of this group
+      float v[32];
+#pragma unroll
+      for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
+      if (EPI == EPI_F32 || EPI == EPI_F32_ATOMIC) {
+        if (EPI == EPI_F32 && ep.bias) {
+#pragma unroll
+          for (int j = 0; j < 32; ++j) v[j] += __ldg(ep.bias + cb + j);
+        }
+        float4* o = reinterpret_cast<float4*>(ep.out_f32 + row * ep.ldo + cb);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const float4 x = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+          if (EPI == EPI_F32_ATOMIC) atomicAdd(o + q, x);
+          else o[q] = x;
+        }
+      } else {
+        if (EPI == EPI_BIAS_GELU) {
+#pragma unroll
+          for (int j = 0; j < 32; ++j) v[j] += __ldg(ep.bias + cb + j);
+          if (ep.out_f32) {
+            float4* o = reinterpret_cast<float4*>(ep.out_f32 + row * ep.ldo + cb);
+#pragma unroll
+            for (int q = 0; q < 8; ++q) o[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+          }
+#pragma unroll
+          for (int j = 0; j < 32; ++j) v[j] = gelu(v[j]);
+        } else {  // EPI_GELU_GRAD
+          const float4* zi = reinterpret_cast<const float4*>(ep.z_in + row * ep.ldo + cb);
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            const float4 z = zi[q];
+            v[4 * q] *= gelu_grad(z.x);
+            v[4 * q + 1] *= gelu_grad(z.y);
+            v[4 * q + 2] *= gelu_grad(z.z);
+            v[4 * q + 3] *= gelu_grad(z.w);
+          }
+          if (ep.colsum) {
+#pragma unroll
+            for (int j = 0; j < 32; ++j) {
+              float s = v[j];
+#pragma unroll
+              for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xFFFFFFFFu, s, o);
+              if (lane == 0) atomicAdd(ep.colsum + cb + j, s);
+            }
+          }
+        }
+        uint32_t pk[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) pk[j] = pack_bf16(v[2 * j], v[2 * j + 1]);
+        if (ep.out_bf16) {
+          uint4* o = reinterpret_cast<uint4*>(ep.out_bf16 + row * ep.ldo + cb);
+#pragma unroll
+          for (int q = 0; q < 4; ++q) o[q] = make_uint4(pk[4 * q], pk[4 * q + 1], pk[4 * q + 2], pk[4 * q + 3]);
+        }
+        if (ep.out_t) {
+          uint16_t* t = reinterpret_cast<uint16_t*>(ep.out_t);
+#pragma unroll
+          for (int j = 0; j < 32; ++j)
+            t[(cb + j) * ep.ldt + row] = (uint16_t)((j & 1) ? (pk[j >> 1] >> 16) : (pk[j >> 1] & 0xFFFFu));
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(taddr), "r"(TCOLS) : "memory");
+}
+
+template <int BN, int EPI>
+constexpr size_t gemm_smem() {
+  return (size_t)2 * (GM + BN) * KC * 2;
+}
+
+template <int BN, int EPI>
+void prepare_gemm() {
+  UB_CUDA(cudaFuncSetAttribute(umma_gemm_kernel<BN, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)gemm_smem<BN, EPI>()));
+}
+
+// C = A[M,K] B[N,K]^T with the K range split into `ksplit` equal parts (EPI_F32_ATOMIC only).
+template <int BN, int EPI>
+void launch_gemm(const bf16* A, int64_t lda, const bf16* B, int64_t ldb, int64_t M, int64_t N, int64_t K,
+                 int ksplit, const EpiArgs& ep, unsigned* err, cudaStream_t s) {
+  if (M <= 0 || M % GM || N % BN || K <= 0 || ksplit < 1 || K % ((int64_t)KC * ksplit) || lda % 8 || ldb % 8 ||
+      M / GM > 0x7FFFFFFF || lda > 0x7FFFFFFF || ldb > 0x7FFFFFFF)
+    throw Error(INVALID_ARGUMENT, "tensor-core GEMM shape: M % 128, N % tile, K % (64 * splits), rows of 16 bytes");
+  if (ksplit > 1 && EPI != EPI_F32_ATOMIC) throw Error(INVALID_ARGUMENT, "split K needs the atomic epilogue");
+  dim3 grid((unsigned)(M / GM), (unsigned)(N / BN), (unsigned)ksplit);
+  umma_gemm_kernel<BN, EPI><<<grid, GT, gemm_smem<BN, EPI>(), s>>>(A, (int)lda, B, (int)ldb, (int)(K / ksplit), ep,
+                                                                   err);
+  UB_LAUNCH_CHECK();
+}
+
+// ------------------------------------------------------------------------------ CUDA-core parts
+// Batch assembly.  Block (bx, by) handles batch rows 32bx..32bx+31 and input columns
+// 64by..64by+63: xb[b] = bf16((X[src(b)] - shift) * scale) row-major and, when xt is set, its
+// transpose xt [in, ldt].  src(b) = rows[b] (training) or min(b, n_valid - 1) (inference,
+// padded tail).  Blocks with by == 0 gather the targets; all blocks zero `zero[0..n_zero)`
+// and block (0, 0) advances the Adam step counter.
+__global__ void __launch_bounds__(256) batch_kernel(
+    const float* __restrict__ X, int in_dim, const uint32_t* __restrict__ rows, int64_t n_valid,
+    const float* __restrict__ shift, const float* __restrict__ scale, bf16* __restrict__ xb, bf16* __restrict__ xt,
+    int64_t ldt, const float* __restrict__ Y, int out_dim, float* __restrict__ yb, float* __restrict__ zero,
+    int64_t n_zero, unsigned* __restrict__ step) {
+  __shared__ uint16_t tile[64][34];
+  const int tid = threadIdx.x;
+  const int64_t b0 = (int64_t)blockIdx.x * 32;
+  const int c0 = blockIdx.y * 64;
+  for (int e = tid; e < 32 * 64; e += 256) {
+    const int r = e >> 6, c = e & 63;
+    const int64_t b = b0 + r;
+    const int64_t src = rows ? (int64_t)rows[b] : std::min<int64_t>(b, n_valid - 1);
+    float x = X[src * in_dim + c0 + c];
+    if (scale) x = (x - shift[c0 + c]) * scale[c0 + c];
+    const bf16 h = __float2bfloat16_rn(x);
+    xb[b * in_dim + c0 + c] = h;
+    tile[c][r] = *reinterpret_cast<const uint16_t*>(&h);
+  }
+  if (Y && blockIdx.y == 0 && tid < 32 * out_dim) {
+    const int r = tid / out_dim, j = tid - r * out_dim;
+    yb[(b0 + r) * out_dim + j] = Y[(int64_t)rows[b0 + r] * out_dim + j];
+  }
+  if (zero) {
+    const int64_t nb = (int64_t)gridDim.x * gridDim.y;
+    const int64_t bid = (int64_t)blockIdx.y * gridDim.x + blockIdx.x;
+    for (int64_t i = bid * 256 + tid; i < n_zero; i += nb * 256) zero[i] = 0.0f;
+    if (step && bid == 0 && tid == 0) *step += 1u;
+  }
+  if (!xt) return;
+  __syncthreads();
+  uint16_t* t = reinterpret_cast<uint16_t*>(xt);
+  for (int e = tid; e < 32 * 64; e += 256) {
+    const int c = e >> 5, r = e & 31;
+    t[(int64_t)(c0 + c) * ldt + b0 + r] = tile[c][r];
+  }
+}
+
+// Output layer (256 -> OUT) on CUDA cores, one warp per row, 32 rows per block; lane l owns
+// hidden columns 8l..8l+7.  y = h2 W3^T + b3.  With a target it also runs the loss and the
+// backward of this layer: e = y - t; loss += sum e^2 / count; dy = 2 e / count;
+// dz2 = (dy W3) * gelu'(z2) -> bf16 row-major and transposed [256, ldt]; dW3 += dy^T h2;
+// db3 += sum dy; db2 += sum dz2 (fp32, before rounding).
+template <int OUT>
+__global__ void __launch_bounds__(256) out_layer_kernel(
+    const bf16* __restrict__ h2, const float* __restrict__ z2, const bf16* __restrict__ w3,
+    const float* __restrict__ b3, const float* __restrict__ target, int64_t n_valid, float inv_count,
+    float* __restrict__ y_out, bf16* __restrict__ dz2, bf16* __restrict__ dz2t, int64_t ldt,
+    float* __restrict__ g_w3, float* __restrict__ g_b3, float* __restrict__ g_b2, float* __restrict__ loss) {
+  __shared__ uint16_t s_t[HID][34];
+  __shared__ float s_gw3[OUT * HID];
+  __shared__ float s_gb2[HID];
+  __shared__ float s_gb3[OUT];
+  __shared__ float s_loss;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const bool train = target != nullptr;
+  if (train) {
+    for (int i = tid; i < OUT * HID; i += 256) s_gw3[i] = 0.0f;
+    s_gb2[tid] = 0.0f;
+    if (tid < OUT) s_gb3[tid] = 0.0f;
+    if (tid == 0) s_loss = 0.0f;
+    __syncthreads();
+  }
+  float w[OUT][8];
+#pragma unroll
+  for (int j = 0; j < OUT; ++j) {
+    const uint4 u = *reinterpret_cast<const uint4*>(w3 + j * HID + 8 * lane);
+    const __nv_bfloat162* p = reinterpret_cast<const __nv_bfloat162*>(&u);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const float2 f = __bfloat1622float2(p[i]);
+      w[j][2 * i] = f.x;
+      w[j][2 * i + 1] = f.y;
+    }
+  }
+  float bias[OUT];
+#pragma unroll
+  for (int j = 0; j < OUT; ++j) bias[j] = b3[j];
+  float gw[OUT][8] = {}, gb2[8] = {}, gb3[OUT] = {}, lsum = 0.0f;
+  for (int rr = 0; rr < 4; ++rr) {
+    const int rl = warp * 4 + rr;
+    const int64_t row = (int64_t)blockIdx.x * 32 + rl;
+    float h[8];
+    {
+      const uint4 u = *reinterpret_cast<const uint4*>(h2 + row * HID + 8 * lane);
+      const __nv_bfloat162* p = reinterpret_cast<const __nv_bfloat162*>(&u);
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const float2 f = __bfloat1622float2(p[i]);
+        h[2 * i] = f.x;
+        h[2 * i + 1] = f.y;
+      }
+    }
+    float y[OUT];
+#pragma unroll
+    for (int j = 0; j < OUT; ++j) {
+      float s = 0.0f;
+#pragma unroll
+      for (int i = 0; i < 8; ++i) s += h[i] * w[j][i];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xFFFFFFFFu, s, o);
+      y[j] = s + bias[j];
+    }
+    if (y_out && lane == 0 && row < n_valid) {
+#pragma unroll
+      for (int j = 0; j < OUT; ++j) y_out[row * OUT + j] = y[j];
+    }
+    if (!train) continue;
+    float dy[OUT];
+#pragma unroll
+    for (int j = 0; j < OUT; ++j) {
+      const float e = y[j] - target[row * OUT + j];
+      lsum += e * e * inv_count;
+      dy[j] = 2.0f * e * inv_count;
+      gb3[j] += dy[j];
+    }
+    const float4* zr = reinterpret_cast<const float4*>(z2 + row * HID + 8 * lane);
+    const float4 za = zr[0], zb = zr[1];
+    const float z[8] = {za.x, za.y, za.z, za.w, zb.x, zb.y, zb.z, zb.w};
+    float d[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      float dh = 0.0f;
+#pragma unroll
+      for (int j = 0; j < OUT; ++j) dh += dy[j] * w[j][i];
+      d[i] = dh * gelu_grad(z[i]);
+      gb2[i] += d[i];
+#pragma unroll
+      for (int j = 0; j < OUT; ++j) gw[j][i] += dy[j] * h[i];
+    }
+    uint32_t pk[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) pk[i] = pack_bf16(d[2 * i], d[2 * i + 1]);
+    *reinterpret_cast<uint4*>(dz2 + row * HID + 8 * lane) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+      s_t[8 * lane + i][rl] = (uint16_t)((i & 1) ? (pk[i >> 1] >> 16) : (pk[i >> 1] & 0xFFFFu));
+  }
+  if (!train) return;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    atomicAdd(&s_gb2[8 * lane + i], gb2[i]);
+#pragma unroll
+    for (int j = 0; j < OUT; ++j) atomicAdd(&s_gw3[j * HID + 8 * lane + i], gw[j][i]);
+  }
+  if (lane == 0) {
+#pragma unroll
+    for (int j = 0; j < OUT; ++j) atomicAdd(&s_gb3[j], gb3[j]);
+    atomicAdd(&s_loss, lsum);
+  }
+  __syncthreads();
+  // transposed dz2: thread = hidden column, 32 consecutive rows as 16 packed pairs
+  {
+    uint32_t* dst = reinterpret_cast<uint32_t*>(dz2t + (int64_t)tid * ldt + (int64_t)blockIdx.x * 32);
+    const uint16_t* src = s_t[tid];
+#pragma unroll
+    for (int p = 0; p < 16; ++p) dst[p] = (uint32_t)src[2 * p] | ((uint32_t)src[2 * p + 1] << 16);
+  }
+  for (int i = tid; i < OUT * HID; i += 256) atomicAdd(g_w3 + i, s_gw3[i]);
+  atomicAdd(g_b2 + tid, s_gb2[tid]);
+  if (tid < OUT) atomicAdd(g_b3 + tid, s_gb3[tid]);
+  if (tid == 0) atomicAdd(loss, s_loss);
+}
+
+// Adam (Kingma & Ba 2015) over the flat fp32 parameters, bias-corrected with the step count
+// held on the device; refreshes the bf16 working copies of the three weight matrices (and W2^T).
+struct AdamArgs {
+  float* w;
+  float* m;
+  float* v;
+  const float* g;
+  int64_t n;
+  float lr, b1, b2, eps;
+  const unsigned* step;
+  int64_t o_w1, o_w2, o_w3, n_w1, n_w3;
+  bf16* w1b;
+  bf16* w2b;
+  bf16* w2t;
+  bf16* w3b;
+};
+
+__global__ void adam_kernel(AdamArgs a) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.n) return;
+  const float t = (float)*a.step;
+  const float c1 = 1.0f - powf(a.b1, t), c2 = 1.0f - powf(a.b2, t);
+  const float gi = a.g[i];
+  const float mi = a.b1 * a.m[i] + (1.0f - a.b1) * gi;
+  const float vi = a.b2 * a.v[i] + (1.0f - a.b2) * gi * gi;
+  a.m[i] = mi;
+  a.v[i] = vi;
+  const float wi = a.w[i] - a.lr * (mi / c1) / (sqrtf(vi / c2) + a.eps);
+  a.w[i] = wi;
+  const bf16 h = __float2bfloat16_rn(wi);
+  if (i >= a.o_w1 && i < a.o_w1 + a.n_w1) {
+    a.w1b[i - a.o_w1] = h;
+  } else if (i >= a.o_w2 && i < a.o_w2 + (int64_t)HID * HID) {
+    const int64_t k = i - a.o_w2;
+    a.w2b[k] = h;
+    a.w2t[(k % HID) * HID + k / HID] = h;
+  } else if (i >= a.o_w3 && i < a.o_w3 + a.n_w3) {
+    a.w3b[i - a.o_w3] = h;
+  }
+}
+
+__global__ void to_bf16_kernel(const float* __restrict__ w, int64_t n, bf16* __restrict__ wb, bf16* __restrict__ wt,
+                               int cols) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const bf16 b = __float2bfloat16_rn(w[i]);
+  wb[i] = b;
+  if (wt) {
+    const int64_t r = i / cols, c = i - r * cols;
+    wt[c * (n / cols) + r] = b;
+  }
+}
+
+// Per-column mean and 1/std (population) of X [n, d]; one block per column, fp64 sums.
+__global__ void column_stats_kernel(const float* __restrict__ X, int64_t n, int d, float* __restrict__ mean,
+                                    float* __restrict__ inv_std) {
+  __shared__ double s1[256], s2[256];
+  const int c = blockIdx.x;
+  double a = 0.0, b = 0.0;
+  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+    const double x = X[i * d + c];
+    a += x;
+    b += x * x;
+  }
+  s1[threadIdx.x] = a;
+  s2[threadIdx.x] = b;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) {
+      s1[threadIdx.x] += s1[threadIdx.x + w];
+      s2[threadIdx.x] += s2[threadIdx.x + w];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const double mu = s1[0] / (double)n;
+    const double var = std::max(s2[0] / (double)n - mu * mu, 0.0);
+    mean[c] = (float)mu;
+    inv_std[c] = var > 1e-24 ? (float)(1.0 / sqrt(var)) : 1.0f;
+  }
+}
+
+inline unsigned grid_for(int64_t n, unsigned bt) { return (unsigned)((n + bt - 1) / bt); }
+
+bool graphs_enabled() {
+  const char* e = std::getenv("UMAP_B200_GRAPH");
+  return !(e && e[0] == '0');
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------------------ model
+struct Mlp::Impl {
+  int in_dim = 0, out_dim = 0;
+  cudaStream_t s = nullptr;
+  int64_t P = 0, o_w1 = 0, o_b1 = 0, o_w2 = 0, o_b2 = 0, o_w3 = 0, o_b3 = 0;
+  DevBuf<float> w, m, v, g;         // flat fp32 parameters, Adam moments, gradients
+  DevBuf<bf16> w1b, w2b, w2t, w3b;  // bf16 working copies (w2t = W2^T)
+  DevBuf<float> shift, scale;       // input standardisation
+  bool has_norm = false;
+  DevBuf<unsigned> err, step;
+  DevBuf<float> loss;
+  // per-batch activations, capacity `cap` rows
+  int64_t cap = 0;
+  bool cap_train = false;
+  DevBuf<bf16> xb, xt, h1, h1t, h2, dz2, dz2t, dz1t;
+  DevBuf<float> z1, z2, yb;
+
+  void ensure(int64_t B, bool train) {
+    if (B <= cap && (!train || cap_train)) return;
+    cap = std::max(cap, B);
+    cap_train = cap_train || train;
+    xb.alloc(cap * in_dim, s);
+    h1.alloc(cap * HID, s);
+    h2.alloc(cap * HID, s);
+    if (cap_train) {
+      xt.alloc(cap * in_dim, s);
+      h1t.alloc(cap * HID, s);
+      dz2.alloc(cap * HID, s);
+      dz2t.alloc(cap * HID, s);
+      dz1t.alloc(cap * HID, s);
+      z1.alloc(cap * HID, s);
+      z2.alloc(cap * HID, s);
+      yb.alloc(cap * out_dim, s);
+    }
+  }
+};
+
+int64_t Mlp::param_count(int in_dim, int out_dim) {
+  return (int64_t)HID * in_dim + HID + (int64_t)HID * HID + HID + (int64_t)out_dim * HID + out_dim;
+}
+
+// Split of a batch-row contraction of length K over `tiles` output tiles: the largest power
+// of two that keeps about 128 CTAs and whole 64-row chunks per split.
+static int k_splits(int64_t K, int tiles) {
+  int ks = 1;
+  while ((int64_t)ks * 2 * tiles <= 128 && K % ((int64_t)KC * ks * 2) == 0) ks *= 2;
+  return ks;
+}
+
+static void prepare_all_gemms() {
+  static std::mutex mu;
+  static bool prepared = false;  // the attribute is per function and process-wide
+  std::lock_guard<std::mutex> lock(mu);
+  if (prepared) return;
+  prepare_gemm<64, EPI_BIAS_GELU>();
+  prepare_gemm<64, EPI_GELU_GRAD>();
+  prepare_gemm<256, EPI_F32_ATOMIC>();
+  prepare_gemm<64, EPI_F32_ATOMIC>();
+  prepare_gemm<256, EPI_F32>();
+  prepare_gemm<128, EPI_F32>();
+  prepare_gemm<64, EPI_F32>();
+  prepare_gemm<32, EPI_F32>();
+  prepared = true;
+}
+
+Mlp::Mlp(int in_dim, int out_dim, const float* host_params, cudaStream_t s) : p(nullptr) {
+  if (in_dim < 64 || in_dim % 64 || in_dim > 4096 || out_dim < 1 || out_dim > 4)
+    throw Error(INVALID_ARGUMENT, "MLP input width must be a positive multiple of 64 (at most 4096) and output width 1..4");
+  prepare_all_gemms();
+  p = new Impl;
+  Impl& m = *p;
+  m.in_dim = in_dim;
+  m.out_dim = out_dim;
+  m.s = s;
+  m.o_w1 = 0;
+  m.o_b1 = (int64_t)HID * in_dim;
+  m.o_w2 = m.o_b1 + HID;
+  m.o_b2 = m.o_w2 + (int64_t)HID * HID;
+  m.o_w3 = m.o_b2 + HID;
+  m.o_b3 = m.o_w3 + (int64_t)out_dim * HID;
+  m.P = m.o_b3 + out_dim;
+  try {
+    m.w.alloc(m.P, s);
+    m.m.alloc(m.P, s);
+    m.v.alloc(m.P, s);
+    m.g.alloc(m.P, s);
+    UB_CUDA(cudaMemsetAsync(m.m.p, 0, m.P * 4, s));
+    UB_CUDA(cudaMemsetAsync(m.v.p, 0, m.P * 4, s));
+    UB_CUDA(cudaMemsetAsync(m.g.p, 0, m.P * 4, s));
+    m.w1b.alloc((int64_t)HID * in_dim, s);
+    m.w2b.alloc((int64_t)HID * HID, s);
+    m.w2t.alloc((int64_t)HID * HID, s);
+    m.w3b.alloc((int64_t)out_dim * HID, s);
+    m.err.alloc(1, s);
+    m.step.alloc(1, s);
+    m.loss.alloc(1, s);
+    UB_CUDA(cudaMemsetAsync(m.err.p, 0, 4, s));
+    UB_CUDA(cudaMemsetAsync(m.step.p, 0, 4, s));
+    UB_CUDA(cudaMemsetAsync(m.loss.p, 0, 4, s));
+    set_params(host_params);
+  } catch (...) {
+    delete p;
+    p = nullptr;
+    throw;
+  }
+}
+
+Mlp::~Mlp() { delete p; }
+
+int Mlp::in_dim() const { return p->in_dim; }
+int Mlp::out_dim() const { return p->out_dim; }
+int64_t Mlp::n_params() const { return p->P; }
+
+void Mlp::set_params(const float* host) {
+  Impl& m = *p;
+  cudaStream_t s = m.s;
+  UB_CUDA(cudaMemcpyAsync(m.w.p, host, m.P * 4, cudaMemcpyHostToDevice, s));
+  to_bf16_kernel<<<grid_for(m.w1b.n, 256), 256, 0, s>>>(m.w.p + m.o_w1, m.w1b.n, m.w1b.p, nullptr, m.in_dim);
+  UB_LAUNCH_CHECK();
+  to_bf16_kernel<<<grid_for(m.w2b.n, 256), 256, 0, s>>>(m.w.p + m.o_w2, m.w2b.n, m.w2b.p, m.w2t.p, HID);
+  UB_LAUNCH_CHECK();
+  to_bf16_kernel<<<grid_for(m.w3b.n, 256), 256, 0, s>>>(m.w.p + m.o_w3, m.w3b.n, m.w3b.p, nullptr, HID);
+  UB_LAUNCH_CHECK();
+  UB_CUDA(cudaStreamSynchronize(s));
+}
+
+void Mlp::get_params(float* host) const {
+  UB_CUDA(cudaMemcpyAsync(host, p->w.p, p->P * 4, cudaMemcpyDeviceToHost, p->s));
+  UB_CUDA(cudaStreamSynchronize(p->s));
+}
+
+void Mlp::fit_input_norm(const float* X, int64_t n) {
+  Impl& m = *p;
+  if (n < 1) throw Error(INVALID_ARGUMENT, "input normalisation needs at least one row");
+  m.shift.alloc(m.in_dim, m.s);
+  m.scale.alloc(m.in_dim, m.s);
+  column_stats_kernel<<<m.in_dim, 256, 0, m.s>>>(X, n, m.in_dim, m.shift.p, m.scale.p);
+  UB_LAUNCH_CHECK();
+  UB_CUDA(cudaStreamSynchronize(m.s));
+  m.has_norm = true;
+}
+
+void Mlp::get_input_norm(float* shift, float* scale) const {
+  const Impl& m = *p;
+  if (!m.has_norm) {
+    for (int c = 0; c < m.in_dim; ++c) {
+      shift[c] = 0.0f;
+      scale[c] = 1.0f;
+    }
+    return;
+  }
+  UB_CUDA(cudaMemcpyAsync(shift, m.shift.p, m.in_dim * 4, cudaMemcpyDeviceToHost, m.s));
+  UB_CUDA(cudaMemcpyAsync(scale, m.scale.p, m.in_dim * 4, cudaMemcpyDeviceToHost, m.s));
+  UB_CUDA(cudaStreamSynchronize(m.s));
+}
+
+void Mlp::set_input_norm(const float* shift, const float* scale) {
+  Impl& m = *p;
+  m.shift.alloc(m.in_dim, m.s);
+  m.scale.alloc(m.in_dim, m.s);
+  UB_CUDA(cudaMemcpyAsync(m.shift.p, shift, m.in_dim * 4, cudaMemcpyHostToDevice, m.s));
+  UB_CUDA(cudaMemcpyAsync(m.scale.p, scale, m.in_dim * 4, cudaMemcpyHostToDevice, m.s));
+  UB_CUDA(cudaStreamSynchronize(m.s));
+  m.has_norm = true;
+}
+
+// Forward of one batch of B rows (B % 128 == 0).  With targets Y (training; `rows` selects
+// the batch rows of X and Y) also the backward into g (zeroed here), the loss into `loss`
+// and, with with_adam, the Adam update.  Inference writes y for rows < n_valid.
+static void run_batch(Mlp::Impl& m, const float* X, const uint32_t* rows, int64_t B, int64_t n_valid,
+                      const float* Y, float* y_out, bool with_adam, float lr) {
+  cudaStream_t s = m.s;
+  const bool train = Y != nullptr;
+  const float* shift = m.has_norm ? m.shift.p : nullptr;
+  const float* scale = m.has_norm ? m.scale.p : nullptr;
+  dim3 bg((unsigned)(B / 32), (unsigned)(m.in_dim / 64));
+  batch_kernel<<<bg, 256, 0, s>>>(X, m.in_dim, rows, n_valid, shift, scale, m.xb.p, train ? m.xt.p : nullptr, B, Y,
+                                  m.out_dim, train ? m.yb.p : nullptr, train ? m.g.p : nullptr, train ? m.P : 0,
+                                  with_adam ? m.step.p : nullptr);
+  UB_LAUNCH_CHECK();
+  float* g = m.g.p;
+  EpiArgs e1{};
+  e1.bias = m.w.p + m.o_b1;
+  e1.out_f32 = train ? m.z1.p : nullptr;
+  e1.out_bf16 = m.h1.p;
+  e1.out_t = train ? m.h1t.p : nullptr;
+  e1.ldo = HID;
+  e1.ldt = (int)B;
+  launch_gemm<64, EPI_BIAS_GELU>(m.xb.p, m.in_dim, m.w1b.p, m.in_dim, B, HID, m.in_dim, 1, e1, m.err.p, s);
+  EpiArgs e2{};
+  e2.bias = m.w.p + m.o_b2;
+  e2.out_f32 = train ? m.z2.p : nullptr;
+  e2.out_bf16 = m.h2.p;
+  e2.ldo = HID;
+  launch_gemm<64, EPI_BIAS_GELU>(m.h1.p, HID, m.w2b.p, HID, B, HID, HID, 1, e2, m.err.p, s);
+  const float inv = 1.0f / (float)(B * m.out_dim);
+#define UB_OUT_ARGS                                                                                                  \
+  m.h2.p, m.z2.p, m.w3b.p, m.w.p + m.o_b3, train ? m.yb.p : nullptr, n_valid, inv, y_out, m.dz2.p, m.dz2t.p, B, \
+      g + m.o_w3, g + m.o_b3, g + m.o_b2, m.loss.p
+  const unsigned og = (unsigned)(B / 32);
+  switch (m.out_dim) {
+    case 1: out_layer_kernel<1><<<og, 256, 0, s>>>(UB_OUT_ARGS); break;
+    case 2: out_layer_kernel<2><<<og, 256, 0, s>>>(UB_OUT_ARGS); break;
+    case 3: out_layer_kernel<3><<<og, 256, 0, s>>>(UB_OUT_ARGS); break;
+    default: out_layer_kernel<4><<<og, 256, 0, s>>>(UB_OUT_ARGS); break;
+  }
+#undef UB_OUT_ARGS
+  UB_LAUNCH_CHECK();
+  if (!train) return;
+  // dH1 = dZ2 W2 (B operand W2^T: row i = column i of W2); dZ1 = dH1 * gelu'(Z1), kept
+  // transposed for dW1; db1 = its column sums.
+  EpiArgs e3{};
+  e3.z_in = m.z1.p;
+  e3.out_t = m.dz1t.p;
+  e3.colsum = g + m.o_b1;
+  e3.ldo = HID;
+  e3.ldt = (int)B;
+  launch_gemm<64, EPI_GELU_GRAD>(m.dz2.p, HID, m.w2t.p, HID, B, HID, HID, 1, e3, m.err.p, s);
+  // dW2 = dZ2^T H1 and dW1 = dZ1^T X: contractions over the batch rows, split along the
+  // batch so that each launch has about 128 CTAs.
+  EpiArgs e4{};
+  e4.out_f32 = g + m.o_w2;
+  e4.ldo = HID;
+  launch_gemm<64, EPI_F32_ATOMIC>(m.dz2t.p, B, m.h1t.p, B, HID, HID, B, k_splits(B, (HID / GM) * (HID / 64)), e4,
+                                  m.err.p, s);
+  EpiArgs e5{};
+  e5.out_f32 = g + m.o_w1;
+  e5.ldo = m.in_dim;
+  launch_gemm<64, EPI_F32_ATOMIC>(m.dz1t.p, B, m.xt.p, B, HID, m.in_dim, B, k_splits(B, (HID / GM) * (m.in_dim / 64)),
+                                  e5, m.err.p, s);
+  if (!with_adam) return;
+  AdamArgs a{};
+  a.w = m.w.p;
+  a.m = m.m.p;
+  a.v = m.v.p;
+  a.g = m.g.p;
+  a.n = m.P;
+  a.lr = lr;
+  a.b1 = 0.9f;
+  a.b2 = 0.999f;
+  a.eps = 1e-8f;
+  a.step = m.step.p;
+  a.o_w1 = m.o_w1;
+  a.o_w2 = m.o_w2;
+  a.o_w3 = m.o_w3;
+  a.n_w1 = (int64_t)HID * m.in_dim;
+  a.n_w3 = (int64_t)m.out_dim * HID;
+  a.w1b = m.w1b.p;
+  a.w2b = m.w2b.p;
+  a.w2t = m.w2t.p;
+  a.w3b = m.w3b.p;
+  adam_kernel<<<grid_for(m.P, 256), 256, 0, s>>>(a);
+  UB_LAUNCH_CHECK();
+}
+
+void Mlp::gradients(const float* X, const float* Y, int64_t B, float* host_grads, float* loss_out) {
+  Impl& m = *p;
+  if (B < 128 || B % 128) throw Error(INVALID_ARGUMENT, "batch rows must be a positive multiple of 128");
+  if (B > (1 << 24)) throw Error(INVALID_ARGUMENT, "at most 16777216 rows per gradient batch");
+  m.ensure(B, true);
+  std::vector<uint32_t> ident(B);
+  for (int64_t i = 0; i < B; ++i) ident[i] = (uint32_t)i;
+  DevBuf<uint32_t> rows(B, m.s);
+  UB_CUDA(cudaMemcpyAsync(rows.p, ident.data(), B * 4, cudaMemcpyHostToDevice, m.s));
+  UB_CUDA(cudaMemsetAsync(m.loss.p, 0, 4, m.s));
+  run_batch(m, X, rows.p, B, B, Y, nullptr, false, 0.0f);
+  UB_CUDA(cudaMemcpyAsync(host_grads, m.g.p, m.P * 4, cudaMemcpyDeviceToHost, m.s));
+  UB_CUDA(cudaMemcpyAsync(loss_out, m.loss.p, 4, cudaMemcpyDeviceToHost, m.s));
+  check_error();
+}
+
+void Mlp::train(const float* X, const float* Y, int64_t n, int epochs, int64_t batch, float lr, uint64_t seed,
+                float* losses) {
+  Impl& m = *p;
+  cudaStream_t s = m.s;
+  if (batch < 128 || batch % 128 || batch > (1 << 24))
+    throw Error(INVALID_ARGUMENT, "batch must be a positive multiple of 128 (at most 16777216)");
+  if (epochs < 0) throw Error(INVALID_ARGUMENT, "epochs must be >= 0");
+  if (n > 0xFFFFFFFFll) throw Error(INVALID_ARGUMENT, "at most 2^32 - 1 training rows");
+  const int64_t steps = n / batch;  // the last partial batch of each shuffled epoch is dropped
+  if (steps < 1) throw Error(INVALID_ARGUMENT, "fewer training rows than one batch");
+  if (epochs == 0) return;
+  m.ensure(batch, true);
+  // Shuffles: Fisher-Yates driven by splitmix64(seed), one permutation per epoch, uploaded once.
+  const int64_t per_epoch = steps * batch;
+  std::vector<uint32_t> perm((size_t)epochs * per_epoch);
+  std::vector<uint32_t> p0(n);
+  uint64_t st = seed;
+  auto next = [&]() {
+    uint64_t z = (st += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+  };
+  for (int e = 0; e < epochs; ++e) {
+    for (int64_t i = 0; i < n; ++i) p0[i] = (uint32_t)i;
+    for (int64_t i = n - 1; i > 0; --i) std::swap(p0[i], p0[(int64_t)(next() % (uint64_t)(i + 1))]);
+    std::copy(p0.begin(), p0.begin() + per_epoch, perm.begin() + (size_t)e * per_epoch);
+  }
+  DevBuf<uint32_t> dperm(perm.size(), s), cur(per_epoch, s);
+  DevBuf<float> dloss(epochs, s);
+  UB_CUDA(cudaMemcpyAsync(dperm.p, perm.data(), perm.size() * 4, cudaMemcpyHostToDevice, s));
+  auto one_epoch = [&]() {
+    for (int64_t t = 0; t < steps; ++t) run_batch(m, X, cur.p + t * batch, batch, batch, Y, nullptr, true, lr);
+  };
+  cudaGraphExec_t exec = nullptr;
+  if (graphs_enabled()) {
+    cudaGraph_t graph = nullptr;
+    UB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    try {
+      one_epoch();
+    } catch (...) {
+      cudaGraph_t g2 = nullptr;
+      (void)cudaStreamEndCapture(s, &g2);
+      if (g2) (void)cudaGraphDestroy(g2);
+      throw;
+    }
+    UB_CUDA(cudaStreamEndCapture(s, &graph));
+    const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+    (void)cudaGraphDestroy(graph);
+    UB_CUDA(ie);
+  }
+  struct ExecGuard {
+    cudaGraphExec_t e;
+    ~ExecGuard() {
+      if (e) (void)cudaGraphExecDestroy(e);
+    }
+  } guard{exec};
+  const uint64_t launches_per_epoch = (uint64_t)steps * 8;
+  for (int e = 0; e < epochs; ++e) {
+    UB_CUDA(cudaMemcpyAsync(cur.p, dperm.p + (int64_t)e * per_epoch, per_epoch * 4, cudaMemcpyDeviceToDevice, s));
+    UB_CUDA(cudaMemsetAsync(m.loss.p, 0, 4, s));
+    if (exec) {
+      UB_CUDA(cudaGraphLaunch(exec, s));
+      for (uint64_t i = 0; i < launches_per_epoch; ++i) count_launch();
+    } else {
+      one_epoch();
+    }
+    UB_CUDA(cudaMemcpyAsync(dloss.p + e, m.loss.p, 4, cudaMemcpyDeviceToDevice, s));
+  }
+  std::vector<float> hl(epochs);
+  UB_CUDA(cudaMemcpyAsync(hl.data(), dloss.p, epochs * 4, cudaMemcpyDeviceToHost, s));
+  check_error();
+  if (losses)
+    for (int e = 0; e < epochs; ++e) losses[e] = hl[e] / (float)steps;
+}
+
+void Mlp::predict(const float* X, int64_t n, float* Y) {
+  Impl& m = *p;
+  if (n < 1) return;
+  const int64_t tile = 131072;
+  m.ensure(std::min<int64_t>(tile, (n + 127) / 128 * 128), false);
+  for (int64_t r0 = 0; r0 < n; r0 += tile) {
+    const int64_t rows = std::min(tile, n - r0);
+    const int64_t padded = (rows + 127) / 128 * 128;
+    run_batch(m, X + r0 * m.in_dim, nullptr, padded, rows, nullptr, Y + r0 * m.out_dim, false, 0.0f);
+  }
+  check_error();
+}
+
+void Mlp::check_error() {
+  unsigned e = 0;
+  UB_CUDA(cudaMemcpyAsync(&e, p->err.p, 4, cudaMemcpyDeviceToHost, p->s));
+  UB_CUDA(cudaStreamSynchronize(p->s));
+  if (e) throw Error(CUDA, "tensor-core MMA completion wait timed out");
+}
+
+// Standalone tensor-core GEMM: C[M,N] (f32) = A[M,K] B[N,K]^T with bf16 A, B, both K-major.
+// ksplit > 1 accumulates split-K partial sums into C with atomics (C must be zeroed).
+void umma_gemm_f32(const void* A, const void* B, float* C, int64_t M, int64_t N, int64_t K, int ksplit,
+                   cudaStream_t s) {
+  prepare_all_gemms();
+  if (N > (1 << 30) || K > (1 << 30)) throw Error(INVALID_ARGUMENT, "GEMM dimension too large");
+  DevBuf<unsigned> err(1, s);
+  UB_CUDA(cudaMemsetAsync(err.p, 0, 4, s));
+  EpiArgs ep{};
+  ep.out_f32 = C;
+  ep.ldo = (int)N;
+  const bf16* a = static_cast<const bf16*>(A);
+  const bf16* b = static_cast<const bf16*>(B);
+  if (ksplit > 1) {
+    if (N % 256 == 0) launch_gemm<256, EPI_F32_ATOMIC>(a, K, b, K, M, N, K, ksplit, ep, err.p, s);
+    else if (N % 64 == 0) launch_gemm<64, EPI_F32_ATOMIC>(a, K, b, K, M, N, K, ksplit, ep, err.p, s);
+    else throw Error(INVALID_ARGUMENT, "split-K GEMM needs N % 64 == 0");
+  } else if (N % 256 == 0) {
+    launch_gemm<256, EPI_F32>(a, K, b, K, M, N, K, 1, ep, err.p, s);
+  } else if (N % 128 == 0) {
+    launch_gemm<128, EPI_F32>(a, K, b, K, M, N, K, 1, ep, err.p, s);
+  } else if (N % 64 == 0) {
+    launch_gemm<64, EPI_F32>(a, K, b, K, M, N, K, 1, ep, err.p, s);
+  } else if (N % 32 == 0) {
+    launch_gemm<32, EPI_F32>(a, K, b, K, M, N, K, 1, ep, err.p, s);
+  } else {
+    throw Error(INVALID_ARGUMENT, "GEMM N must be a multiple of 32");
+  }
+  unsigned e = 0;
+  UB_CUDA(cudaMemcpyAsync(&e, err.p, 4, cudaMemcpyDeviceToHost, s));
+  UB_CUDA(cudaStreamSynchronize(s));
+  if (e) throw Error(CUDA, "tensor-core MMA completion wait timed out");
+}
+
+}  // namespace ub

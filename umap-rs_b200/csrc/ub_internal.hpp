@@ -243,4 +243,43 @@ void schedule_totals(const SgdLayout& L, uint32_t neg_rate, uint32_t start, uint
 void nan_empty_rows(const uint64_t* indptr, uint64_t n, uint32_t dim, float* emb,
                     cudaStream_t s);
 
+// ---------------------------------------------------------------- warm-start MLP (mlp.cu)
+// in -> 256 -> 256 -> out network with GELU, bf16 weights/activations, fp32 accumulation.
+// Flat fp32 parameters in the order W1 [256, in], b1 [256], W2 [256, 256], b2 [256],
+// W3 [out, 256], b3 [out] (weights row-major, one row per output unit).  All X / Y pointers
+// are device memory; X rows are `in` floats, Y rows `out` floats.
+class Mlp {
+ public:
+  struct Impl;
+  Mlp(int in_dim, int out_dim, const float* host_params, cudaStream_t s);
+  ~Mlp();
+  Mlp(const Mlp&) = delete;
+  Mlp& operator=(const Mlp&) = delete;
+  static int64_t param_count(int in_dim, int out_dim);
+  int in_dim() const;
+  int out_dim() const;
+  int64_t n_params() const;
+  void set_params(const float* host);
+  void get_params(float* host) const;
+  // Input standardisation x' = (x - shift) * scale applied before the first layer.
+  void fit_input_norm(const float* X, int64_t n);
+  void set_input_norm(const float* shift, const float* scale);
+  void get_input_norm(float* shift, float* scale) const;
+  // Forward + backward of one batch (rows % 128 == 0) without an update: gradients of the
+  // mean squared error (flat layout, host) and the loss.
+  void gradients(const float* X, const float* Y, int64_t rows, float* host_grads, float* loss);
+  // Adam training over shuffled batches; per-epoch mean loss into losses[epochs] (host).
+  void train(const float* X, const float* Y, int64_t n, int epochs, int64_t batch, float lr,
+             uint64_t seed, float* losses);
+  void predict(const float* X, int64_t n, float* Y);
+  void check_error();
+
+ private:
+  Impl* p;
+};
+// C[M,N] (f32, device) = A[M,K] B[N,K]^T, bf16 operands both K-major, on the tensor cores.
+// M % 128, N % 32, K % (64 * ksplit); ksplit > 1 adds into C with atomics.
+void umma_gemm_f32(const void* A, const void* B, float* C, int64_t M, int64_t N, int64_t K, int ksplit,
+                   cudaStream_t s);
+
 }  // namespace ub

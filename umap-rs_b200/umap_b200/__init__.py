@@ -414,6 +414,26 @@ class Umap:
         return FittedUmap(out.value)
 
 
+    def fit_manifold(self, manifold: "LearnedManifold", init) -> "FittedUmap":
+        """embedding.rs:299-337: `fit` after its learn_manifold step.  Consumes `manifold`."""
+        L = _lib.load()
+        if self.output_metric.metric_type() != MetricType.Euclidean:
+            raise UmapError(ERR_UNSUPPORTED, "MetricType::Generic output metrics are not implemented "
+                                             "on the GPU path")
+        cfg = self._cfg()
+        irows, icols = int(init.shape[0]), int(init.shape[1])
+        mh = manifold._take()
+        out = C.c_void_p()
+        if _is_cuda_tensor(init):
+            import torch
+            tn, pn = _device(init, torch.float32)
+            _check(L.umap_fit_manifold_device(mh, C.byref(cfg), pn, irows, icols, C.byref(out)))
+        else:
+            an, pn = _host(init, np.float32)
+            _check(L.umap_fit_manifold(mh, C.byref(cfg), pn, irows, icols, C.byref(out)))
+        return FittedUmap(out.value)
+
+
 # ------------------------------------------------------------------ Optimizer (optimizer.rs)
 class Optimizer(_Handle):
     _free = "umap_optimizer_free"
@@ -600,3 +620,7 @@ class FittedUmap(_Handle):
     @staticmethod
     def from_bytes(b: bytes) -> "FittedUmap":
         return FittedUmap(_deserialize("umap_fitted_deserialize", b))
+
+
+# ------------------------------------------------------------------ learned warm start
+from .warm_start import Mlp, gemm_bf16, init_params as mlp_init_params, warm_start_fit  # noqa: E402

@@ -85,6 +85,21 @@ SIGNATURES = {
     "umap_radix_sort_pairs_device": [P, P, P, P, u64, i32],
     "umap_radix_sort_pairs_device_noalloc": [P, P, P, P, u64, i32, P],
     "umap_radix_sort_noalloc_max_pairs": [C.POINTER(u64)],
+    "umap_fit_manifold": [P, C.POINTER(UmapConfigC), P, u64, u64, PP],
+    "umap_fit_manifold_device": [P, C.POINTER(UmapConfigC), P, u64, u64, PP],
+    "umap_mlp_param_count": [u64, u64, C.POINTER(u64)],
+    "umap_mlp_new": [u64, u64, P, PP],
+    "umap_mlp_dims": [P, C.POINTER(u64), C.POINTER(u64)],
+    "umap_mlp_get_params": [P, P],
+    "umap_mlp_set_params": [P, P],
+    "umap_mlp_fit_input_norm_device": [P, P, u64],
+    "umap_mlp_input_norm": [P, P, P],
+    "umap_mlp_set_input_norm": [P, P, P],
+    "umap_mlp_gradients_device": [P, P, P, u64, P, C.POINTER(f32)],
+    "umap_mlp_train_device": [P, P, P, u64, u64, u64, f32, u64, P],
+    "umap_mlp_predict_device": [P, P, u64, P],
+    "umap_mlp_free": [P],
+    "umap_gemm_bf16_device": [P, P, P, u64, u64, u64, u64],
 }
 
 _lib = None

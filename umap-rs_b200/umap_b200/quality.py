@@ -40,6 +40,7 @@ def _nn_lowdim_torch(emb: np.ndarray, rows: np.ndarray, m: int, chunk: int = 409
     sq = (e * e).sum(1)
     rr = torch.from_numpy(rows).cuda()
     out = torch.empty((len(rows), m), dtype=torch.int64, device="cuda")
+    chunk = max(1, min(chunk, int(4e9 // (8 * e.shape[0]))))  # distance block of at most ~4 GB
     for s in range(0, len(rows), chunk):
         r = rr[s:s + chunk]
         D = sq[r, None] + sq[None, :] - 2.0 * (e[r] @ e.T)
@@ -99,3 +100,56 @@ def fuzzy_cross_entropy(emb: np.ndarray, head: np.ndarray, tail: np.ndarray, wei
     keep = (ri != rj) & ~(np.isnan(emb[ri]).any(1) | np.isnan(emb[rj]).any(1))
     qr = q_of(ri[keep], rj[keep])
     return float(pos.sum() + neg.sum() + (-np.log(1.0 - qr)).sum())
+
+
+def fuzzy_cross_entropy_torch(emb, head, tail, weight, a: float, b: float, neg_factor: int = 5, seed: int = 0,
+                              chunk: int = 1 << 24) -> float:
+    """``fuzzy_cross_entropy`` evaluated on the GPU in float64 (same definition; the random
+    pairs come from a seeded torch generator, so the value differs from the numpy scorer's
+    by the sampling of the non-edge pairs only)."""
+    import torch
+    dev = "cuda"
+    e = torch.as_tensor(np.asarray(emb) if not hasattr(emb, "is_cuda") else emb).to(dev, torch.float64)
+    h = torch.as_tensor(np.asarray(head, np.int64) if not hasattr(head, "is_cuda") else head).to(dev, torch.int64)
+    t = torch.as_tensor(np.asarray(tail, np.int64) if not hasattr(tail, "is_cuda") else tail).to(dev, torch.int64)
+    w = torch.as_tensor(np.asarray(weight) if not hasattr(weight, "is_cuda") else weight).to(dev, torch.float64)
+    bad = torch.isnan(e).any(1)
+    ok = ~(bad[h] | bad[t])
+    h, t, w = h[ok], t[ok], w[ok]
+
+    def q_of(i, j):
+        d2 = ((e[i] - e[j]) ** 2).sum(1)
+        return torch.clamp(1.0 / (1.0 + a * torch.pow(d2, b)), EPS, 1.0 - EPS)
+
+    total = 0.0
+    for s in range(0, h.numel(), chunk):
+        q = q_of(h[s:s + chunk], t[s:s + chunk])
+        ww = w[s:s + chunk]
+        pos = torch.where(ww > 0, ww * torch.log(torch.clamp(ww, EPS, 1.0) / q), torch.zeros_like(q))
+        neg = torch.where(ww < 1, (1 - ww) * torch.log(torch.clamp(1 - ww, EPS, 1.0) / (1 - q)), torch.zeros_like(q))
+        total += float(pos.sum() + neg.sum())
+    g = torch.Generator(device=dev).manual_seed(seed)
+    n = e.shape[0]
+    m = neg_factor * h.numel()
+    for s in range(0, m, chunk):
+        c = min(chunk, m - s)
+        ri = torch.randint(0, n, (c,), device=dev, generator=g)
+        rj = torch.randint(0, n, (c,), device=dev, generator=g)
+        keep = (ri != rj) & ~(bad[ri] | bad[rj])
+        total += float((-torch.log(1.0 - q_of(ri[keep], rj[keep]))).sum())
+    return total
+
+
+def pruned_edges(manifold, total_epochs: int):
+    """(head, tail, weight) of the graph edges an optimiser for `total_epochs` keeps
+    (weight >= max weight / total_epochs, or the 500 / 200 default when total_epochs <= 10;
+    optimizer.rs:90-117), as host arrays."""
+    g = manifold.graph()
+    indptr = np.asarray(g.indptr, np.int64)
+    w = np.asarray(g.data, np.float32)
+    n = len(indptr) - 1
+    epochs = total_epochs if total_epochs > 10 else (500 if n <= 10000 else 200)
+    thr = np.float32(max(float(w.max()), 0.0) / np.float32(epochs)) if w.size else np.float32(0)
+    keep = w >= thr
+    head = np.repeat(np.arange(len(indptr) - 1, dtype=np.int64), np.diff(indptr))
+    return head[keep], np.asarray(g.indices, np.int64)[keep], w[keep]

@@ -5,16 +5,23 @@
 //
 // Tensor-core GEMM.  C[M,N] = A[M,K] * B[N,K]^T with A and B BF16, both K-major (row-major,
 // K contiguous), FP32 accumulation in tensor memory.  One CTA (4 warps) owns a 128 x BN
-// output tile and a K range (blockIdx.z splits K; split partial sums are added with
-// atomics).  Warp 0 allocates BN tensor-memory columns.  K is staged 64 at a time into shared
-// memory in the canonical no-swizzle K-major layout: 8-row x 16-byte core matrices, element
-// (r, k) of a 64-wide chunk at byte (r/8)*1024 + (k/8)*128 + (r%8)*16 + (k%8)*2, so the
-// descriptor of MMA step s (k = 16s..16s+15) starts at +256*s with leading byte offset 128
-// (the next 8 k) and stride byte offset 1024 (the next 8 rows).  One thread issues the four
-// tcgen05.mma (M=128, N=BN, K=16) of a chunk and commits them to an mbarrier; all threads
-// wait on it (bounded by a timer) before the chunk buffer is refilled.  The epilogue reads
-// the accumulator with tcgen05.ld (warp w owns rows 32w..32w+31, thread = row) and fuses
-// bias, GELU, the GELU derivative, column sums and transposed copies.
+// output tile and a K range (blockIdx.z splits K).  Warp 0 allocates BN tensor-memory
+// columns.  K is staged 64 at a time into shared memory in the canonical no-swizzle K-major
+// layout: 8-row x 16-byte core matrices, element (r, k) of a 64-wide chunk at byte
+// (r/8)*1024 + (k/8)*128 + (r%8)*16 + (k%8)*2, so the descriptor of MMA step s
+// (k = 16s..16s+15) starts at +256*s with leading byte offset 128 (the next 8 k) and stride
+// byte offset 1024 (the next 8 rows).  Two stages: while the four tcgen05.mma (M=128, N=BN,
+// K=16) of chunk c run, the threads stage chunk c+1; one thread issues the MMAs and commits
+// them to the stage's mbarrier, and a stage is refilled only after its MMAs completed (every
+// wait bounded by a timer).  The epilogue reads the accumulator with tcgen05.ld (warp w owns
+// rows 32w..32w+31, thread = row) and fuses bias, GELU, the GELU derivative, column sums and
+// transposed copies.  The first layer's A operand is gathered straight from the fp32 input
+// rows (standardised, rounded to bf16) by the staging threads.
+//
+// One training step (batch B): L1 GEMM (gather) -> L2 GEMM -> output layer + loss + its
+// backward (CUDA cores) -> { dH1 GEMM (GELU derivative, db1) -> dW1 GEMM } || dW2 GEMM on a
+// second stream -> Adam.  The dW GEMMs contract over the batch in K splits whose partial sums
+// are stored to separate slices and summed by the Adam kernel.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -37,7 +44,7 @@ constexpr int GT = 128;   // threads per GEMM CTA
 constexpr int HID = 256;  // hidden width
 
 enum Epi : int {
-  EPI_F32 = 0,         // out_f32 = acc (+ bias)
+  EPI_F32 = 0,         // out_f32 (slice blockIdx.z) = acc (+ bias)
   EPI_F32_ATOMIC = 1,  // out_f32 += acc (split-K partial sums)
   EPI_BIAS_GELU = 2,   // z = acc + bias -> out_f32 (if set); h = gelu(z) -> out_bf16 (+ out_t)
   EPI_GELU_GRAD = 3,   // d = acc * gelu'(z_in) -> out_bf16 / out_t (if set); colsum += sum_rows d
@@ -46,11 +53,26 @@ enum Epi : int {
 struct EpiArgs {
   const float* bias;
   float* out_f32;
+  int64_t split_stride;  // EPI_F32: elements between the slices of K splits
   const float* z_in;
   bf16* out_bf16;
-  bf16* out_t;   // transposed copy [N, ldt]
+  bf16* out_t;  // transposed copy [N, ldt]
   float* colsum;
   int ldo, ldt;
+};
+
+// First-layer A operand gathered from fp32 rows: A[r] = bf16((X[src(r)] - shift) * scale) with
+// src(r) = rows[r] (training) or min(r, n_valid - 1) (inference, padded tail).  CTAs with
+// blockIdx.y == 0 also write the transposed copy xt [K, ldt] (for dW1).
+struct GatherA {
+  const float* X;
+  int ldx;
+  const uint32_t* rows;
+  int64_t n_valid;
+  const float* shift;
+  const float* scale;
+  bf16* xt;
+  int64_t ldt;
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -109,14 +131,15 @@ __device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
   return *reinterpret_cast<const uint32_t*>(&h);
 }
 
-template <int BN, int EPI>
+template <int BN, int EPI, bool GATHER>
 __global__ void __launch_bounds__(GT) umma_gemm_kernel(const bf16* __restrict__ A, int lda,
                                                        const bf16* __restrict__ B, int ldb, int k_per_cta,
-                                                       EpiArgs ep, unsigned* __restrict__ err) {
+                                                       EpiArgs ep, GatherA ga, unsigned* __restrict__ err) {
   // UMMA with M=128 takes N % 16 == 0 up to 256; the epilogue reads 32 columns at a time.
   static_assert(BN % 32 == 0 && BN >= 32 && BN <= 256, "tile width");
   constexpr uint32_t TCOLS = BN <= 32 ? 32 : BN <= 64 ? 64 : BN <= 128 ? 128 : 256;
   constexpr int STAGE = (GM + BN) * KC * 2;  // bytes of one K chunk of A and B
+  static_assert(STAGE >= 4 * 32 * 33 * 4, "epilogue reduction scratch reuses a stage");
   extern __shared__ __align__(1024) uint8_t smem[];  // two stages: [A | B] [A | B]
   __shared__ __align__(8) uint64_t mbar[2];          // MMA completion, one per stage
   __shared__ uint32_t tmem_base;
@@ -145,11 +168,40 @@ __global__ void __launch_bounds__(GT) umma_gemm_kernel(const bf16* __restrict__ 
     const int64_t kg = k_begin + (int64_t)c * KC;
     uint8_t* sA = smem + st * STAGE;
     uint8_t* sB = sA + GM * KC * 2;
+    if (GATHER) {
+      // consecutive threads take consecutive rows: the transposed copy is written coalesced
+#pragma unroll 2
+      for (int v = tid; v < GM * (KC / 8); v += GT) {
+        const int r = v & (GM - 1), c8 = v / GM;
+        const int64_t b = m0 + r;
+        const int64_t src = ga.rows ? (int64_t)ga.rows[b] : (b < ga.n_valid ? b : ga.n_valid - 1);
+        const int64_t k0 = kg + c8 * 8;
+        const float4* xp = reinterpret_cast<const float4*>(ga.X + src * ga.ldx + k0);
+        const float4 x0 = __ldg(xp), x1 = __ldg(xp + 1);
+        float f[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
+        if (ga.scale) {
+#pragma unroll
+          for (int e = 0; e < 8; ++e) f[e] = (f[e] - __ldg(ga.shift + k0 + e)) * __ldg(ga.scale + k0 + e);
+        }
+        uint32_t pk[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) pk[e] = pack_bf16(f[2 * e], f[2 * e + 1]);
+        *reinterpret_cast<uint4*>(sA + (r >> 3) * (KC * 16) + c8 * 128 + (r & 7) * 16) =
+            make_uint4(pk[0], pk[1], pk[2], pk[3]);
+        if (ga.xt && blockIdx.y == 0) {
+          uint16_t* t = reinterpret_cast<uint16_t*>(ga.xt);
+#pragma unroll
+          for (int e = 0; e < 8; ++e)
+            t[(k0 + e) * ga.ldt + b] = (uint16_t)((e & 1) ? (pk[e >> 1] >> 16) : (pk[e >> 1] & 0xFFFFu));
+        }
+      }
+    } else {
 #pragma unroll 4
-    for (int v = tid; v < GM * (KC / 8); v += GT) {
-      const int r = v >> 3, c8 = v & 7;
-      const uint4 x = __ldg(reinterpret_cast<const uint4*>(A + (m0 + r) * lda + kg + c8 * 8));
-      *reinterpret_cast<uint4*>(sA + (r >> 3) * (KC * 16) + c8 * 128 + (r & 7) * 16) = x;
+      for (int v = tid; v < GM * (KC / 8); v += GT) {
+        const int r = v >> 3, c8 = v & 7;
+        const uint4 x = __ldg(reinterpret_cast<const uint4*>(A + (m0 + r) * lda + kg + c8 * 8));
+        *reinterpret_cast<uint4*>(sA + (r >> 3) * (KC * 16) + c8 * 128 + (r & 7) * 16) = x;
+      }
     }
 #pragma unroll 4
     for (int v = tid; v < BN * (KC / 8); v += GT) {
@@ -234,7 +286,8 @@ __global__ void __launch_bounds__(GT) umma_gemm_kernel(const bf16* __restrict__ 
 #pragma unroll
           for (int j = 0; j < 32; ++j) v[j] += __ldg(ep.bias + cb + j);
         }
-        float4* o = reinterpret_cast<float4*>(ep.out_f32 + row * ep.ldo + cb);
+        float* base = ep.out_f32 + (EPI == EPI_F32 ? (int64_t)blockIdx.z * ep.split_stride : 0);
+        float4* o = reinterpret_cast<float4*>(base + row * ep.ldo + cb);
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
           const float4 x = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
@@ -263,13 +316,17 @@ __global__ void __launch_bounds__(GT) umma_gemm_kernel(const bf16* __restrict__ 
             v[4 * q + 3] *= gelu_grad(z.w);
           }
           if (ep.colsum) {
+            // column sums over the warp's 32 rows through shared memory (the K stages are
+            // free once the MMAs completed), one atomic per column per warp
+            float* red = reinterpret_cast<float*>(smem) + warp * (32 * 33);
 #pragma unroll
-            for (int j = 0; j < 32; ++j) {
-              float s = v[j];
-#pragma unroll
-              for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xFFFFFFFFu, s, o);
-              if (lane == 0) atomicAdd(ep.colsum + cb + j, s);
-            }
+            for (int j = 0; j < 32; ++j) red[lane * 33 + j] = v[j];
+            __syncwarp();
+            float sum = 0.0f;
+#pragma unroll 8
+            for (int rr = 0; rr < 32; ++rr) sum += red[rr * 33 + lane];
+            atomicAdd(ep.colsum + cb + lane, sum);
+            __syncwarp();
           }
         }
         uint32_t pk[16];
@@ -295,104 +352,69 @@ __global__ void __launch_bounds__(GT) umma_gemm_kernel(const bf16* __restrict__ 
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(taddr), "r"(TCOLS) : "memory");
 }
 
-template <int BN, int EPI>
+template <int BN>
 constexpr size_t gemm_smem() {
   return (size_t)2 * (GM + BN) * KC * 2;
 }
 
-template <int BN, int EPI>
+template <int BN, int EPI, bool GATHER = false>
 void prepare_gemm() {
-  UB_CUDA(cudaFuncSetAttribute(umma_gemm_kernel<BN, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)gemm_smem<BN, EPI>()));
+  UB_CUDA(cudaFuncSetAttribute(umma_gemm_kernel<BN, EPI, GATHER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)gemm_smem<BN>()));
 }
 
-// C = A[M,K] B[N,K]^T with the K range split into `ksplit` equal parts (EPI_F32_ATOMIC only).
-template <int BN, int EPI>
+// C = A[M,K] B[N,K]^T, the K range split into `ksplit` equal parts: EPI_F32 stores each
+// part's sum to its own slice (ep.split_stride apart), EPI_F32_ATOMIC adds them up.
+template <int BN, int EPI, bool GATHER = false>
 void launch_gemm(const bf16* A, int64_t lda, const bf16* B, int64_t ldb, int64_t M, int64_t N, int64_t K,
-                 int ksplit, const EpiArgs& ep, unsigned* err, cudaStream_t s) {
+                 int ksplit, const EpiArgs& ep, unsigned* err, cudaStream_t s, const GatherA* ga = nullptr) {
   if (M <= 0 || M % GM || N % BN || K <= 0 || ksplit < 1 || K % ((int64_t)KC * ksplit) || lda % 8 || ldb % 8 ||
-      M / GM > 0x7FFFFFFF || lda > 0x7FFFFFFF || ldb > 0x7FFFFFFF)
+      M / GM > 0x7FFFFFFF || lda > 0x7FFFFFFF || ldb > 0x7FFFFFFF || ksplit > 65535)
     throw Error(INVALID_ARGUMENT, "tensor-core GEMM shape: M % 128, N % tile, K % (64 * splits), rows of 16 bytes");
-  if (ksplit > 1 && EPI != EPI_F32_ATOMIC) throw Error(INVALID_ARGUMENT, "split K needs the atomic epilogue");
+  if (ksplit > 1 && !(EPI == EPI_F32_ATOMIC || (EPI == EPI_F32 && ep.split_stride > 0)))
+    throw Error(INVALID_ARGUMENT, "split K needs per-split output slices or the atomic epilogue");
+  if (GATHER && (!ga || ga->ldx % 4)) throw Error(INVALID_ARGUMENT, "gathered rows must be 16-byte aligned");
+  GatherA g{};
+  if (ga) g = *ga;
   dim3 grid((unsigned)(M / GM), (unsigned)(N / BN), (unsigned)ksplit);
-  umma_gemm_kernel<BN, EPI><<<grid, GT, gemm_smem<BN, EPI>(), s>>>(A, (int)lda, B, (int)ldb, (int)(K / ksplit), ep,
-                                                                   err);
+  umma_gemm_kernel<BN, EPI, GATHER><<<grid, GT, gemm_smem<BN>(), s>>>(A, (int)lda, B, (int)ldb, (int)(K / ksplit),
+                                                                      ep, g, err);
   UB_LAUNCH_CHECK();
 }
 
 // ------------------------------------------------------------------------------ CUDA-core parts
-// Batch assembly.  Block (bx, by) handles batch rows 32bx..32bx+31 and input columns
-// 64by..64by+63: xb[b] = bf16((X[src(b)] - shift) * scale) row-major and, when xt is set, its
-// transpose xt [in, ldt].  src(b) = rows[b] (training) or min(b, n_valid - 1) (inference,
-// padded tail).  Blocks with by == 0 gather the targets; all blocks zero `zero[0..n_zero)`
-// and block (0, 0) advances the Adam step counter.
-__global__ void __launch_bounds__(256) batch_kernel(
-    const float* __restrict__ X, int in_dim, const uint32_t* __restrict__ rows, int64_t n_valid,
-    const float* __restrict__ shift, const float* __restrict__ scale, bf16* __restrict__ xb, bf16* __restrict__ xt,
-    int64_t ldt, const float* __restrict__ Y, int out_dim, float* __restrict__ yb, float* __restrict__ zero,
-    int64_t n_zero, unsigned* __restrict__ step) {
-  __shared__ uint16_t tile[64][34];
-  const int tid = threadIdx.x;
-  const int64_t b0 = (int64_t)blockIdx.x * 32;
-  const int c0 = blockIdx.y * 64;
-  for (int e = tid; e < 32 * 64; e += 256) {
-    const int r = e >> 6, c = e & 63;
-    const int64_t b = b0 + r;
-    const int64_t src = rows ? (int64_t)rows[b] : std::min<int64_t>(b, n_valid - 1);
-    float x = X[src * in_dim + c0 + c];
-    if (scale) x = (x - shift[c0 + c]) * scale[c0 + c];
-    const bf16 h = __float2bfloat16_rn(x);
-    xb[b * in_dim + c0 + c] = h;
-    tile[c][r] = *reinterpret_cast<const uint16_t*>(&h);
-  }
-  if (Y && blockIdx.y == 0 && tid < 32 * out_dim) {
-    const int r = tid / out_dim, j = tid - r * out_dim;
-    yb[(b0 + r) * out_dim + j] = Y[(int64_t)rows[b0 + r] * out_dim + j];
-  }
-  if (zero) {
-    const int64_t nb = (int64_t)gridDim.x * gridDim.y;
-    const int64_t bid = (int64_t)blockIdx.y * gridDim.x + blockIdx.x;
-    for (int64_t i = bid * 256 + tid; i < n_zero; i += nb * 256) zero[i] = 0.0f;
-    if (step && bid == 0 && tid == 0) *step += 1u;
-  }
-  if (!xt) return;
-  __syncthreads();
-  uint16_t* t = reinterpret_cast<uint16_t*>(xt);
-  for (int e = tid; e < 32 * 64; e += 256) {
-    const int c = e >> 5, r = e & 31;
-    t[(int64_t)(c0 + c) * ldt + b0 + r] = tile[c][r];
-  }
-}
-
-// Output layer (256 -> OUT) on CUDA cores, one warp per row, 32 rows per block; lane l owns
-// hidden columns 8l..8l+7.  y = h2 W3^T + b3.  With a target it also runs the loss and the
-// backward of this layer: e = y - t; loss += sum e^2 / count; dy = 2 e / count;
-// dz2 = (dy W3) * gelu'(z2) -> bf16 row-major and transposed [256, ldt]; dW3 += dy^T h2;
-// db3 += sum dy; db2 += sum dz2 (fp32, before rounding).
+// Output layer (256 -> OUT) on CUDA cores, one warp per row, 32 rows per block (4 per warp);
+// lane l owns hidden columns 8l..8l+7.  y = h2 W3^T + b3.  With targets it also runs the loss
+// and this layer's backward: t = Y[rows[b]]; e = y - t; loss += sum e^2 / count;
+// dy = 2 e / count; dz2 = (dy W3) * gelu'(z2) -> bf16 row-major and transposed [256, ldt];
+// dW3 += dy^T h2; db3 += sum dy; db2 += sum dz2 (fp32, before rounding); and it advances the
+// Adam step counter.
 template <int OUT>
 __global__ void __launch_bounds__(256) out_layer_kernel(
     const bf16* __restrict__ h2, const float* __restrict__ z2, const bf16* __restrict__ w3,
-    const float* __restrict__ b3, const float* __restrict__ target, int64_t n_valid, float inv_count,
-    float* __restrict__ y_out, bf16* __restrict__ dz2, bf16* __restrict__ dz2t, int64_t ldt,
-    float* __restrict__ g_w3, float* __restrict__ g_b3, float* __restrict__ g_b2, float* __restrict__ loss) {
+    const float* __restrict__ b3, const float* __restrict__ Y, const uint32_t* __restrict__ rows, int64_t n_valid,
+    float inv_count, float* __restrict__ y_out, bf16* __restrict__ dz2, bf16* __restrict__ dz2t, int64_t ldt,
+    float* __restrict__ g_w3, float* __restrict__ g_b3, float* __restrict__ g_b2, float* __restrict__ loss,
+    unsigned* __restrict__ step) {
   __shared__ uint16_t s_t[HID][34];
   __shared__ float s_gw3[OUT * HID];
   __shared__ float s_gb2[HID];
   __shared__ float s_gb3[OUT];
   __shared__ float s_loss;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const bool train = target != nullptr;
+  const bool train = Y != nullptr;
   if (train) {
     for (int i = tid; i < OUT * HID; i += 256) s_gw3[i] = 0.0f;
     s_gb2[tid] = 0.0f;
     if (tid < OUT) s_gb3[tid] = 0.0f;
     if (tid == 0) s_loss = 0.0f;
+    if (step && blockIdx.x == 0 && tid == 0) *step += 1u;
     __syncthreads();
   }
   float w[OUT][8];
 #pragma unroll
   for (int j = 0; j < OUT; ++j) {
-    const uint4 u = *reinterpret_cast<const uint4*>(w3 + j * HID + 8 * lane);
+    const uint4 u = __ldg(reinterpret_cast<const uint4*>(w3 + j * HID + 8 * lane));
     const __nv_bfloat162* p = reinterpret_cast<const __nv_bfloat162*>(&u);
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
@@ -404,14 +426,31 @@ __global__ void __launch_bounds__(256) out_layer_kernel(
   float bias[OUT];
 #pragma unroll
   for (int j = 0; j < OUT; ++j) bias[j] = b3[j];
+  // issue every load of the warp's 4 rows first
+  const int64_t row0 = (int64_t)blockIdx.x * 32 + warp * 4;
+  uint4 hu[4];
+  float4 za[4], zb[4];
+  float tg[4][OUT];
+#pragma unroll
+  for (int rr = 0; rr < 4; ++rr) {
+    hu[rr] = *reinterpret_cast<const uint4*>(h2 + (row0 + rr) * HID + 8 * lane);
+    if (train) {
+      const float4* zr = reinterpret_cast<const float4*>(z2 + (row0 + rr) * HID + 8 * lane);
+      za[rr] = zr[0];
+      zb[rr] = zr[1];
+      const int64_t src = rows ? (int64_t)rows[row0 + rr] : row0 + rr;
+#pragma unroll
+      for (int j = 0; j < OUT; ++j) tg[rr][j] = Y[src * OUT + j];
+    }
+  }
   float gw[OUT][8] = {}, gb2[8] = {}, gb3[OUT] = {}, lsum = 0.0f;
+#pragma unroll
   for (int rr = 0; rr < 4; ++rr) {
     const int rl = warp * 4 + rr;
-    const int64_t row = (int64_t)blockIdx.x * 32 + rl;
+    const int64_t row = row0 + rr;
     float h[8];
     {
-      const uint4 u = *reinterpret_cast<const uint4*>(h2 + row * HID + 8 * lane);
-      const __nv_bfloat162* p = reinterpret_cast<const __nv_bfloat162*>(&u);
+      const __nv_bfloat162* p = reinterpret_cast<const __nv_bfloat162*>(&hu[rr]);
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
         const float2 f = __bfloat1622float2(p[i]);
@@ -437,14 +476,12 @@ __global__ void __launch_bounds__(256) out_layer_kernel(
     float dy[OUT];
 #pragma unroll
     for (int j = 0; j < OUT; ++j) {
-      const float e = y[j] - target[row * OUT + j];
+      const float e = y[j] - tg[rr][j];
       lsum += e * e * inv_count;
       dy[j] = 2.0f * e * inv_count;
       gb3[j] += dy[j];
     }
-    const float4* zr = reinterpret_cast<const float4*>(z2 + row * HID + 8 * lane);
-    const float4 za = zr[0], zb = zr[1];
-    const float z[8] = {za.x, za.y, za.z, za.w, zb.x, zb.y, zb.z, zb.w};
+    const float z[8] = {za[rr].x, za[rr].y, za[rr].z, za[rr].w, zb[rr].x, zb[rr].y, zb[rr].z, zb[rr].w};
     float d[8];
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
@@ -491,28 +528,49 @@ __global__ void __launch_bounds__(256) out_layer_kernel(
 }
 
 // Adam (Kingma & Ba 2015) over the flat fp32 parameters, bias-corrected with the step count
-// held on the device; refreshes the bf16 working copies of the three weight matrices (and W2^T).
+// held on the device.  Gradients of W1 and W2 are the sums of their K-split slices; the other
+// gradients were accumulated atomically and are zeroed here for the next step.  Refreshes the
+// bf16 working copies of the weight matrices (and W2^T).
 struct AdamArgs {
   float* w;
   float* m;
   float* v;
-  const float* g;
+  float* g;
   int64_t n;
   float lr, b1, b2, eps;
   const unsigned* step;
   int64_t o_w1, o_w2, o_w3, n_w1, n_w3;
+  const float* part1;  // [ks1][n_w1]
+  const float* part2;  // [ks2][HID * HID]
+  int ks1, ks2;
   bf16* w1b;
   bf16* w2b;
   bf16* w2t;
   bf16* w3b;
 };
 
+__device__ __forceinline__ float slice_sum(const float* part, int ks, int64_t stride, int64_t k) {
+  float s = 0.0f;
+  for (int z = 0; z < ks; ++z) s += part[(int64_t)z * stride + k];
+  return s;
+}
+
 __global__ void adam_kernel(AdamArgs a) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= a.n) return;
   const float t = (float)*a.step;
   const float c1 = 1.0f - powf(a.b1, t), c2 = 1.0f - powf(a.b2, t);
-  const float gi = a.g[i];
+  const bool in_w1 = i >= a.o_w1 && i < a.o_w1 + a.n_w1;
+  const bool in_w2 = i >= a.o_w2 && i < a.o_w2 + (int64_t)HID * HID;
+  float gi;
+  if (in_w1) {
+    gi = slice_sum(a.part1, a.ks1, a.n_w1, i - a.o_w1);
+  } else if (in_w2) {
+    gi = slice_sum(a.part2, a.ks2, (int64_t)HID * HID, i - a.o_w2);
+  } else {
+    gi = a.g[i];
+    a.g[i] = 0.0f;
+  }
   const float mi = a.b1 * a.m[i] + (1.0f - a.b1) * gi;
   const float vi = a.b2 * a.v[i] + (1.0f - a.b2) * gi * gi;
   a.m[i] = mi;
@@ -520,15 +578,21 @@ __global__ void adam_kernel(AdamArgs a) {
   const float wi = a.w[i] - a.lr * (mi / c1) / (sqrtf(vi / c2) + a.eps);
   a.w[i] = wi;
   const bf16 h = __float2bfloat16_rn(wi);
-  if (i >= a.o_w1 && i < a.o_w1 + a.n_w1) {
+  if (in_w1) {
     a.w1b[i - a.o_w1] = h;
-  } else if (i >= a.o_w2 && i < a.o_w2 + (int64_t)HID * HID) {
+  } else if (in_w2) {
     const int64_t k = i - a.o_w2;
     a.w2b[k] = h;
     a.w2t[(k % HID) * HID + k / HID] = h;
   } else if (i >= a.o_w3 && i < a.o_w3 + a.n_w3) {
     a.w3b[i - a.o_w3] = h;
   }
+}
+
+// g[W1] and g[W2] from their K-split slices (the gradient query without an update).
+__global__ void reduce_slices_kernel(const float* __restrict__ part, int ks, int64_t n, float* __restrict__ out) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) out[k] = slice_sum(part, ks, n, k);
 }
 
 __global__ void to_bf16_kernel(const float* __restrict__ w, int64_t n, bf16* __restrict__ wb, bf16* __restrict__ wt,
@@ -579,12 +643,39 @@ bool graphs_enabled() {
   return !(e && e[0] == '0');
 }
 
+// Split of a batch-row contraction of length K over `tiles` output tiles: the largest power
+// of two that keeps about 128 CTAs and whole 64-row chunks per split.
+int k_splits(int64_t K, int tiles) {
+  int ks = 1;
+  while ((int64_t)ks * 2 * tiles <= 128 && K % ((int64_t)KC * ks * 2) == 0) ks *= 2;
+  return ks;
+}
+
+void prepare_all_gemms() {
+  static std::mutex mu;
+  static bool prepared = false;  // the attribute is per function and process-wide
+  std::lock_guard<std::mutex> lock(mu);
+  if (prepared) return;
+  prepare_gemm<64, EPI_BIAS_GELU, true>();
+  prepare_gemm<64, EPI_BIAS_GELU>();
+  prepare_gemm<64, EPI_GELU_GRAD>();
+  prepare_gemm<64, EPI_F32>();
+  prepare_gemm<256, EPI_F32>();
+  prepare_gemm<128, EPI_F32>();
+  prepare_gemm<32, EPI_F32>();
+  prepare_gemm<256, EPI_F32_ATOMIC>();
+  prepare_gemm<64, EPI_F32_ATOMIC>();
+  prepared = true;
+}
+
 }  // namespace
 
 // ------------------------------------------------------------------------------ model
 struct Mlp::Impl {
   int in_dim = 0, out_dim = 0;
-  cudaStream_t s = nullptr;
+  cudaStream_t s = nullptr;   // owner's stream
+  cudaStream_t s2 = nullptr;  // second stream: dW2 runs beside dH1 / dW1
+  cudaEvent_t fork = nullptr, join = nullptr;
   int64_t P = 0, o_w1 = 0, o_b1 = 0, o_w2 = 0, o_b2 = 0, o_w3 = 0, o_b3 = 0;
   DevBuf<float> w, m, v, g;         // flat fp32 parameters, Adam moments, gradients
   DevBuf<bf16> w1b, w2b, w2t, w3b;  // bf16 working copies (w2t = W2^T)
@@ -595,14 +686,23 @@ struct Mlp::Impl {
   // per-batch activations, capacity `cap` rows
   int64_t cap = 0;
   bool cap_train = false;
-  DevBuf<bf16> xb, xt, h1, h1t, h2, dz2, dz2t, dz1t;
-  DevBuf<float> z1, z2, yb;
+  int ks1 = 1, ks2 = 1;  // K splits of dW1 / dW2 for the current batch size
+  DevBuf<bf16> xt, h1, h1t, h2, dz2, dz2t, dz1t;
+  DevBuf<float> z1, z2, part1, part2;
+
+  ~Impl() {
+    if (fork) (void)cudaEventDestroy(fork);
+    if (join) (void)cudaEventDestroy(join);
+    if (s2) {
+      (void)cudaStreamSynchronize(s2);
+      (void)cudaStreamDestroy(s2);
+    }
+  }
 
   void ensure(int64_t B, bool train) {
     if (B <= cap && (!train || cap_train)) return;
     cap = std::max(cap, B);
     cap_train = cap_train || train;
-    xb.alloc(cap * in_dim, s);
     h1.alloc(cap * HID, s);
     h2.alloc(cap * HID, s);
     if (cap_train) {
@@ -613,37 +713,20 @@ struct Mlp::Impl {
       dz1t.alloc(cap * HID, s);
       z1.alloc(cap * HID, s);
       z2.alloc(cap * HID, s);
-      yb.alloc(cap * out_dim, s);
     }
+  }
+  // Slices for the K splits of a batch of B rows.
+  void ensure_slices(int64_t B) {
+    const int k1 = k_splits(B, (HID / GM) * (in_dim / 64)), k2 = k_splits(B, (HID / GM) * (HID / 64));
+    if (k1 != ks1 || !part1.p) part1.alloc((uint64_t)k1 * HID * in_dim, s);
+    if (k2 != ks2 || !part2.p) part2.alloc((uint64_t)k2 * HID * HID, s);
+    ks1 = k1;
+    ks2 = k2;
   }
 };
 
 int64_t Mlp::param_count(int in_dim, int out_dim) {
   return (int64_t)HID * in_dim + HID + (int64_t)HID * HID + HID + (int64_t)out_dim * HID + out_dim;
-}
-
-// Split of a batch-row contraction of length K over `tiles` output tiles: the largest power
-// of two that keeps about 128 CTAs and whole 64-row chunks per split.
-static int k_splits(int64_t K, int tiles) {
-  int ks = 1;
-  while ((int64_t)ks * 2 * tiles <= 128 && K % ((int64_t)KC * ks * 2) == 0) ks *= 2;
-  return ks;
-}
-
-static void prepare_all_gemms() {
-  static std::mutex mu;
-  static bool prepared = false;  // the attribute is per function and process-wide
-  std::lock_guard<std::mutex> lock(mu);
-  if (prepared) return;
-  prepare_gemm<64, EPI_BIAS_GELU>();
-  prepare_gemm<64, EPI_GELU_GRAD>();
-  prepare_gemm<256, EPI_F32_ATOMIC>();
-  prepare_gemm<64, EPI_F32_ATOMIC>();
-  prepare_gemm<256, EPI_F32>();
-  prepare_gemm<128, EPI_F32>();
-  prepare_gemm<64, EPI_F32>();
-  prepare_gemm<32, EPI_F32>();
-  prepared = true;
 }
 
 Mlp::Mlp(int in_dim, int out_dim, const float* host_params, cudaStream_t s) : p(nullptr) {
@@ -663,6 +746,9 @@ Mlp::Mlp(int in_dim, int out_dim, const float* host_params, cudaStream_t s) : p(
   m.o_b3 = m.o_w3 + (int64_t)out_dim * HID;
   m.P = m.o_b3 + out_dim;
   try {
+    UB_CUDA(cudaStreamCreateWithFlags(&m.s2, cudaStreamNonBlocking));
+    UB_CUDA(cudaEventCreateWithFlags(&m.fork, cudaEventDisableTiming));
+    UB_CUDA(cudaEventCreateWithFlags(&m.join, cudaEventDisableTiming));
     m.w.alloc(m.P, s);
     m.m.alloc(m.P, s);
     m.v.alloc(m.P, s);
@@ -748,20 +834,23 @@ void Mlp::set_input_norm(const float* shift, const float* scale) {
 }
 
 // Forward of one batch of B rows (B % 128 == 0).  With targets Y (training; `rows` selects
-// the batch rows of X and Y) also the backward into g (zeroed here), the loss into `loss`
-// and, with with_adam, the Adam update.  Inference writes y for rows < n_valid.
+// the batch rows of X and Y) also the backward: dW1 / dW2 into their K-split slices, the other
+// gradients added into g, the loss into `loss`; with_adam then applies the Adam update.
+// Inference writes y for rows < n_valid.
 static void run_batch(Mlp::Impl& m, const float* X, const uint32_t* rows, int64_t B, int64_t n_valid,
                       const float* Y, float* y_out, bool with_adam, float lr) {
   cudaStream_t s = m.s;
   const bool train = Y != nullptr;
-  const float* shift = m.has_norm ? m.shift.p : nullptr;
-  const float* scale = m.has_norm ? m.scale.p : nullptr;
-  dim3 bg((unsigned)(B / 32), (unsigned)(m.in_dim / 64));
-  batch_kernel<<<bg, 256, 0, s>>>(X, m.in_dim, rows, n_valid, shift, scale, m.xb.p, train ? m.xt.p : nullptr, B, Y,
-                                  m.out_dim, train ? m.yb.p : nullptr, train ? m.g.p : nullptr, train ? m.P : 0,
-                                  with_adam ? m.step.p : nullptr);
-  UB_LAUNCH_CHECK();
   float* g = m.g.p;
+  GatherA ga{};
+  ga.X = X;
+  ga.ldx = m.in_dim;
+  ga.rows = rows;
+  ga.n_valid = n_valid;
+  ga.shift = m.has_norm ? m.shift.p : nullptr;
+  ga.scale = m.has_norm ? m.scale.p : nullptr;
+  ga.xt = train ? m.xt.p : nullptr;
+  ga.ldt = B;
   EpiArgs e1{};
   e1.bias = m.w.p + m.o_b1;
   e1.out_f32 = train ? m.z1.p : nullptr;
@@ -769,7 +858,7 @@ static void run_batch(Mlp::Impl& m, const float* X, const uint32_t* rows, int64_
   e1.out_t = train ? m.h1t.p : nullptr;
   e1.ldo = HID;
   e1.ldt = (int)B;
-  launch_gemm<64, EPI_BIAS_GELU>(m.xb.p, m.in_dim, m.w1b.p, m.in_dim, B, HID, m.in_dim, 1, e1, m.err.p, s);
+  launch_gemm<64, EPI_BIAS_GELU, true>(nullptr, 8, m.w1b.p, m.in_dim, B, HID, m.in_dim, 1, e1, m.err.p, s, &ga);
   EpiArgs e2{};
   e2.bias = m.w.p + m.o_b2;
   e2.out_f32 = train ? m.z2.p : nullptr;
@@ -777,9 +866,9 @@ static void run_batch(Mlp::Impl& m, const float* X, const uint32_t* rows, int64_
   e2.ldo = HID;
   launch_gemm<64, EPI_BIAS_GELU>(m.h1.p, HID, m.w2b.p, HID, B, HID, HID, 1, e2, m.err.p, s);
   const float inv = 1.0f / (float)(B * m.out_dim);
-#define UB_OUT_ARGS                                                                                                  \
-  m.h2.p, m.z2.p, m.w3b.p, m.w.p + m.o_b3, train ? m.yb.p : nullptr, n_valid, inv, y_out, m.dz2.p, m.dz2t.p, B, \
-      g + m.o_w3, g + m.o_b3, g + m.o_b2, m.loss.p
+#define UB_OUT_ARGS                                                                                                   \
+  m.h2.p, m.z2.p, m.w3b.p, m.w.p + m.o_b3, train ? Y : nullptr, rows, n_valid, inv, y_out, m.dz2.p, m.dz2t.p, B, \
+      g + m.o_w3, g + m.o_b3, g + m.o_b2, m.loss.p, with_adam ? m.step.p : nullptr
   const unsigned og = (unsigned)(B / 32);
   switch (m.out_dim) {
     case 1: out_layer_kernel<1><<<og, 256, 0, s>>>(UB_OUT_ARGS); break;
@@ -790,6 +879,15 @@ static void run_batch(Mlp::Impl& m, const float* X, const uint32_t* rows, int64_
 #undef UB_OUT_ARGS
   UB_LAUNCH_CHECK();
   if (!train) return;
+  // dW2 = dZ2^T H1 on the second stream, beside dH1 and dW1.
+  UB_CUDA(cudaEventRecord(m.fork, s));
+  UB_CUDA(cudaStreamWaitEvent(m.s2, m.fork, 0));
+  EpiArgs e4{};
+  e4.out_f32 = m.part2.p;
+  e4.split_stride = (int64_t)HID * HID;
+  e4.ldo = HID;
+  launch_gemm<64, EPI_F32>(m.dz2t.p, B, m.h1t.p, B, HID, HID, B, m.ks2, e4, m.err.p, m.s2);
+  UB_CUDA(cudaEventRecord(m.join, m.s2));
   // dH1 = dZ2 W2 (B operand W2^T: row i = column i of W2); dZ1 = dH1 * gelu'(Z1), kept
   // transposed for dW1; db1 = its column sums.
   EpiArgs e3{};
@@ -799,18 +897,13 @@ static void run_batch(Mlp::Impl& m, const float* X, const uint32_t* rows, int64_
   e3.ldo = HID;
   e3.ldt = (int)B;
   launch_gemm<64, EPI_GELU_GRAD>(m.dz2.p, HID, m.w2t.p, HID, B, HID, HID, 1, e3, m.err.p, s);
-  // dW2 = dZ2^T H1 and dW1 = dZ1^T X: contractions over the batch rows, split along the
-  // batch so that each launch has about 128 CTAs.
-  EpiArgs e4{};
-  e4.out_f32 = g + m.o_w2;
-  e4.ldo = HID;
-  launch_gemm<64, EPI_F32_ATOMIC>(m.dz2t.p, B, m.h1t.p, B, HID, HID, B, k_splits(B, (HID / GM) * (HID / 64)), e4,
-                                  m.err.p, s);
+  // dW1 = dZ1^T X
   EpiArgs e5{};
-  e5.out_f32 = g + m.o_w1;
+  e5.out_f32 = m.part1.p;
+  e5.split_stride = (int64_t)HID * m.in_dim;
   e5.ldo = m.in_dim;
-  launch_gemm<64, EPI_F32_ATOMIC>(m.dz1t.p, B, m.xt.p, B, HID, m.in_dim, B, k_splits(B, (HID / GM) * (m.in_dim / 64)),
-                                  e5, m.err.p, s);
+  launch_gemm<64, EPI_F32>(m.dz1t.p, B, m.xt.p, B, HID, m.in_dim, B, m.ks1, e5, m.err.p, s);
+  UB_CUDA(cudaStreamWaitEvent(s, m.join, 0));
   if (!with_adam) return;
   AdamArgs a{};
   a.w = m.w.p;
@@ -828,6 +921,10 @@ static void run_batch(Mlp::Impl& m, const float* X, const uint32_t* rows, int64_
   a.o_w3 = m.o_w3;
   a.n_w1 = (int64_t)HID * m.in_dim;
   a.n_w3 = (int64_t)m.out_dim * HID;
+  a.part1 = m.part1.p;
+  a.part2 = m.part2.p;
+  a.ks1 = m.ks1;
+  a.ks2 = m.ks2;
   a.w1b = m.w1b.p;
   a.w2b = m.w2b.p;
   a.w2t = m.w2t.p;
@@ -841,15 +938,19 @@ void Mlp::gradients(const float* X, const float* Y, int64_t B, float* host_grads
   if (B < 128 || B % 128) throw Error(INVALID_ARGUMENT, "batch rows must be a positive multiple of 128");
   if (B > (1 << 24)) throw Error(INVALID_ARGUMENT, "at most 16777216 rows per gradient batch");
   m.ensure(B, true);
-  std::vector<uint32_t> ident(B);
-  for (int64_t i = 0; i < B; ++i) ident[i] = (uint32_t)i;
-  DevBuf<uint32_t> rows(B, m.s);
-  UB_CUDA(cudaMemcpyAsync(rows.p, ident.data(), B * 4, cudaMemcpyHostToDevice, m.s));
+  m.ensure_slices(B);
+  UB_CUDA(cudaMemsetAsync(m.g.p, 0, m.P * 4, m.s));
   UB_CUDA(cudaMemsetAsync(m.loss.p, 0, 4, m.s));
-  run_batch(m, X, rows.p, B, B, Y, nullptr, false, 0.0f);
+  run_batch(m, X, nullptr, B, B, Y, nullptr, false, 0.0f);
+  const int64_t n1 = (int64_t)HID * m.in_dim, n2 = (int64_t)HID * HID;
+  reduce_slices_kernel<<<grid_for(n1, 256), 256, 0, m.s>>>(m.part1.p, m.ks1, n1, m.g.p + m.o_w1);
+  UB_LAUNCH_CHECK();
+  reduce_slices_kernel<<<grid_for(n2, 256), 256, 0, m.s>>>(m.part2.p, m.ks2, n2, m.g.p + m.o_w2);
+  UB_LAUNCH_CHECK();
   UB_CUDA(cudaMemcpyAsync(host_grads, m.g.p, m.P * 4, cudaMemcpyDeviceToHost, m.s));
   UB_CUDA(cudaMemcpyAsync(loss_out, m.loss.p, 4, cudaMemcpyDeviceToHost, m.s));
   check_error();
+  UB_CUDA(cudaMemsetAsync(m.g.p, 0, m.P * 4, m.s));
 }
 
 void Mlp::train(const float* X, const float* Y, int64_t n, int epochs, int64_t batch, float lr, uint64_t seed,
@@ -864,6 +965,7 @@ void Mlp::train(const float* X, const float* Y, int64_t n, int epochs, int64_t b
   if (steps < 1) throw Error(INVALID_ARGUMENT, "fewer training rows than one batch");
   if (epochs == 0) return;
   m.ensure(batch, true);
+  m.ensure_slices(batch);
   // Shuffles: Fisher-Yates driven by splitmix64(seed), one permutation per epoch, uploaded once.
   const int64_t per_epoch = steps * batch;
   std::vector<uint32_t> perm((size_t)epochs * per_epoch);
@@ -883,6 +985,7 @@ void Mlp::train(const float* X, const float* Y, int64_t n, int epochs, int64_t b
   DevBuf<uint32_t> dperm(perm.size(), s), cur(per_epoch, s);
   DevBuf<float> dloss(epochs, s);
   UB_CUDA(cudaMemcpyAsync(dperm.p, perm.data(), perm.size() * 4, cudaMemcpyHostToDevice, s));
+  UB_CUDA(cudaMemsetAsync(m.g.p, 0, m.P * 4, s));
   auto one_epoch = [&]() {
     for (int64_t t = 0; t < steps; ++t) run_batch(m, X, cur.p + t * batch, batch, batch, Y, nullptr, true, lr);
   };
@@ -909,7 +1012,7 @@ void Mlp::train(const float* X, const float* Y, int64_t n, int epochs, int64_t b
       if (e) (void)cudaGraphExecDestroy(e);
     }
   } guard{exec};
-  const uint64_t launches_per_epoch = (uint64_t)steps * 8;
+  const uint64_t launches_per_epoch = (uint64_t)steps * 7;
   for (int e = 0; e < epochs; ++e) {
     UB_CUDA(cudaMemcpyAsync(cur.p, dperm.p + (int64_t)e * per_epoch, per_epoch * 4, cudaMemcpyDeviceToDevice, s));
     UB_CUDA(cudaMemsetAsync(m.loss.p, 0, 4, s));

@@ -718,8 +718,8 @@ uint32_t pick_chunk(uint64_t n_edges) {
     long v = atol(e);
     if (v >= 1 && v <= (1 << 30)) return (uint32_t)v;
   }
-  uint64_t c = (n_edges / 135000 + 7) / 8 * 8;
-  return (uint32_t)std::min<uint64_t>(512, std::max<uint64_t>(32, c));
+  uint64_t c = (n_edges / 135000 + 4) / 8 * 8;
+  return (uint32_t)std::min<uint64_t>(512, std::max<uint64_t>(16, c));
 }
 
 void build_sgd_layout(const uint64_t* kept_ptr, const uint32_t* ktail, const double* keps, uint64_t n,

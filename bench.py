@@ -186,13 +186,21 @@ def run_reference(a):
 
 def run_batched(a):
     """Batched many-instance workload: one batched fit (one kernel launch per epoch over all
-    instances, graph-captured, autotuned) vs a per-instance loop of the plain fit."""
+    instances, graph-captured, autotuned) vs a per-instance loop of the plain fit.  With N
+    ranks the instances are cut into N contiguous, edge-balanced shards (no data-path
+    collective); value = all ranks' edge-updates / the slowest rank's time."""
     import torch
     import umap_b200 as ub
+    from umap_b200 import replicas as R
     from umap_b200 import workloads as W
-    torch.cuda.set_device(0)
+    rank, world, local = R.env()
+    torch.cuda.set_device(local)
+    R.init("nccl", timeout_s=600)
+    dev = torch.device("cuda", local)
+    all_sizes = W.instance_sizes(a.instances)
+    lo_i, hi_i = R.shard_by_cost(all_sizes, world)[rank]
     t0 = time.time()
-    sizes, idx, dist, init = W.instances_torch(a.instances)
+    sizes, idx, dist, init = W.instances_torch(a.instances, device=dev, which=range(lo_i, hi_i))
     torch.cuda.synchronize()
     gen_s = time.time() - t0
     off = np.concatenate([[0], np.cumsum(sizes)]).astype(np.uint64)
@@ -207,32 +215,45 @@ def run_batched(a):
     for _ in range(max(1, a.warmup)):
         ub.batch_fit(cfg, off, idx, dist, init)
     torch.cuda.synchronize()
+    R.barrier(dev)
+    torch.cuda.synchronize()
     launches0 = ub.kernel_launches()
-    with Clocks(0) as clk:
+    with Clocks(local) as clk:
         ev0.record()
         for _ in range(a.steps):
             ub.batch_fit(cfg, off, idx, dist, init)
         ev1.record()
         torch.cuda.synchronize()
-    ms = ev0.elapsed_time(ev1) / a.steps
+    R.barrier(dev)
+    ms = R.max_over_ranks(ev0.elapsed_time(ev1) / a.steps, device=dev)
     launches = (ub.kernel_launches() - launches0) // a.steps
-    # per-instance loop of the plain GPU path on every loop_sample-th instance
-    step = max(1, a.loop_sample)
-    t1 = time.perf_counter()
-    for i in range(0, len(sizes), step):
-        lo, hi = int(off[i]), int(off[i + 1])
-        ub.Umap(cfg).fit(hi - lo, idx[lo:hi], dist[lo:hi], init[lo:hi])
-    torch.cuda.synchronize()
-    loop_ms = (time.perf_counter() - t1) * 1e3 * step
-    line = {"metric": "SGD edge-updates/s (batched instances)", "value": F / (ms / 1e3), "unit": "edge-updates/s",
-            "n_gpus": 1, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True,
-            "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"instances_{len(sizes)}_logu500-50000_d32_k15_200ep", "points": int(off[-1]),
-                       "kept_edges": E, "edge_updates_per_fit": F, "negatives_per_fit": Nn,
-                       "autotuned_chunk": chunk, "autotuned_block": bt, "generate_s": round(gen_s, 1)},
-            "per_instance_loop_ms": loop_ms, "loop_sample": f"every {step}-th instance, time x {step}",
-            "speedup_vs_loop": loop_ms / ms, "gpu_launches_per_fit": launches, "clocks": clk.summary()}
-    print(json.dumps(line), flush=True)
+    F_all = R.sum_over_ranks(F, device=dev)
+    loop_ms = None
+    if world == 1:
+        # per-instance loop of the plain GPU path on every loop_sample-th instance
+        step = max(1, a.loop_sample)
+        t1 = time.perf_counter()
+        for i in range(0, len(sizes), step):
+            lo, hi = int(off[i]), int(off[i + 1])
+            ub.Umap(cfg).fit(hi - lo, idx[lo:hi], dist[lo:hi], init[lo:hi])
+        torch.cuda.synchronize()
+        loop_ms = (time.perf_counter() - t1) * 1e3 * step
+    line = {"metric": "SGD edge-updates/s (batched instances)", "value": F_all / (ms / 1e3), "unit": "edge-updates/s",
+            "n_gpus": world, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "strong" if world > 1 else "weak", "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"instances_{a.instances}_logu500-50000_d32_k15_200ep",
+                       "points_rank0": int(off[-1]), "kept_edges_rank0": E, "edge_updates_per_fit": F_all,
+                       "negatives_per_fit_rank0": Nn, "autotuned_chunk": chunk, "autotuned_block": bt,
+                       "generate_s": round(gen_s, 1),
+                       "parallelism": f"instance shards x{world}" if world > 1 else "single"},
+            "per_instance_loop_ms": loop_ms,
+            "loop_sample": f"every {max(1, a.loop_sample)}-th instance, time x {max(1, a.loop_sample)}"
+            if loop_ms is not None else None,
+            "speedup_vs_loop": loop_ms / ms if loop_ms else None, "gpu_launches_per_fit": launches,
+            "clocks": clk.summary()}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    R.finalize()
 
 
 def run_warm_start(a):
@@ -350,12 +371,10 @@ def main():
         return run_warm_start(a)
     import torch
     import umap_b200 as ub
-    rank, world, local = dist_info()
+    from umap_b200 import replicas as R
+    rank, world, local = R.env()
     torch.cuda.set_device(local)
-    if world > 1:
-        import torch.distributed as tdist
-        import datetime
-        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    R.init("nccl", timeout_s=600)
     ub.lib()
 
     idx, dist, init, winfo = make_workload(a.n)
@@ -397,8 +416,8 @@ def main():
     for _ in range(a.warmup):
         one_fit()
     torch.cuda.synchronize()
-    if world > 1:
-        torch.distributed.barrier()
+    R.barrier(torch.device("cuda", local))
+    torch.cuda.synchronize()
     launches0 = ub.kernel_launches()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     sgd_ms = []
@@ -409,12 +428,10 @@ def main():
             sgd_ms.append(ms)
         ev1.record()
         torch.cuda.synchronize()
+    R.barrier(torch.device("cuda", local))
     launches = ub.kernel_launches() - launches0
     ms_total = ev0.elapsed_time(ev1)
-    if world > 1:
-        t = torch.tensor([ms_total], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms_total = float(t.item())
+    ms_total = R.max_over_ranks(ms_total, device="cuda")
     ms_step = ms_total / a.steps
     value = F_tot * world / (ms_step / 1e3)
 
@@ -475,8 +492,7 @@ def main():
         line["cpu_baseline"] = cpu_baseline(idx, dist, init, a.epochs, a.cpu_epochs, a.cpu_skip)
     if rank == 0:
         print(json.dumps(line), flush=True)
-    if world > 1:
-        torch.distributed.destroy_process_group()
+    R.finalize()
 
 
 if __name__ == "__main__":

@@ -266,20 +266,24 @@ def knn_exact_clustered_torch(X: np.ndarray, labels: np.ndarray, k: int, device=
             int(bad_rows.numel()))
 
 
-def instances_torch(count: int = 4096, k: int = 15, seed: int = 4, device="cuda", lo=500, hi=50_000):
+def instances_torch(count: int = 4096, k: int = 15, seed: int = 4, device="cuda", lo=500, hi=50_000,
+                    which: range | None = None):
     """The batched workload on the GPU: `count` datasets with sizes log-uniform in [lo, hi],
     each D=32, 5 Gaussians (centres ~N(0, 5^2 I), std 1), per-instance seed; exact kNN k
-    (self first, local ids) by brute force per instance; init U[-10, 10]^2.
-    Returns (sizes i64[count], idx i32 CUDA [N, k], dist f32 CUDA [N, k], init f32 CUDA [N, 2])."""
+    (self first, local ids) by brute force per instance; init U[-10, 10]^2.  `which` (a
+    range of instance ids) generates only those instances, exactly as in the full set.
+    Returns (sizes i64[m], idx i32 CUDA [N, k], dist f32 CUDA [N, k], init f32 CUDA [N, 2])."""
     import torch
 
     torch.backends.cuda.matmul.allow_tf32 = False
-    sizes = instance_sizes(count, lo, hi, seed)
+    all_sizes = instance_sizes(count, lo, hi, seed)
+    which = range(count) if which is None else which
+    sizes = all_sizes[which.start:which.stop]
     N = int(sizes.sum())
     idx = torch.empty((N, k), dtype=torch.int32, device=device)
     dst = torch.empty((N, k), dtype=torch.float32, device=device)
     off = 0
-    for i, n in enumerate(sizes.tolist()):
+    for i, n in zip(which, sizes.tolist()):
         g = torch.Generator(device=device).manual_seed(1000 + i)
         centres = torch.randn((5, 32), generator=g, device=device) * 5.0
         lab = torch.randint(0, 5, (n,), generator=g, device=device)
@@ -294,5 +298,7 @@ def instances_torch(count: int = 4096, k: int = 15, seed: int = 4, device="cuda"
             dst[off + s:off + e] = cd
         off += n
     g = torch.Generator(device=device).manual_seed(77)
-    init = torch.rand((N, 2), generator=g, device=device) * 20.0 - 10.0
+    init = torch.rand((int(all_sizes.sum()), 2), generator=g, device=device) * 20.0 - 10.0
+    first = int(all_sizes[:which.start].sum())
+    init = init[first:first + N].contiguous()
     return sizes, idx, dst, init

@@ -45,12 +45,15 @@ def parse():
     ap.add_argument("--profile", action="store_true",
                     help="profiling run: build one optimizer, run --profile-epochs epochs, exit")
     ap.add_argument("--profile-epochs", type=int, default=24)
-    ap.add_argument("--workload", default="gaussians_2m", choices=["gaussians_2m", "batched", "warm_start"],
+    ap.add_argument("--workload", default="gaussians_2m",
+                    choices=["gaussians_2m", "batched", "warm_start", "swiss_roll"],
                     help="batched: 4096 independent instances, 200 epochs, vs a per-instance loop; "
                          "warm_start: learned initial embedding + a shortened fit vs the plain fit")
     ap.add_argument("--sub", type=int, default=100_000, help="warm_start: subsample size")
     ap.add_argument("--warm-epochs", type=int, default=100, help="warm_start: epochs of the refining fit")
     ap.add_argument("--warm-lr", type=float, default=None, help="warm_start: learning rate of the refining fit")
+    ap.add_argument("--n-swiss", type=int, default=100_000_000, help="swiss_roll: points")
+    ap.add_argument("--swiss-epochs", type=int, default=200, help="swiss_roll: epochs")
     ap.add_argument("--instances", type=int, default=4096)
     ap.add_argument("--loop-sample", type=int, default=8,
                     help="per-instance loop timed on every n-th instance, scaled by n")
@@ -361,6 +364,125 @@ def run_warm_start(a):
     print(json.dumps(line), flush=True)
 
 
+def run_swiss_roll(a):
+    """HBM-bound workload: a noisy 3-D swiss roll of --n-swiss points (default 100,000,000),
+    exact kNN k=15 on a uniform grid (harness, timed separately), init U[-10,10]^2, 200
+    epochs.  One step = one fit from kNN + init resident in HBM.  The 800 MB embedding does
+    not fit the 126 MB L2, so the SGD epoch streams it from HBM.  Spot checks: rho / sigma of
+    a seeded sample of rows against the oracle's smooth-kNN on those rows.  cpu_baseline: the
+    oracle on a 2,000,000-point swiss roll of the same distribution (per-edge-update
+    throughput; the full-size state does not fit host memory)."""
+    import torch
+    import umap_b200 as ub
+    from umap_b200 import workloads as W
+    torch.cuda.set_device(0)
+    n = a.n_swiss
+    t0 = time.time()
+    X = W.swiss_roll_torch(n, seed=2)
+    idx, dist, redone = W.knn_grid_torch(X, 15)
+    torch.cuda.synchronize()
+    knn_s = time.time() - t0
+    del X
+    torch.cuda.empty_cache()  # return the kNN harness's temporaries before the fit
+    g = torch.Generator(device="cuda").manual_seed(0)
+    init = torch.rand((n, 2), generator=g, device="cuda") * 20.0 - 10.0
+    cfg = ub.UmapConfig()
+    cfg.optimization.n_epochs = a.swiss_epochs
+    free0, total_mem = torch.cuda.mem_get_info()
+    if a.profile:
+        # bounded profiling target: one optimizer, a few epochs, few launches before them
+        opt = ub.Optimizer(ub.Umap(cfg).learn_manifold(n, idx, dist), init, a.swiss_epochs, cfg)
+        opt.step_epochs(a.profile_epochs)
+        torch.cuda.synchronize()
+        print(json.dumps({"profile": True, "epochs": a.profile_epochs, "ms": opt.last_step_ms(),
+                          "edges": opt.n_edges(), "fired_negatives": opt.schedule_totals(0, a.profile_epochs)}),
+              flush=True)
+        return
+
+    def one_fit(stats=None):
+        m = ub.Umap(cfg).learn_manifold(n, idx, dist)
+        if stats is not None:
+            s, r = m.sigmas_rhos()
+            stats["sig_rho"] = (s, r)
+        opt = ub.Optimizer(m, init, a.swiss_epochs, cfg)
+        if stats is not None:
+            stats["E"] = opt.n_edges()
+            stats["FN"] = opt.schedule_totals(0, a.swiss_epochs)
+            stats["free_after_setup"] = torch.cuda.mem_get_info()[0]
+        opt.step_epochs(a.swiss_epochs)
+        ms = opt.last_step_ms()
+        f = opt.into_fitted(cfg)
+        return f, ms
+
+    stats = {}
+    f, _ = one_fit(stats)
+    emb = f.embedding()
+    finite = float(np.isfinite(emb).all(1).mean())
+    del f
+    for _ in range(max(0, a.warmup - 1)):
+        one_fit()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sgd = []
+    launches0 = ub.kernel_launches()
+    torch.cuda.synchronize()
+    with Clocks(0) as clk:
+        ev0.record()
+        for _ in range(a.steps):
+            f, ms = one_fit()
+            sgd.append(ms)
+            del f
+        ev1.record()
+        torch.cuda.synchronize()
+    launches = ub.kernel_launches() - launches0
+    ms_step = ev0.elapsed_time(ev1) / a.steps
+    E = stats["E"]
+    F_tot, N_tot = stats["FN"]
+    sgd_ms = float(np.median(sgd))
+    alg = 4.0 * E * a.swiss_epochs + 40.0 * F_tot + 8.0 * N_tot
+    pk = peaks()
+    hbm = pk.get("hbm_gbs") or 6650.0
+    achieved = alg / (sgd_ms / 1e3) / 1e9
+    # spot check: sampled rows' rho (bit-exact) and sigma (1e-5 relative) against the oracle
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    O.build()
+    rows = np.sort(np.random.Generator(np.random.PCG64(5)).choice(n, 20000, replace=False))
+    d_rows = dist[torch.from_numpy(rows).cuda()].cpu().numpy()
+    so, ro = O.smooth_knn_dist(d_rows, 15)
+    sg, rg = stats["sig_rho"]
+    rho_exact = bool(np.array_equal(rg[rows].view(np.uint32), ro.view(np.uint32)))
+    sig_rel = float(np.max(np.abs(sg[rows].astype(np.float64) - so) / np.maximum(np.abs(so), 1e-30)))
+    cpu = None
+    if not a.no_cpu:
+        Xc = W.swiss_roll_torch(2_000_000, seed=3)
+        ci, cd, _ = W.knn_grid_torch(Xc, 15)
+        cpu = cpu_baseline(ci.cpu().numpy().view(np.uint32), cd.cpu().numpy(),
+                           W.uniform_init(2_000_000), a.swiss_epochs, a.cpu_epochs, a.cpu_skip)
+        cpu["sample"] = "2,000,000-point swiss roll (same distribution, seed 3): " + cpu["sample"]
+    line = {"metric": "SGD edge-updates/s", "value": F_tot / (ms_step / 1e3), "unit": "edge-updates/s",
+            "n_gpus": 1, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"swiss_roll_{n}_d3_k15_{a.swiss_epochs}ep", "n_points": n,
+                       "kept_edges": E, "edge_updates_per_fit": F_tot, "negatives_per_fit": N_tot,
+                       "knn_seconds_harness": round(knn_s, 1), "knn_rows_redone": redone,
+                       "l2": "embedding 800 MB and edge slices exceed L2"},
+            "sgd_ms_per_fit": sgd_ms, "sgd_edge_updates_per_s": F_tot / (sgd_ms / 1e3),
+            "graph_and_setup_ms": ms_step - sgd_ms,
+            "roofline": {"bound": "hbm", "kernel": "sgd_epoch_kernel2<2>", "achieved": achieved, "peak": hbm,
+                         "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
+                         "algorithmic_bytes_per_launch": alg / a.swiss_epochs,
+                         "avg_launch_ms": sgd_ms / a.swiss_epochs},
+            "device_memory_gb": {"total": total_mem / 1e9, "inputs_resident": (total_mem - free0) / 1e9,
+                                 "in_use_after_optimizer_setup":
+                                     (total_mem - stats["free_after_setup"]) / 1e9},
+            "checks": {"sample_rows": 20000, "rho_bit_exact": rho_exact, "sigma_max_rel_err": sig_rel,
+                       "finite_rows": finite},
+            "gpu_launches": launches, "clocks": clk.summary()}
+    if cpu:
+        line["cpu_baseline"] = cpu
+    print(json.dumps(line), flush=True)
+
+
 def main():
     a = parse()
     if a.impl == "reference":
@@ -369,6 +491,8 @@ def main():
         return run_batched(a)
     if a.workload == "warm_start":
         return run_warm_start(a)
+    if a.workload == "swiss_roll":
+        return run_swiss_roll(a)
     import torch
     import umap_b200 as ub
     from umap_b200 import replicas as R

@@ -302,3 +302,113 @@ def instances_torch(count: int = 4096, k: int = 15, seed: int = 4, device="cuda"
     first = int(all_sizes[:which.start].sum())
     init = init[first:first + N].contiguous()
     return sizes, idx, dst, init
+
+
+# ------------------------------------------------------------------ 100M-point swiss roll
+def swiss_roll_torch(n: int, seed: int = 2, device="cuda"):
+    """``swiss_roll`` generated on the GPU in chunks (t~U[1.5pi, 4.5pi], height~U[0, 20],
+    Gaussian noise std 0.05); returns f32 CUDA [n, 3]."""
+    import torch
+    X = torch.empty((n, 3), dtype=torch.float32, device=device)
+    g = torch.Generator(device=device).manual_seed(seed)
+    chunk = 1 << 24
+    for s in range(0, n, chunk):
+        e = min(n, s + chunk)
+        m = e - s
+        t = torch.rand(m, generator=g, device=device, dtype=torch.float64) * (3.0 * math.pi) + 1.5 * math.pi
+        h = torch.rand(m, generator=g, device=device, dtype=torch.float64) * 20.0
+        P = torch.stack([t * torch.cos(t), h, t * torch.sin(t)], dim=1)
+        P += torch.randn((m, 3), generator=g, device=device, dtype=torch.float64) * 0.05
+        X[s:e] = P.to(torch.float32)
+    return X
+
+
+def _grid_keys(torch, X, lo, h, dims):
+    c = torch.floor((X - lo) / h).to(torch.int64)
+    c = torch.minimum(torch.clamp(c, min=0), dims - 1)
+    return (c[:, 0] * dims[1] + c[:, 1]) * dims[2] + c[:, 2], c
+
+
+def _grid_pass(torch, X, rows, k, h, chunk):
+    """Candidates from the 27 cells around each query row on a grid of cell size h.
+    Returns (idx [m, k] int64, dist [m, k] f32, certified [m] bool): a row is certified when
+    its k-th distance is <= h, so no point outside the 27 cells can be closer."""
+    dev = X.device
+    lo = X.min(0).values
+    dims = (torch.floor((X.max(0).values - lo) / h).to(torch.int64) + 1)
+    keys, _ = _grid_keys(torch, X, lo, h, dims)
+    keys_sorted, order = torch.sort(keys)
+    uniq, counts = torch.unique_consecutive(keys_sorted, return_counts=True)
+    starts = torch.cumsum(counts, 0) - counts
+    M = int(counts.max())
+    Xs = X[order]
+    offs = torch.tensor([(a, b, c) for a in (-1, 0, 1) for b in (-1, 0, 1) for c in (-1, 0, 1)],
+                        dtype=torch.int64, device=dev)
+    ar = torch.arange(M, device=dev)
+    m = rows.numel()
+    out_i = torch.empty((m, k), dtype=torch.int64, device=dev)
+    out_d = torch.empty((m, k), dtype=torch.float32, device=dev)
+    q_chunk = max(1024, min(chunk, int(2e8 // (27 * M))))
+    for s in range(0, m, q_chunk):
+        e = min(m, s + q_chunk)
+        q = X[rows[s:e]]
+        _, qc = _grid_keys(torch, q, lo, h, dims)
+        nc = qc[:, None, :] + offs[None, :, :]                                   # [Q, 27, 3]
+        inside = ((nc >= 0) & (nc < dims)).all(-1)
+        nk = (nc[..., 0] * dims[1] + nc[..., 1]) * dims[2] + nc[..., 2]
+        pos = torch.searchsorted(uniq, nk).clamp(max=uniq.numel() - 1)
+        found = inside & (uniq[pos] == nk)
+        cnt = torch.where(found, counts[pos], torch.zeros_like(pos))
+        cand = starts[pos][..., None] + ar                                       # [Q, 27, M]
+        valid = ar < cnt[..., None]
+        cand = torch.where(valid, cand, torch.zeros_like(cand)).reshape(e - s, -1)
+        valid = valid.reshape(e - s, -1)
+        diff = Xs[cand] - q[:, None, :]
+        d2 = (diff * diff).sum(-1)
+        d2 = torch.where(valid, d2, torch.full_like(d2, float("inf")))
+        kk = min(k, d2.shape[1])
+        vals, p = torch.topk(d2, kk, dim=1, largest=False, sorted=True)
+        gid = order[torch.gather(cand, 1, p)]
+        out_i[s:e, :kk] = gid
+        out_d[s:e, :kk] = torch.sqrt(vals)
+        if kk < k:
+            out_i[s:e, kk:] = 0
+            out_d[s:e, kk:] = float("inf")
+    ok = out_d[:, k - 1] <= h
+    return out_i, out_d, ok
+
+
+def knn_grid_torch(X, k: int, chunk: int = 1 << 17, occupancy: float = 6.0):
+    """Exact kNN (self first at distance 0) of low-dimensional points (CUDA f32 [n, d]) with
+    a uniform grid: each query searches the 3^d cells around its own.  The cell size is set
+    so that occupied cells hold about `occupancy` points; rows whose k-th distance exceeds
+    the cell size are redone on a grid with twice the cell size until every row is
+    certified.  Returns (idx int32 CUDA [n, k], dist f32 CUDA [n, k], rows redone)."""
+    import torch
+    n, d = X.shape
+    lo = X.min(0).values
+    ext = (X.max(0).values - lo).clamp(min=1e-6)
+    h = float((ext.prod() / max(n, 1) * occupancy) ** (1.0 / d))
+    for _ in range(8):  # refine h towards the target occupancy of occupied cells
+        dims = (torch.floor(ext / h).to(torch.int64) + 1)
+        keys, _ = _grid_keys(torch, X, lo, h, dims)
+        occ = n / float(torch.unique(keys).numel())
+        if 0.7 * occupancy <= occ <= 1.4 * occupancy:
+            break
+        h *= (occupancy / occ) ** (1.0 / d)
+        del keys
+    rows = torch.arange(n, device=X.device)
+    idx = torch.empty((n, k), dtype=torch.int32, device=X.device)
+    dst = torch.empty((n, k), dtype=torch.float32, device=X.device)
+    redone = 0
+    first = True
+    while rows.numel():
+        oi, od, ok = _grid_pass(torch, X, rows, k, h, chunk)
+        idx[rows[ok]] = oi[ok].to(torch.int32)
+        dst[rows[ok]] = od[ok]
+        rows = rows[~ok]
+        if not first:
+            redone += int(ok.sum())
+        first = False
+        h *= 2.0
+    return idx, dst, redone

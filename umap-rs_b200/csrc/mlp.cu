@@ -22,6 +22,7 @@
 // backward (CUDA cores) -> { dH1 GEMM (GELU derivative, db1) -> dW1 GEMM } || dW2 GEMM on a
 // second stream -> Adam.  The dW GEMMs contract over the batch in K splits whose partial sums
 // are stored to separate slices and summed by the Adam kernel.
+#include <cuda.h>  // CUtensorMap and its enums; the encoder is fetched from the runtime
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -129,6 +130,98 @@ __device__ __forceinline__ bool mbar_wait(uint32_t addr, uint32_t phase) {
 __device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
   const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
   return *reinterpret_cast<const uint32_t*>(&h);
+}
+
+// Epilogue: thread (warp w, lane l) owns output row m0 + 32w + l; reads the accumulator from
+// tensor memory 32 columns at a time and applies the layer's elementwise work.  `scratch`
+// (>= 4 x 32 x 33 floats of shared memory no longer read by the MMAs) serves the column sums.
+template <int BN, int EPI>
+__device__ __forceinline__ void epilogue(uint32_t taddr, int64_t m0, int64_t n0, const EpiArgs& ep,
+                                         uint8_t* scratch, int warp, int lane) {
+  uint8_t* smem = scratch;
+  const int64_t row = m0 + warp * 32 + lane;
+#pragma unroll 1
+  for (int c0 = 0; c0 < BN; c0 += 32) {
+    uint32_t r[32];
+    const uint32_t ta = taddr + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(ta));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+    const int64_t cb = n0 + c0;  // first column of this group
+    float v[32];
+#pragma unroll
+    for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
+    if (EPI == EPI_F32 || EPI == EPI_F32_ATOMIC) {
+      if (EPI == EPI_F32 && ep.bias) {
+#pragma unroll
+        for (int j = 0; j < 32; ++j) v[j] += __ldg(ep.bias + cb + j);
+      }
+      float* base = ep.out_f32 + (EPI == EPI_F32 ? (int64_t)blockIdx.z * ep.split_stride : 0);
+      float4* o = reinterpret_cast<float4*>(base + row * ep.ldo + cb);
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const float4 x = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+        if (EPI == EPI_F32_ATOMIC) atomicAdd(o + q, x);
+        else o[q] = x;
+      }
+    } else {
+      if (EPI == EPI_BIAS_GELU) {
+#pragma unroll
+        for (int j = 0; j < 32; ++j) v[j] += __ldg(ep.bias + cb + j);
+        if (ep.out_f32) {
+          float4* o = reinterpret_cast<float4*>(ep.out_f32 + row * ep.ldo + cb);
+#pragma unroll
+          for (int q = 0; q < 8; ++q) o[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+        }
+#pragma unroll
+        for (int j = 0; j < 32; ++j) v[j] = gelu(v[j]);
+      } else {  // EPI_GELU_GRAD
+        const float4* zi = reinterpret_cast<const float4*>(ep.z_in + row * ep.ldo + cb);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const float4 z = zi[q];
+          v[4 * q] *= gelu_grad(z.x);
+          v[4 * q + 1] *= gelu_grad(z.y);
+          v[4 * q + 2] *= gelu_grad(z.z);
+          v[4 * q + 3] *= gelu_grad(z.w);
+        }
+        if (ep.colsum) {
+          // column sums over the warp's 32 rows through shared memory (the K stages are
+          // free once the MMAs completed), one atomic per column per warp
+          float* red = reinterpret_cast<float*>(smem) + warp * (32 * 33);
+#pragma unroll
+          for (int j = 0; j < 32; ++j) red[lane * 33 + j] = v[j];
+          __syncwarp();
+          float sum = 0.0f;
+#pragma unroll 8
+          for (int rr = 0; rr < 32; ++rr) sum += red[rr * 33 + lane];
+          atomicAdd(ep.colsum + cb + lane, sum);
+          __syncwarp();
+        }
+      }
+      uint32_t pk[16];
+#pragma unroll
+      for (int j = 0; j < 16; ++j) pk[j] = pack_bf16(v[2 * j], v[2 * j + 1]);
+      if (ep.out_bf16) {
+        uint4* o = reinterpret_cast<uint4*>(ep.out_bf16 + row * ep.ldo + cb);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) o[q] = make_uint4(pk[4 * q], pk[4 * q + 1], pk[4 * q + 2], pk[4 * q + 3]);
+      }
+      if (ep.out_t) {
+        uint16_t* t = reinterpret_cast<uint16_t*>(ep.out_t);
+#pragma unroll
+        for (int j = 0; j < 32; ++j)
+          t[(cb + j) * ep.ldt + row] = (uint16_t)((j & 1) ? (pk[j >> 1] >> 16) : (pk[j >> 1] & 0xFFFFu));
+      }
+    }
+  }
 }
 
 template <int BN, int EPI, bool GATHER>
@@ -261,95 +354,146 @@ __global__ void __launch_bounds__(GT) umma_gemm_kernel(const bf16* __restrict__ 
   }
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 
-  if (ok) {
-    const int64_t row = m0 + warp * 32 + lane;
-#pragma unroll 1
-    for (int c0 = 0; c0 < BN; c0 += 32) {
-      uint32_t r[32];
-      const uint32_t ta = taddr + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
-      asm volatile(
-          "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
-          "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-          "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-            "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
-            "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-            "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-          : "r"(ta));
-      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      const int64_t cb = n0 + c0;  // first column of this group
-      float v[32];
-#pragma unroll
-      for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
-      if (EPI == EPI_F32 || EPI == EPI_F32_ATOMIC) {
-        if (EPI == EPI_F32 && ep.bias) {
-#pragma unroll
-          for (int j = 0; j < 32; ++j) v[j] += __ldg(ep.bias + cb + j);
-        }
-        float* base = ep.out_f32 + (EPI == EPI_F32 ? (int64_t)blockIdx.z * ep.split_stride : 0);
-        float4* o = reinterpret_cast<float4*>(base + row * ep.ldo + cb);
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-          const float4 x = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
-          if (EPI == EPI_F32_ATOMIC) atomicAdd(o + q, x);
-          else o[q] = x;
-        }
-      } else {
-        if (EPI == EPI_BIAS_GELU) {
-#pragma unroll
-          for (int j = 0; j < 32; ++j) v[j] += __ldg(ep.bias + cb + j);
-          if (ep.out_f32) {
-            float4* o = reinterpret_cast<float4*>(ep.out_f32 + row * ep.ldo + cb);
-#pragma unroll
-            for (int q = 0; q < 8; ++q) o[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
-          }
-#pragma unroll
-          for (int j = 0; j < 32; ++j) v[j] = gelu(v[j]);
-        } else {  // EPI_GELU_GRAD
-          const float4* zi = reinterpret_cast<const float4*>(ep.z_in + row * ep.ldo + cb);
-#pragma unroll
-          for (int q = 0; q < 8; ++q) {
-            const float4 z = zi[q];
-            v[4 * q] *= gelu_grad(z.x);
-            v[4 * q + 1] *= gelu_grad(z.y);
-            v[4 * q + 2] *= gelu_grad(z.z);
-            v[4 * q + 3] *= gelu_grad(z.w);
-          }
-          if (ep.colsum) {
-            // column sums over the warp's 32 rows through shared memory (the K stages are
-            // free once the MMAs completed), one atomic per column per warp
-            float* red = reinterpret_cast<float*>(smem) + warp * (32 * 33);
-#pragma unroll
-            for (int j = 0; j < 32; ++j) red[lane * 33 + j] = v[j];
-            __syncwarp();
-            float sum = 0.0f;
-#pragma unroll 8
-            for (int rr = 0; rr < 32; ++rr) sum += red[rr * 33 + lane];
-            atomicAdd(ep.colsum + cb + lane, sum);
-            __syncwarp();
-          }
-        }
-        uint32_t pk[16];
-#pragma unroll
-        for (int j = 0; j < 16; ++j) pk[j] = pack_bf16(v[2 * j], v[2 * j + 1]);
-        if (ep.out_bf16) {
-          uint4* o = reinterpret_cast<uint4*>(ep.out_bf16 + row * ep.ldo + cb);
-#pragma unroll
-          for (int q = 0; q < 4; ++q) o[q] = make_uint4(pk[4 * q], pk[4 * q + 1], pk[4 * q + 2], pk[4 * q + 3]);
-        }
-        if (ep.out_t) {
-          uint16_t* t = reinterpret_cast<uint16_t*>(ep.out_t);
-#pragma unroll
-          for (int j = 0; j < 32; ++j)
-            t[(cb + j) * ep.ldt + row] = (uint16_t)((j & 1) ? (pk[j >> 1] >> 16) : (pk[j >> 1] & 0xFFFFu));
-        }
-      }
-    }
-  }
+  if (ok) epilogue<BN, EPI>(taddr, m0, n0, ep, smem, warp, lane);
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 0)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(taddr), "r"(TCOLS) : "memory");
+}
+
+
+// K-major, 128-byte-swizzled shared-memory matrix descriptor (layout type 2): rows of 128 B
+// (64 bf16) with 16-byte chunks XOR-swizzled by row % 8, 8-row atoms 1024 B apart (stride
+// byte offset), leading byte offset unused (16 B); the tile starts 1024-byte aligned and
+// K step s (16 bf16 = 32 B) is addressed by advancing the start address 32 B.
+__device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)1u << 16;
+  d |= (uint64_t)(1024u >> 4) << 32;
+  d |= (uint64_t)1u << 46;
+  d |= (uint64_t)2u << 61;
+  return d;
+}
+
+constexpr int TS = 4;  // TMA pipeline stages
+
+// Tensor-core GEMM fed by TMA.  Thread 0 arms each stage's `full` barrier with the stage's
+// byte count and issues two 2-D bulk tensor loads (A tile 128 x 64, B tile BN x 64, 128-byte
+// swizzle) for up to TS chunks ahead, issues the four MMAs of a chunk once its stage is full,
+// commits them to the stage's `empty` barrier and refills the stage after they completed.
+// Every wait is bounded; on a timeout the kernel records the error, drains the loads it
+// issued (bounded), frees tensor memory and leaves the tile unwritten.
+template <int BN, int EPI>
+__global__ void __launch_bounds__(GT) umma_tma_gemm_kernel(const __grid_constant__ CUtensorMap ta,
+                                                           const __grid_constant__ CUtensorMap tb, int k_per_cta,
+                                                           EpiArgs ep, unsigned* __restrict__ err) {
+  static_assert(BN % 32 == 0 && BN >= 32 && BN <= 256, "tile width");
+  constexpr uint32_t TCOLS = BN <= 32 ? 32 : BN <= 64 ? 64 : BN <= 128 ? 128 : 256;
+  constexpr uint32_t A_BYTES = GM * 128, B_BYTES = BN * 128, STAGE = A_BYTES + B_BYTES;
+  static_assert(STAGE % 1024 == 0, "stages stay 1024-byte aligned");
+  static_assert(STAGE >= 4 * 32 * 33 * 4, "epilogue reduction scratch reuses a stage");
+  extern __shared__ uint8_t smem_raw[];
+  __shared__ __align__(8) uint64_t full[TS], empty[TS];
+  __shared__ uint32_t tmem_base;
+  __shared__ int s_fail;
+  uint8_t* smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int64_t m0 = (int64_t)blockIdx.x * GM, n0 = (int64_t)blockIdx.y * BN;
+  const int64_t k_begin = (int64_t)blockIdx.z * k_per_cta;
+  const int n_chunks = k_per_cta / KC;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                 :: "r"(smem_u32(&tmem_base)), "r"(TCOLS) : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    for (int i = 0; i < TS; ++i) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(&full[i])), "r"(1) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(&empty[i])), "r"(1) : "memory");
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    s_fail = 0;
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t taddr = tmem_base;
+
+  if (tid == 0) {
+    auto issue = [&](int c) {
+      const int st = c % TS;
+      const uint32_t a_dst = smem_u32(smem + st * STAGE), b_dst = a_dst + A_BYTES;
+      const uint32_t fb = smem_u32(&full[st]);
+      const int x = (int)(k_begin + (int64_t)c * KC);
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(fb), "r"(STAGE) : "memory");
+      asm volatile(
+          "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+          :: "r"(a_dst), "l"(reinterpret_cast<uint64_t>(&ta)), "r"(x), "r"((int)m0), "r"(fb) : "memory");
+      asm volatile(
+          "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+          :: "r"(b_dst), "l"(reinterpret_cast<uint64_t>(&tb)), "r"(x), "r"((int)n0), "r"(fb) : "memory");
+    };
+    int issued = 0, consumed = 0;
+    bool ok = true;
+    for (; issued < n_chunks && issued < TS; ++issued) issue(issued);
+    constexpr uint32_t idesc = instr_desc(GM, BN);
+    for (int c = 0; c < n_chunks; ++c) {
+      const int st = c % TS;
+      if (!mbar_wait(smem_u32(&full[st]), (uint32_t)((c / TS) & 1))) {
+        ok = false;
+        break;
+      }
+      consumed = c + 1;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t a0 = smem_u32(smem + st * STAGE), b0 = a0 + A_BYTES;
+#pragma unroll
+      for (int k = 0; k < KC / 16; ++k) {
+        const uint64_t ad = smem_desc_sw128(a0 + k * 32), bd = smem_desc_sw128(b0 + k * 32);
+        const uint32_t acc = (c > 0 || k > 0) ? 1u : 0u;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+            :: "r"(taddr), "l"(ad), "l"(bd), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+            : "memory");
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                   :: "r"(smem_u32(&empty[st])) : "memory");
+      if (issued < n_chunks) {
+        // the stage is refilled once the MMAs that read it completed
+        if (!mbar_wait(smem_u32(&empty[st]), (uint32_t)((c / TS) & 1))) {
+          ok = false;
+          break;
+        }
+        issue(issued++);
+      }
+    }
+    if (!ok) {
+      s_fail = 1;
+      atomicOr(err, 1u);
+      for (int c = consumed; c < issued; ++c) (void)mbar_wait(smem_u32(&full[c % TS]), (uint32_t)((c / TS) & 1));
+    }
+  }
+  __syncthreads();
+  bool ok = s_fail == 0;
+  if (ok && n_chunks > 0) {
+    const int last = n_chunks - 1;
+    ok = __syncthreads_and(mbar_wait(smem_u32(&empty[last % TS]), (uint32_t)((last / TS) & 1)));
+    if (!ok && tid == 0) atomicOr(err, 1u);
+  }
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (ok) epilogue<BN, EPI>(taddr, m0, n0, ep, smem, warp, lane);
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(taddr), "r"(TCOLS) : "memory");
+}
+
+template <int BN>
+constexpr size_t tma_gemm_smem() {
+  return (size_t)TS * (GM + BN) * 128 + 1024;
 }
 
 template <int BN>
@@ -379,6 +523,65 @@ void launch_gemm(const bf16* A, int64_t lda, const bf16* B, int64_t ldb, int64_t
   dim3 grid((unsigned)(M / GM), (unsigned)(N / BN), (unsigned)ksplit);
   umma_gemm_kernel<BN, EPI, GATHER><<<grid, GT, gemm_smem<BN>(), s>>>(A, (int)lda, B, (int)ldb, (int)(K / ksplit),
                                                                       ep, g, err);
+  UB_LAUNCH_CHECK();
+}
+
+
+// ------------------------------------------------------------------------------ TMA tensor maps
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_tiled() {
+  static std::mutex mu;
+  static EncodeTiledFn fn = nullptr;
+  std::lock_guard<std::mutex> lock(mu);
+  if (!fn) {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    UB_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q));
+    if (q != cudaDriverEntryPointSuccess || !f) throw Error(CUDA, "cuTensorMapEncodeTiled is not available");
+    fn = reinterpret_cast<EncodeTiledFn>(f);
+  }
+  return fn;
+}
+
+// Tensor map of a row-major bf16 matrix [rows, cols] (row stride ld elements) read in boxes of
+// box_rows x 64 with 128-byte swizzle.
+CUtensorMap bf16_tile_map(const void* base, int64_t rows, int64_t cols, int64_t ld, int box_rows) {
+  if (reinterpret_cast<uintptr_t>(base) % 16 || (ld * 2) % 16 || cols < KC || rows < box_rows)
+    throw Error(INVALID_ARGUMENT, "TMA operand must be 16-byte aligned with 16-byte rows");
+  CUtensorMap m;
+  const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
+  const cuuint32_t box[2] = {(cuuint32_t)KC, (cuuint32_t)box_rows};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r = encode_tiled()(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides,
+                                    box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) throw Error(CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+  return m;
+}
+
+template <int BN, int EPI>
+void prepare_tma_gemm() {
+  UB_CUDA(cudaFuncSetAttribute(umma_tma_gemm_kernel<BN, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)tma_gemm_smem<BN>()));
+}
+
+// C = A[M,K] B[N,K]^T through the TMA-fed kernel; K split into `ksplit` parts as launch_gemm.
+template <int BN, int EPI>
+void launch_tma_gemm(const bf16* A, int64_t lda, const bf16* B, int64_t ldb, int64_t M, int64_t N, int64_t K,
+                     int ksplit, const EpiArgs& ep, unsigned* err, cudaStream_t s) {
+  if (M <= 0 || M % GM || N <= 0 || N % BN || K <= 0 || ksplit < 1 || K % ((int64_t)KC * ksplit) ||
+      M / GM > 0x7FFFFFFF || ksplit > 65535 || K > 0x7FFFFFFF || M > 0x7FFFFFFF || N > 0x7FFFFFFF)
+    throw Error(INVALID_ARGUMENT, "tensor-core GEMM shape: M % 128, N % tile, K % (64 * splits), rows of 16 bytes");
+  if (ksplit > 1 && !(EPI == EPI_F32_ATOMIC || (EPI == EPI_F32 && ep.split_stride > 0)))
+    throw Error(INVALID_ARGUMENT, "split K needs per-split output slices or the atomic epilogue");
+  const CUtensorMap ta = bf16_tile_map(A, M, K, lda, GM);
+  const CUtensorMap tb = bf16_tile_map(B, N, K, ldb, BN);
+  dim3 grid((unsigned)(M / GM), (unsigned)(N / BN), (unsigned)ksplit);
+  umma_tma_gemm_kernel<BN, EPI><<<grid, GT, tma_gemm_smem<BN>(), s>>>(ta, tb, (int)(K / ksplit), ep, err);
   UB_LAUNCH_CHECK();
 }
 
@@ -638,6 +841,17 @@ __global__ void column_stats_kernel(const float* __restrict__ X, int64_t n, int 
 
 inline unsigned grid_for(int64_t n, unsigned bt) { return (unsigned)((n + bt - 1) / bt); }
 
+// Sort keys of one epoch's shuffle: splitmix64 finaliser of (seed, epoch, row), top 32 bits.
+__global__ void shuffle_keys_kernel(uint32_t* __restrict__ keys, int64_t n, uint64_t seed, uint32_t epoch) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint64_t z = seed * 0x9E3779B97F4A7C15ull + ((uint64_t)epoch << 32) + (uint64_t)i + 0x632BE59BD9B4E019ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  z ^= z >> 31;
+  keys[i] = (uint32_t)(z >> 32);
+}
+
 bool graphs_enabled() {
   const char* e = std::getenv("UMAP_B200_GRAPH");
   return !(e && e[0] == '0');
@@ -657,14 +871,15 @@ void prepare_all_gemms() {
   std::lock_guard<std::mutex> lock(mu);
   if (prepared) return;
   prepare_gemm<64, EPI_BIAS_GELU, true>();
-  prepare_gemm<64, EPI_BIAS_GELU>();
-  prepare_gemm<64, EPI_GELU_GRAD>();
-  prepare_gemm<64, EPI_F32>();
-  prepare_gemm<256, EPI_F32>();
-  prepare_gemm<128, EPI_F32>();
-  prepare_gemm<32, EPI_F32>();
-  prepare_gemm<256, EPI_F32_ATOMIC>();
-  prepare_gemm<64, EPI_F32_ATOMIC>();
+  prepare_tma_gemm<64, EPI_BIAS_GELU>();
+  prepare_tma_gemm<64, EPI_GELU_GRAD>();
+  prepare_tma_gemm<64, EPI_F32>();
+  prepare_tma_gemm<256, EPI_F32>();
+  prepare_tma_gemm<128, EPI_F32>();
+  prepare_tma_gemm<32, EPI_F32>();
+  prepare_tma_gemm<256, EPI_F32_ATOMIC>();
+  prepare_tma_gemm<64, EPI_F32_ATOMIC>();
+  (void)encode_tiled();
   prepared = true;
 }
 
@@ -864,7 +1079,7 @@ static void run_batch(Mlp::Impl& m, const float* X, const uint32_t* rows, int64_
   e2.out_f32 = train ? m.z2.p : nullptr;
   e2.out_bf16 = m.h2.p;
   e2.ldo = HID;
-  launch_gemm<64, EPI_BIAS_GELU>(m.h1.p, HID, m.w2b.p, HID, B, HID, HID, 1, e2, m.err.p, s);
+  launch_tma_gemm<64, EPI_BIAS_GELU>(m.h1.p, HID, m.w2b.p, HID, B, HID, HID, 1, e2, m.err.p, s);
   const float inv = 1.0f / (float)(B * m.out_dim);
 #define UB_OUT_ARGS                                                                                                   \
   m.h2.p, m.z2.p, m.w3b.p, m.w.p + m.o_b3, train ? Y : nullptr, rows, n_valid, inv, y_out, m.dz2.p, m.dz2t.p, B, \
@@ -886,7 +1101,7 @@ static void run_batch(Mlp::Impl& m, const float* X, const uint32_t* rows, int64_
   e4.out_f32 = m.part2.p;
   e4.split_stride = (int64_t)HID * HID;
   e4.ldo = HID;
-  launch_gemm<64, EPI_F32>(m.dz2t.p, B, m.h1t.p, B, HID, HID, B, m.ks2, e4, m.err.p, m.s2);
+  launch_tma_gemm<64, EPI_F32>(m.dz2t.p, B, m.h1t.p, B, HID, HID, B, m.ks2, e4, m.err.p, m.s2);
   UB_CUDA(cudaEventRecord(m.join, m.s2));
   // dH1 = dZ2 W2 (B operand W2^T: row i = column i of W2); dZ1 = dH1 * gelu'(Z1), kept
   // transposed for dW1; db1 = its column sums.
@@ -896,13 +1111,13 @@ static void run_batch(Mlp::Impl& m, const float* X, const uint32_t* rows, int64_
   e3.colsum = g + m.o_b1;
   e3.ldo = HID;
   e3.ldt = (int)B;
-  launch_gemm<64, EPI_GELU_GRAD>(m.dz2.p, HID, m.w2t.p, HID, B, HID, HID, 1, e3, m.err.p, s);
+  launch_tma_gemm<64, EPI_GELU_GRAD>(m.dz2.p, HID, m.w2t.p, HID, B, HID, HID, 1, e3, m.err.p, s);
   // dW1 = dZ1^T X
   EpiArgs e5{};
   e5.out_f32 = m.part1.p;
   e5.split_stride = (int64_t)HID * m.in_dim;
   e5.ldo = m.in_dim;
-  launch_gemm<64, EPI_F32>(m.dz1t.p, B, m.xt.p, B, HID, m.in_dim, B, m.ks1, e5, m.err.p, s);
+  launch_tma_gemm<64, EPI_F32>(m.dz1t.p, B, m.xt.p, B, HID, m.in_dim, B, m.ks1, e5, m.err.p, s);
   UB_CUDA(cudaStreamWaitEvent(s, m.join, 0));
   if (!with_adam) return;
   AdamArgs a{};
@@ -966,25 +1181,18 @@ void Mlp::train(const float* X, const float* Y, int64_t n, int epochs, int64_t b
   if (epochs == 0) return;
   m.ensure(batch, true);
   m.ensure_slices(batch);
-  // Shuffles: Fisher-Yates driven by splitmix64(seed), one permutation per epoch, uploaded once.
+  // Shuffles on the device: epoch e orders the rows by a 32-bit hash of (seed, e, row)
+  // (stable radix sort, so equal hashes keep row order); the first steps * batch rows of
+  // each epoch's order are its batches.
   const int64_t per_epoch = steps * batch;
-  std::vector<uint32_t> perm((size_t)epochs * per_epoch);
-  std::vector<uint32_t> p0(n);
-  uint64_t st = seed;
-  auto next = [&]() {
-    uint64_t z = (st += 0x9E3779B97F4A7C15ull);
-    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
-    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
-    return z ^ (z >> 31);
-  };
+  DevBuf<uint32_t> hkeys((uint64_t)n, s), hsorted((uint64_t)n, s), dperm((uint64_t)epochs * n, s);
+  DevBuf<uint32_t> cur(per_epoch, s);
   for (int e = 0; e < epochs; ++e) {
-    for (int64_t i = 0; i < n; ++i) p0[i] = (uint32_t)i;
-    for (int64_t i = n - 1; i > 0; --i) std::swap(p0[i], p0[(int64_t)(next() % (uint64_t)(i + 1))]);
-    std::copy(p0.begin(), p0.begin() + per_epoch, perm.begin() + (size_t)e * per_epoch);
+    shuffle_keys_kernel<<<grid_for(n, 256), 256, 0, s>>>(hkeys.p, n, seed, (uint32_t)e);
+    UB_LAUNCH_CHECK();
+    radix_sort_pairs(hkeys.p, nullptr, hsorted.p, dperm.p + (int64_t)e * n, (uint64_t)n, 32, s);
   }
-  DevBuf<uint32_t> dperm(perm.size(), s), cur(per_epoch, s);
   DevBuf<float> dloss(epochs, s);
-  UB_CUDA(cudaMemcpyAsync(dperm.p, perm.data(), perm.size() * 4, cudaMemcpyHostToDevice, s));
   UB_CUDA(cudaMemsetAsync(m.g.p, 0, m.P * 4, s));
   auto one_epoch = [&]() {
     for (int64_t t = 0; t < steps; ++t) run_batch(m, X, cur.p + t * batch, batch, batch, Y, nullptr, true, lr);
@@ -1014,7 +1222,7 @@ void Mlp::train(const float* X, const float* Y, int64_t n, int epochs, int64_t b
   } guard{exec};
   const uint64_t launches_per_epoch = (uint64_t)steps * 7;
   for (int e = 0; e < epochs; ++e) {
-    UB_CUDA(cudaMemcpyAsync(cur.p, dperm.p + (int64_t)e * per_epoch, per_epoch * 4, cudaMemcpyDeviceToDevice, s));
+    UB_CUDA(cudaMemcpyAsync(cur.p, dperm.p + (int64_t)e * n, per_epoch * 4, cudaMemcpyDeviceToDevice, s));
     UB_CUDA(cudaMemsetAsync(m.loss.p, 0, 4, s));
     if (exec) {
       UB_CUDA(cudaGraphLaunch(exec, s));
@@ -1065,17 +1273,17 @@ void umma_gemm_f32(const void* A, const void* B, float* C, int64_t M, int64_t N,
   const bf16* a = static_cast<const bf16*>(A);
   const bf16* b = static_cast<const bf16*>(B);
   if (ksplit > 1) {
-    if (N % 256 == 0) launch_gemm<256, EPI_F32_ATOMIC>(a, K, b, K, M, N, K, ksplit, ep, err.p, s);
-    else if (N % 64 == 0) launch_gemm<64, EPI_F32_ATOMIC>(a, K, b, K, M, N, K, ksplit, ep, err.p, s);
+    if (N % 256 == 0) launch_tma_gemm<256, EPI_F32_ATOMIC>(a, K, b, K, M, N, K, ksplit, ep, err.p, s);
+    else if (N % 64 == 0) launch_tma_gemm<64, EPI_F32_ATOMIC>(a, K, b, K, M, N, K, ksplit, ep, err.p, s);
     else throw Error(INVALID_ARGUMENT, "split-K GEMM needs N % 64 == 0");
   } else if (N % 256 == 0) {
-    launch_gemm<256, EPI_F32>(a, K, b, K, M, N, K, 1, ep, err.p, s);
+    launch_tma_gemm<256, EPI_F32>(a, K, b, K, M, N, K, 1, ep, err.p, s);
   } else if (N % 128 == 0) {
-    launch_gemm<128, EPI_F32>(a, K, b, K, M, N, K, 1, ep, err.p, s);
+    launch_tma_gemm<128, EPI_F32>(a, K, b, K, M, N, K, 1, ep, err.p, s);
   } else if (N % 64 == 0) {
-    launch_gemm<64, EPI_F32>(a, K, b, K, M, N, K, 1, ep, err.p, s);
+    launch_tma_gemm<64, EPI_F32>(a, K, b, K, M, N, K, 1, ep, err.p, s);
   } else if (N % 32 == 0) {
-    launch_gemm<32, EPI_F32>(a, K, b, K, M, N, K, 1, ep, err.p, s);
+    launch_tma_gemm<32, EPI_F32>(a, K, b, K, M, N, K, 1, ep, err.p, s);
   } else {
     throw Error(INVALID_ARGUMENT, "GEMM N must be a multiple of 32");
   }

@@ -41,7 +41,7 @@ using bf16 = __nv_bfloat16;
 
 constexpr int GM = 128;   // tile rows (UMMA M)
 constexpr int KC = 64;    // K staged per chunk
-constexpr int GT = 128;   // threads per GEMM CTA
+constexpr int GT = 256;   // threads per GEMM CTA: warps w and w + 4 share TMEM lanes, split columns
 constexpr int HID = 256;  // hidden width
 
 enum Epi : int {
@@ -139,11 +139,15 @@ template <int BN, int EPI>
 __device__ __forceinline__ void epilogue(uint32_t taddr, int64_t m0, int64_t n0, const EpiArgs& ep,
                                          uint8_t* scratch, int warp, int lane) {
   uint8_t* smem = scratch;
-  const int64_t row = m0 + warp * 32 + lane;
+  // warp w reads TMEM lanes 32 * (w % 4) .. + 31 (its rows) and the columns of half w / 4
+  const int quarter = warp & 3, half = warp >> 2;
+  constexpr int HALF = BN >= 64 ? BN / 2 : BN;
+  if (BN < 64 && half) return;
+  const int64_t row = m0 + quarter * 32 + lane;
 #pragma unroll 1
-  for (int c0 = 0; c0 < BN; c0 += 32) {
+  for (int c0 = half * HALF; c0 < (half + 1) * HALF; c0 += 32) {
     uint32_t r[32];
-    const uint32_t ta = taddr + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+    const uint32_t ta = taddr + ((uint32_t)(quarter * 32) << 16) + (uint32_t)c0;
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
         "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
@@ -232,7 +236,7 @@ __global__ void __launch_bounds__(GT) umma_gemm_kernel(const bf16* __restrict__ 
   static_assert(BN % 32 == 0 && BN >= 32 && BN <= 256, "tile width");
   constexpr uint32_t TCOLS = BN <= 32 ? 32 : BN <= 64 ? 64 : BN <= 128 ? 128 : 256;
   constexpr int STAGE = (GM + BN) * KC * 2;  // bytes of one K chunk of A and B
-  static_assert(STAGE >= 4 * 32 * 33 * 4, "epilogue reduction scratch reuses a stage");
+  static_assert(2 * STAGE >= 8 * 32 * 33 * 4, "epilogue reduction scratch reuses the stages");
   extern __shared__ __align__(1024) uint8_t smem[];  // two stages: [A | B] [A | B]
   __shared__ __align__(8) uint64_t mbar[2];          // MMA completion, one per stage
   __shared__ uint32_t tmem_base;
@@ -392,7 +396,7 @@ __global__ void __launch_bounds__(GT) umma_tma_gemm_kernel(const __grid_constant
   constexpr uint32_t TCOLS = BN <= 32 ? 32 : BN <= 64 ? 64 : BN <= 128 ? 128 : 256;
   constexpr uint32_t A_BYTES = GM * 128, B_BYTES = BN * 128, STAGE = A_BYTES + B_BYTES;
   static_assert(STAGE % 1024 == 0, "stages stay 1024-byte aligned");
-  static_assert(STAGE >= 4 * 32 * 33 * 4, "epilogue reduction scratch reuses a stage");
+  static_assert(2 * STAGE >= 8 * 32 * 33 * 4, "epilogue reduction scratch reuses the stages");
   extern __shared__ uint8_t smem_raw[];
   __shared__ __align__(8) uint64_t full[TS], empty[TS];
   __shared__ uint32_t tmem_base;
@@ -858,10 +862,11 @@ bool graphs_enabled() {
 }
 
 // Split of a batch-row contraction of length K over `tiles` output tiles: the largest power
-// of two that keeps about 128 CTAs and whole 64-row chunks per split.
+// of two that keeps about 64 CTAs and whole 64-row chunks per split (the TMA pipeline keeps
+// a CTA's chunks in flight, so fewer, longer splits cost less than more slices to sum).
 int k_splits(int64_t K, int tiles) {
   int ks = 1;
-  while ((int64_t)ks * 2 * tiles <= 128 && K % ((int64_t)KC * ks * 2) == 0) ks *= 2;
+  while ((int64_t)ks * 2 * tiles <= 64 && K % ((int64_t)KC * ks * 2) == 0) ks *= 2;
   return ks;
 }
 

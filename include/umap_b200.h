@@ -139,8 +139,8 @@ int umap_optimizer_manifold(const umap_optimizer* opt, const umap_manifold** out
 /* into_fitted (optimizer.rs:397-403).  Consumes `opt`. */
 int umap_optimizer_into_fitted(umap_optimizer* opt, const umap_config* cfg, umap_fitted** out);
 int umap_optimizer_free(umap_optimizer* opt);
-/* Extension (the reference has no seed API; its RNG is unseeded): the Philox key for
- * negative sampling.  Default 0. */
+/* Extension (the reference has no seed API; its RNG is unseeded): the seed of the
+ * counter-based generator that draws negative samples.  Default 0. */
 int umap_optimizer_set_seed(umap_optimizer* opt, uint64_t seed);
 /* Number of kept edges (the reference's head/tail length, optimizer.rs:133-163). */
 int umap_optimizer_n_edges(const umap_optimizer* opt, uint64_t* out);

@@ -44,24 +44,24 @@ constexpr uint32_t PAD_ROW = 0xFFFFFFFFu;
 #ifndef UB_SGD_KERNEL
 #define UB_SGD_KERNEL 2      // 1: warp-batched entries, 2: independent lane progress
 #endif
-#ifndef UB_PHILOX_ROUNDS
-#define UB_PHILOX_ROUNDS 10
-#endif
 
-// ------------------------------------------------------------------------------ Philox
-// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as easy as 1, 2, 3",
-// SC'11): counter-based, so every (seed, entry, epoch, block) has its own stream.
-__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k) {
-#pragma unroll
-  for (int r = 0; r < UB_PHILOX_ROUNDS; ++r) {
-    const uint32_t hi0 = __umulhi(0xD2511F53u, c.x), lo0 = 0xD2511F53u * c.x;
-    const uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u * c.z;
-    c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
-    k.x += 0x9E3779B9u;
-    k.y += 0xBB67AE85u;
-  }
-  return c;
+// ------------------------------------------------------------------------------ negatives' RNG
+// Counter-based: the firing of entry `idx` at `epoch` draws its negatives in pairs; pair t is
+// the SplitMix64 finaliser (Steele, Lea, Flood, "Fast splittable pseudorandom number
+// generators", OOPSLA 2014) of a counter derived from (seed, idx, epoch, t), and each 32-bit
+// half maps to [0, n) by a multiply-high.  The reference draws from an unseeded thread-local
+// generator (optimize_layout_euclidean.rs:314), so parity with it is statistical.
+__device__ __forceinline__ uint64_t mix64(uint64_t z) {
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
 }
+struct NegRng {
+  uint64_t base;
+  __device__ __forceinline__ NegRng(uint64_t seed, uint64_t idx, uint32_t epoch)
+      : base(seed ^ (idx * 0x9E3779B97F4A7C15ull) ^ ((uint64_t)epoch * 0xC2B2AE3D27D4EB4Full)) {}
+  __device__ __forceinline__ uint64_t pair(uint32_t t) const { return mix64(base + (uint64_t)t * 0xD1B54A32D192ED03ull); }
+};
 
 // ------------------------------------------------------------------------------ schedule
 __host__ __device__ __forceinline__ uint32_t q_minus_1(double eps) {
@@ -84,22 +84,40 @@ __device__ __forceinline__ uint32_t fire_epoch(uint64_t m, uint32_t q) {
   for (int t = 0; t < 8 && fires_by(x, q) < m; ++t) ++x;
   return x;
 }
-// Negatives drawn by the firing at epoch n with index m >= 1 (n * neg < 2^32 is checked on
-// the host).
-__device__ __forceinline__ uint32_t negatives_at(uint32_t n, uint64_t m, uint32_t q, uint32_t neg) {
-  const int64_t y = (int64_t)fires_by(n * neg, q);
-  const int64_t prev = m <= 1 ? 1 : (int64_t)fires_by(fire_epoch(m - 1, q) * neg, q);
-  const int64_t d = y - prev;
-  return d > 0 ? (uint32_t)d : 0u;
-}
+
 // Negatives drawn in total after m firings.
 __device__ __forceinline__ uint64_t negatives_after(uint64_t m, uint32_t q, uint32_t neg) {
   if (m == 0) return 0;
   const int64_t t = (int64_t)fires_by(fire_epoch(m, q) * neg, q) - 1;
   return t > 0 ? (uint64_t)t : 0ull;
 }
+// Fires at epoch n iff fires_by(n) > fires_by(n - 1), i.e. iff the low 32 bits of (n - 1) * Q
+// are at least 2^32 - Q (Q <= 2^32, so the count grows by at most one): one 32-bit multiply.
 __device__ __forceinline__ bool fires_at(uint32_t n, uint32_t q) {
-  return n > 0 && fires_by(n, q) > fires_by(n - 1, q);
+  const uint32_t nm1 = n - 1u;
+  return n > 0 && nm1 * q + nm1 >= ~q;
+}
+// Negatives drawn by the firing at epoch n (n * neg < 2^32 is checked on the host):
+// y(n) - y(p) with y(x) = fires_by(x * neg) and p the epoch of the previous firing, or
+// y(n) - 1 for the first.  Firings are floor(2^32 / Q) or one more epochs apart, so p is found
+// among a few candidates below n - floor(2^32 / Q) + 1 with the cheap test above.
+__device__ __forceinline__ uint32_t negatives_at(uint32_t n, uint32_t q, uint32_t neg) {
+  const int64_t y = (int64_t)fires_by(n * neg, q);
+  const uint64_t m = fires_by(n, q);
+  int64_t prev = 1;
+  if (m > 1) {
+    const int64_t g0 = (int64_t)__fdividef(4294967296.0f, (float)q + 1.0f);
+    uint32_t pe = 0;
+#pragma unroll
+    for (int t = 1; t >= -2; --t) {
+      const int64_t x = (int64_t)n - g0 + t;
+      if (pe == 0 && x >= 1 && x < (int64_t)n && fires_at((uint32_t)x, q)) pe = (uint32_t)x;
+    }
+    if (pe == 0) pe = fire_epoch(m - 1, q);
+    prev = (int64_t)fires_by(pe * neg, q);
+  }
+  const int64_t d = y - prev;
+  return d > 0 ? (uint32_t)d : 0u;
 }
 
 // Rust f32::clamp(-4, 4) (utils/clip.rs:13-15): NaN passes through.
@@ -164,27 +182,27 @@ __device__ __forceinline__ void sub_row(float* p, const float (&g)[DIM]) {
 template <int DIM>
 __device__ __forceinline__ void fired_edge(float (&cur)[DIM], uint32_t r, uint32_t k, uint32_t nneg,
                                            float* snap, const SgdParams& p, float alpha, uint64_t idx,
-                                           uint32_t epoch, uint2 key, uint32_t seg_lo, uint32_t seg_n) {
+                                           uint32_t epoch, uint64_t seed, uint32_t seg_lo, uint32_t seg_n) {
   const float a = p.a, b = p.b;
   float* oth = snap + (uint64_t)k * DIM;
   float o[DIM];
   load_row<DIM>(o, oth);
-  // Negative q uses word (q & 3) of Philox block (q >> 2) for this (entry, epoch).
+  // Negative q uses half (q & 1) of pair (q >> 1) for this (entry, epoch).
   uint32_t kk[NEG_BATCH];
   float ob[NEG_BATCH][DIM];
-  uint4 rnd = make_uint4(0, 0, 0, 0);
-  uint32_t rblk = 0xFFFFFFFFu;
+  const NegRng rng(seed, idx, epoch);
+  uint64_t rnd = 0;
+  uint32_t rpair = 0xFFFFFFFFu;
   auto fetch = [&](uint32_t q0) {
 #pragma unroll
     for (int q = 0; q < NEG_BATCH; ++q) {
       const uint32_t qq = q0 + q;
       if (qq < nneg) {
-        if ((qq >> 2) != rblk) {
-          rblk = qq >> 2;
-          rnd = philox4x32_10(make_uint4((uint32_t)idx, (uint32_t)(idx >> 32), epoch, rblk), key);
+        if ((qq >> 1) != rpair) {
+          rpair = qq >> 1;
+          rnd = rng.pair(rpair);
         }
-        const uint32_t w = qq & 3;
-        const uint32_t rv = w == 0 ? rnd.x : w == 1 ? rnd.y : w == 2 ? rnd.z : rnd.w;
+        const uint32_t rv = (qq & 1) ? (uint32_t)(rnd >> 32) : (uint32_t)rnd;
         kk[q] = seg_lo + __umulhi(rv, seg_n);
         load_row<DIM>(ob[q], snap + (uint64_t)kk[q] * DIM);
       }
@@ -259,7 +277,7 @@ __global__ void __launch_bounds__(256, UB_SGD_MIN_BLOCKS) sgd_epoch_kernel(
 #pragma unroll
   for (int d = 0; d < DIM; ++d) start[d] = cur[d];
   const uint32_t n = epoch;
-  const uint2 key = make_uint2((uint32_t)p.seed, (uint32_t)(p.seed >> 32));
+  const uint64_t seed = p.seed;
 
   for (uint32_t e0 = 0; e0 < width; e0 += PF) {
     uint2 ent[PF];
@@ -277,9 +295,9 @@ __global__ void __launch_bounds__(256, UB_SGD_MIN_BLOCKS) sgd_epoch_kernel(
 #pragma unroll
       for (int t = 1; t < PF; ++t)
         if (t == j) en = ent[t];
-      const uint32_t nneg = negatives_at(n, fires_by(n, en.y), en.y, p.neg_rate);
+      const uint32_t nneg = negatives_at(n, en.y, p.neg_rate);
       const uint64_t idx = base + (uint64_t)(e0 + j) * 32 + lane;
-      fired_edge<DIM>(cur, r, en.x, nneg, snap, p, alpha, idx, epoch, key, seg_lo, seg_n);
+      fired_edge<DIM>(cur, r, en.x, nneg, snap, p, alpha, idx, epoch, seed, seg_lo, seg_n);
     }
   }
   if (active) {
@@ -328,7 +346,7 @@ __global__ void __launch_bounds__(256, UB_SGD_MIN_BLOCKS) sgd_epoch_kernel2(
 #pragma unroll
   for (int d = 0; d < DIM; ++d) start[d] = cur[d];
   const uint32_t n = epoch;
-  const uint2 key = make_uint2((uint32_t)p.seed, (uint32_t)(p.seed >> 32));
+  const uint64_t seed = p.seed;
   uint2 win[W];
   uint32_t mask = 0, ew = 0, ebase = 0;
   for (;;) {
@@ -352,9 +370,9 @@ __global__ void __launch_bounds__(256, UB_SGD_MIN_BLOCKS) sgd_epoch_kernel2(
 #pragma unroll
       for (int t = 1; t < W; ++t)
         if (t == j) en = win[t];
-      const uint32_t nneg = negatives_at(n, fires_by(n, en.y), en.y, p.neg_rate);
+      const uint32_t nneg = negatives_at(n, en.y, p.neg_rate);
       const uint64_t idx = base + (uint64_t)(ebase + j) * 32 + lane;
-      fired_edge<DIM>(cur, r, en.x, nneg, snap, p, alpha, idx, epoch, key, seg_lo, seg_n);
+      fired_edge<DIM>(cur, r, en.x, nneg, snap, p, alpha, idx, epoch, seed, seg_lo, seg_n);
     }
   }
   if (active) {
@@ -392,7 +410,7 @@ __global__ void __launch_bounds__(256) sgd_epoch_generic(
   const uint32_t dim = p.dim;
   float* cur = live + (uint64_t)r * dim;
   const uint32_t n = epoch;
-  const uint2 key = make_uint2((uint32_t)p.seed, (uint32_t)(p.seed >> 32));
+  const uint64_t seed = p.seed;
   const float a = p.a, b = p.b;
   auto add = [&](uint32_t d, float v) {
     if (split) atomicAdd(cur + d, v);
@@ -416,12 +434,12 @@ __global__ void __launch_bounds__(256) sgd_epoch_generic(
       add(d, g);
       atomicAdd(oth + d, -g);
     }
-    const uint32_t nneg = negatives_at(n, fires_by(n, en.y), en.y, p.neg_rate);
-    uint4 rnd = make_uint4(0, 0, 0, 0);
+    const uint32_t nneg = negatives_at(n, en.y, p.neg_rate);
+    const NegRng rng(seed, idx, epoch);
+    uint64_t rnd = 0;
     for (uint32_t q = 0; q < nneg; ++q) {
-      if ((q & 3) == 0)
-        rnd = philox4x32_10(make_uint4((uint32_t)idx, (uint32_t)(idx >> 32), epoch, q >> 2), key);
-      const uint32_t rv = (q & 3) == 0 ? rnd.x : (q & 3) == 1 ? rnd.y : (q & 3) == 2 ? rnd.z : rnd.w;
+      if ((q & 1) == 0) rnd = rng.pair(q >> 1);
+      const uint32_t rv = (q & 1) ? (uint32_t)(rnd >> 32) : (uint32_t)rnd;
       const uint32_t kk = seg_lo + __umulhi(rv, seg_n);
       if (kk == r) continue;
       const float* ob = snap + (uint64_t)kk * dim;

@@ -39,7 +39,7 @@ constexpr uint32_t PAD_ROW = 0xFFFFFFFFu;
 #define UB_SGD_NEG_BATCH 4   // negative-sample rows fetched together
 #endif
 #ifndef UB_SGD_MIN_BLOCKS
-#define UB_SGD_MIN_BLOCKS 4  // resident 256-thread blocks per SM the register budget targets
+#define UB_SGD_MIN_BLOCKS 5  // resident 256-thread blocks per SM the register budget targets
 #endif
 #ifndef UB_SGD_KERNEL
 #define UB_SGD_KERNEL 2      // 1: warp-batched entries, 2: independent lane progress

@@ -46,7 +46,7 @@ def parse():
                     help="profiling run: build one optimizer, run --profile-epochs epochs, exit")
     ap.add_argument("--profile-epochs", type=int, default=24)
     ap.add_argument("--workload", default="gaussians_2m",
-                    choices=["gaussians_2m", "batched", "warm_start", "swiss_roll"],
+                    choices=["gaussians_2m", "batched", "warm_start", "swiss_roll", "mlp"],
                     help="batched: 4096 independent instances, 200 epochs, vs a per-instance loop; "
                          "warm_start: learned initial embedding + a shortened fit vs the plain fit")
     ap.add_argument("--sub", type=int, default=100_000, help="warm_start: subsample size")
@@ -483,6 +483,60 @@ def run_swiss_roll(a):
     print(json.dumps(line), flush=True)
 
 
+def run_mlp(a):
+    """The warm-start network alone: train 64->256->256->2 (bf16, Adam 1e-3, batch 4096) on
+    100,000 rows for 20 epochs (480 steps) and predict 2,000,000 rows; reports time per
+    training step and tensor throughput.  Inputs: seeded normal features and targets on the
+    device.  --profile: one training epoch (the bounded ncu target)."""
+    import torch
+    import umap_b200 as ub
+    torch.cuda.set_device(0)
+    g = torch.Generator(device="cuda").manual_seed(0)
+    x = torch.randn(100_000, 64, device="cuda", generator=g)
+    y = torch.randn(100_000, 2, device="cuda", generator=g)
+    xp = torch.randn(2_000_000, 64, device="cuda", generator=g)
+    net = ub.Mlp.create(64, 2, seed=0)
+    net.fit_input_norm(x)
+    if a.profile:
+        net.train(x, y, epochs=1, batch=4096)
+        torch.cuda.synchronize()
+        print(json.dumps({"profile": True, "workload": "mlp", "steps": 24}), flush=True)
+        return
+    for _ in range(max(1, a.warmup)):
+        net.train(x, y, epochs=1, batch=4096)
+        net.predict(xp)
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    launches0 = ub.kernel_launches()
+    with Clocks(0) as clk:
+        ev[0].record()
+        for _ in range(a.steps):
+            net.train(x, y, epochs=20, batch=4096)
+        ev[1].record()
+        ev[2].record()
+        for _ in range(a.steps):
+            net.predict(xp)
+        ev[3].record()
+        torch.cuda.synchronize()
+    train_ms = ev[0].elapsed_time(ev[1]) / a.steps
+    pred_ms = ev[2].elapsed_time(ev[3]) / a.steps
+    steps = 20 * (100_000 // 4096)
+    flop_step = 2 * 4096 * (64 * 256 + 256 * 256 + 256 * 2) * 3 - 2 * 4096 * 64 * 256
+    tflops = flop_step * steps / (train_ms / 1e3) / 1e12
+    pflops = 2 * 2_000_000 * (64 * 256 + 256 * 256 + 256 * 2) / (pred_ms / 1e3) / 1e12
+    pk = peaks().get("bf16_tflops")
+    print(json.dumps({"metric": "MLP training step time", "value": train_ms / steps * 1e3, "unit": "us/step",
+                      "higher_is_better": False, "n_gpus": 1, "steps": a.steps, "warmup": a.warmup,
+                      "dtype": "bf16", "data": "synthetic",
+                      "config": {"workload": "mlp 64-256-256-2 gelu, 100000 rows x 20 epochs, batch 4096; "
+                                             "predict 2000000 rows"},
+                      "train_ms": train_ms, "predict_ms": pred_ms,
+                      "roofline": {"bound": "tensor", "achieved": tflops, "peak": pk, "unit": "TFLOP/s",
+                                   "frac": tflops / pk if pk else None, "traffic": None},
+                      "predict_tflops": pflops,
+                      "gpu_launches": ub.kernel_launches() - launches0, "clocks": clk.summary()}), flush=True)
+
+
 def main():
     a = parse()
     if a.impl == "reference":
@@ -493,6 +547,8 @@ def main():
         return run_warm_start(a)
     if a.workload == "swiss_roll":
         return run_swiss_roll(a)
+    if a.workload == "mlp":
+        return run_mlp(a)
     import torch
     import umap_b200 as ub
     from umap_b200 import replicas as R

@@ -364,6 +364,18 @@ def run_warm_start(a):
     print(json.dumps(line), flush=True)
 
 
+def swiss_traffic(edges):
+    """DRAM bytes per SGD launch at `edges` kept edges, scaled from the 20M-point capture."""
+    p = os.path.join(ROOT, "profiles", "sgd_epoch_swiss_roll_20m.md")
+    try:
+        for line in open(p):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":", 1)[1].split()[0]) * edges / 332297330.0
+    except OSError:
+        pass
+    return None
+
+
 def run_swiss_roll(a):
     """HBM-bound workload: a noisy 3-D swiss roll of --n-swiss points (default 100,000,000),
     exact kNN k=15 on a uniform grid (harness, timed separately), init U[-10,10]^2, 200
@@ -469,7 +481,9 @@ def run_swiss_roll(a):
             "sgd_ms_per_fit": sgd_ms, "sgd_edge_updates_per_s": F_tot / (sgd_ms / 1e3),
             "graph_and_setup_ms": ms_step - sgd_ms,
             "roofline": {"bound": "hbm", "kernel": "sgd_epoch_kernel2<2>", "achieved": achieved, "peak": hbm,
-                         "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
+                         "unit": "GB/s", "frac": achieved / hbm, "traffic": swiss_traffic(E),
+                         "traffic_note": "DRAM bytes of one epoch-20 launch captured at 20M points "
+                                         "(profiles/sgd_epoch_swiss_roll_20m.md), scaled by kept edges",
                          "algorithmic_bytes_per_launch": alg / a.swiss_epochs,
                          "avg_launch_ms": sgd_ms / a.swiss_epochs},
             "device_memory_gb": {"total": total_mem / 1e9, "inputs_resident": (total_mem - free0) / 1e9,

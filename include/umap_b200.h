@@ -229,6 +229,22 @@ int umap_optimizer_serialize(const umap_optimizer* o, uint8_t* buf, uint64_t cap
 int umap_optimizer_deserialize(const uint8_t* buf, uint64_t len, umap_optimizer** out);
 int umap_fitted_serialize(const umap_fitted* f, uint8_t* buf, uint64_t cap, uint64_t* needed);
 int umap_fitted_deserialize(const uint8_t* buf, uint64_t len, umap_fitted** out);
+/* The same three objects in the reference's own checkpoint bytes: its serde derives
+ * (manifold.rs:14, optimizer.rs:27, embedding.rs:438, config.rs) encoded by bincode 1.3
+ * `serialize`, as its tests do (tests.rs:150, :179, :207).  Layout: fixed-width little-endian
+ * numbers, usize as u64, sequences as a u64 length then elements, Option as a u8 tag, unit
+ * enum variants as a u32 index; ndarray arrays as {v: u8 = 1, dim, data}; the sprs graph as
+ * {storage (CSR = 0), nrows, ncols, indptr, indices, data}.  The serde formats of ndarray and
+ * sprs are not in the reference tree and are restated from those crates (no Rust-written
+ * file has been checked).  Loading an Optimizer recomputes its schedule state from
+ * epochs_per_sample and current_epoch (the stored arrays are length-checked, then skipped);
+ * the disconnection counts of a loaded manifold are recomputed (edges_removed reads 0). */
+int umap_manifold_serialize_bincode(const umap_manifold* m, uint8_t* buf, uint64_t cap, uint64_t* needed);
+int umap_manifold_deserialize_bincode(const uint8_t* buf, uint64_t len, umap_manifold** out);
+int umap_optimizer_serialize_bincode(const umap_optimizer* opt, uint8_t* buf, uint64_t cap, uint64_t* needed);
+int umap_optimizer_deserialize_bincode(const uint8_t* buf, uint64_t len, umap_optimizer** out);
+int umap_fitted_serialize_bincode(const umap_fitted* f, uint8_t* buf, uint64_t cap, uint64_t* needed);
+int umap_fitted_deserialize_bincode(const uint8_t* buf, uint64_t len, umap_fitted** out);
 
 /* ---- kernel-level entry points (parity hooks, device pointers) ---------------------- */
 /* SmoothKnnDist::exec (umap/smooth_knn_dist.rs:60-198) on device arrays. */

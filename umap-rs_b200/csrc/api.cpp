@@ -377,6 +377,23 @@ void compute_kept_edges(const umap_optimizer& o, KeptEdges& K, bool want_tail, b
                K.ptr.p, nullptr, want_tail ? K.tail.p : nullptr, want_eps ? K.eps.p : nullptr, s, spp);
 }
 
+// optimizer.rs:90-102 (prune threshold) and make_epochs_per_sample.rs:26-32 (max over kept
+// weights: max_val itself is kept) from the manifold's graph and total_epochs.
+void compute_thresholds(umap_optimizer& o) {
+  cudaStream_t s = o.s();
+  const uint64_t n = o.manifold->n_vertices;
+  DevBuf<float> dmax(1, s);
+  reduce_max_f32(o.manifold->data.p, o.manifold->nnz, 0.0f, dmax.p, s);
+  float max_val = 0.0f;
+  d2h(&max_val, dmax.p, 1, s);
+  UB_CUDA(cudaStreamSynchronize(s));
+  const uint64_t default_epochs = n <= 10000 ? 500 : 200;
+  const uint64_t threshold_epochs = o.total_epochs > 10 ? o.total_epochs : default_epochs;
+  o.max_val = max_val;
+  o.threshold = max_val / (float)threshold_epochs;
+  o.max_w = (o.manifold->nnz > 0 && max_val > 0.0f) ? max_val : 1.0f;
+}
+
 // optimizer.rs:74-290.  `init` is a device array of n*dim floats on stream `s` (or host).
 std::unique_ptr<umap_optimizer> optimizer_new_impl(std::unique_ptr<umap_manifold> man, const float* init,
                                                    bool init_on_host, uint64_t rows, uint64_t dims,
@@ -409,17 +426,7 @@ std::unique_ptr<umap_optimizer> optimizer_new_impl(std::unique_ptr<umap_manifold
 
   // :90-102 threshold
   PhaseLog log(s);
-  DevBuf<float> dmax(1, s);
-  reduce_max_f32(o->manifold->data.p, o->manifold->nnz, 0.0f, dmax.p, s);
-  float max_val = 0.0f;
-  d2h(&max_val, dmax.p, 1, s);
-  UB_CUDA(cudaStreamSynchronize(s));
-  const uint64_t default_epochs = n <= 10000 ? 500 : 200;
-  const uint64_t threshold_epochs = total_epochs > 10 ? total_epochs : default_epochs;
-  o->max_val = max_val;
-  o->threshold = max_val / (float)threshold_epochs;
-  // make_epochs_per_sample.rs:26-32: max over kept weights (max_val itself is kept).
-  o->max_w = (o->manifold->nnz > 0 && max_val > 0.0f) ? max_val : 1.0f;
+  compute_thresholds(*o);
   log.mark("optimizer threshold computed");
 
   {
@@ -936,6 +943,176 @@ umap_config read_config(Reader& r) {
   c.symmetrize = r.get<int32_t>();
   c.has_n_epochs = r.get<int32_t>(); c.n_epochs = r.get<uint64_t>(); c.learning_rate = r.get<float>();
   c.negative_sample_rate = r.get<uint64_t>(); c.repulsion_strength = r.get<float>();
+  return c;
+}
+
+// Common end of loading an optimizer: validate the edge list (row-major by head, heads and
+// tails < n) on the host and rebuild the SGD layout from head / tail / epochs_per_sample (the
+// schedule state follows from epochs_per_sample and current_epoch).
+void finish_loaded_optimizer(umap_optimizer& o, const DevBuf<uint32_t>& head, const DevBuf<uint32_t>& tail,
+                             const DevBuf<double>& eps) {
+  cudaStream_t s = o.s();
+  const uint64_t n = o.manifold->n_vertices, E = head.n;
+  if (o.current_epoch > o.total_epochs) throw Error(FORMAT, "current_epoch exceeds total_epochs");
+  if (o.metric_type != UMAP_METRIC_EUCLIDEAN) throw Error(UNSUPPORTED, "only Euclidean optimizers are supported");
+  std::vector<uint32_t> hh(E), tt(E);
+  d2h(hh.data(), head.p, E, s);
+  d2h(tt.data(), tail.p, E, s);
+  UB_CUDA(cudaStreamSynchronize(s));
+  for (uint64_t i = 0; i < E; ++i) {
+    if (hh[i] >= n || tt[i] >= n) throw Error(FORMAT, "edge index out of range");
+    if (i && hh[i] < hh[i - 1]) throw Error(FORMAT, "edges are not ordered by head");
+  }
+  DevBuf<uint64_t> ptr(n + 1, s);
+  segment_starts(head.p, E, n, ptr.p, s);
+  build_sgd_layout(ptr.p, tail.p, eps.p, n, 0, o.layout, s);
+  set_l2_window(o, true);
+  UB_CUDA(cudaStreamSynchronize(s));
+}
+
+// ---- the reference's own checkpoint bytes: serde derive + bincode 1.3 `serialize`
+// bincode 1.3 (legacy options): little-endian fixed-width integers and floats, usize as u64,
+// bool as u8, Option as a u8 tag then the value, a unit enum variant as its u32 index, a
+// sequence as a u64 length then its elements, [T; N] as N elements, struct fields in
+// declaration order with no names.  ndarray 0.17 serialises an array as the struct
+// {v: u8 = 1, dim: [usize; D], data: sequence in logical (row-major) order}; sprs 0.11 a
+// CsMatI as {storage: CompressedStorage (CSR = 0), nrows, ncols, indptr: {storage: Vec<usize>},
+// indices: Vec<u32>, data: Vec<f32>}.  Those two crates are not in the reference tree, so this
+// layout is restated from their published serde implementations.
+constexpr uint8_t NDARRAY_FORMAT_VERSION = 1;
+
+template <class T>
+void bc_array1(Writer& w, const T* dev, uint64_t n, cudaStream_t s) {
+  w.put<uint8_t>(NDARRAY_FORMAT_VERSION);
+  w.put<uint64_t>(n);
+  put_device_array(w, dev, n, s);
+}
+template <class T>
+void bc_array2(Writer& w, const T* dev, uint64_t rows, uint64_t cols, cudaStream_t s) {
+  w.put<uint8_t>(NDARRAY_FORMAT_VERSION);
+  w.put<uint64_t>(rows);
+  w.put<uint64_t>(cols);
+  put_device_array(w, dev, rows * cols, s);
+}
+uint64_t bc_array_header(Reader& r, int ndim, uint64_t* dims) {
+  if (r.get<uint8_t>() != NDARRAY_FORMAT_VERSION) throw Error(FORMAT, "unknown ndarray serialization version");
+  uint64_t total = 1;
+  for (int i = 0; i < ndim; ++i) {
+    dims[i] = r.get<uint64_t>();
+    if (dims[i] && total > UINT64_MAX / dims[i]) throw Error(FORMAT, "array shape overflows");
+    total *= dims[i];
+  }
+  return total;
+}
+template <class T>
+void bc_get_array1(Reader& r, DevBuf<T>& buf, uint64_t expect, cudaStream_t s) {
+  uint64_t d;
+  const uint64_t total = bc_array_header(r, 1, &d);
+  if (expect != UINT64_MAX && total != expect) throw Error(FORMAT, "array length mismatch");
+  get_device_array(r, buf, total, s);
+}
+
+// LearnedManifold (manifold.rs:14-38): graph, sigmas, rhos, n_vertices, a, b.
+void bc_manifold(Writer& w, const umap_manifold& m) {
+  cudaStream_t s = m.s();
+  w.put<uint32_t>(0);  // CompressedStorage::CSR
+  w.put<uint64_t>(m.n_vertices);
+  w.put<uint64_t>(m.n_vertices);
+  put_device_array(w, m.indptr.p, m.n_vertices + 1, s);
+  put_device_array(w, m.indices.p, m.nnz, s);
+  put_device_array(w, m.data.p, m.nnz, s);
+  bc_array1(w, m.sigmas.p, m.n_vertices, s);
+  bc_array1(w, m.rhos.p, m.n_vertices, s);
+  w.put<uint64_t>(m.n_vertices);
+  w.put<float>(m.a);
+  w.put<float>(m.b);
+}
+
+std::unique_ptr<umap_manifold> bc_read_manifold(Reader& r) {
+  if (r.get<uint32_t>() != 0) throw Error(FORMAT, "graph is not stored as CSR");
+  const uint64_t rows = r.get<uint64_t>(), cols = r.get<uint64_t>();
+  if (rows != cols) throw Error(FORMAT, "graph must be square");
+  auto m = std::make_unique<umap_manifold>();
+  m->stream = std::make_unique<Stream>();
+  cudaStream_t s = m->s();
+  get_device_array(r, m->indptr, rows + 1, s);
+  get_device_array(r, m->indices, UINT64_MAX, s);
+  m->nnz = m->indices.n;
+  get_device_array(r, m->data, m->nnz, s);
+  bc_get_array1(r, m->sigmas, rows, s);
+  bc_get_array1(r, m->rhos, rows, s);
+  m->n_vertices = r.get<uint64_t>();
+  if (m->n_vertices != rows) throw Error(FORMAT, "n_vertices does not match the graph shape");
+  m->a = r.get<float>();
+  m->b = r.get<float>();
+  std::vector<uint64_t> ip(rows + 1);
+  std::vector<uint32_t> ix(m->nnz);
+  d2h(ip.data(), m->indptr.p, rows + 1, s);
+  d2h(ix.data(), m->indices.p, m->nnz, s);
+  UB_CUDA(cudaStreamSynchronize(s));
+  if (ip[0] != 0 || ip[rows] != m->nnz) throw Error(FORMAT, "graph indptr does not match nnz");
+  for (uint64_t i = 0; i < rows; ++i)
+    if (ip[i + 1] < ip[i]) throw Error(FORMAT, "graph indptr is not monotone");
+  for (uint64_t q = 0; q < m->nnz; ++q)
+    if (ix[q] >= cols) throw Error(FORMAT, "graph column index out of range");
+  // not part of the reference's struct: the disconnection counts are recomputed
+  DevBuf<unsigned long long> de(1, s);
+  count_empty_rows(m->indptr.p, m->data.p, rows, de.p, s);
+  unsigned long long v = 0;
+  UB_CUDA(cudaMemcpyAsync(&v, de.p, 8, cudaMemcpyDeviceToHost, s));
+  UB_CUDA(cudaStreamSynchronize(s));
+  m->vertices_disconnected = v;
+  m->edges_removed = 0;
+  return m;
+}
+
+// UmapConfig (config.rs:8-235): n_components, manifold {min_dist, spread, a, b},
+// graph {n_neighbors, local_connectivity, set_op_mix_ratio, disconnection_distance,
+// symmetrize}, optimization {n_epochs, learning_rate, negative_sample_rate, repulsion_strength}.
+void bc_config(Writer& w, const umap_config& c) {
+  w.put<uint64_t>(c.n_components);
+  w.put<float>(c.min_dist);
+  w.put<float>(c.spread);
+  w.put<uint8_t>(c.has_a ? 1 : 0);
+  if (c.has_a) w.put<float>(c.a);
+  w.put<uint8_t>(c.has_b ? 1 : 0);
+  if (c.has_b) w.put<float>(c.b);
+  w.put<uint64_t>(c.n_neighbors);
+  w.put<float>(c.local_connectivity);
+  w.put<float>(c.set_op_mix_ratio);
+  w.put<uint8_t>(c.has_disconnection_distance ? 1 : 0);
+  if (c.has_disconnection_distance) w.put<float>(c.disconnection_distance);
+  w.put<uint8_t>(c.symmetrize ? 1 : 0);
+  w.put<uint8_t>(c.has_n_epochs ? 1 : 0);
+  if (c.has_n_epochs) w.put<uint64_t>(c.n_epochs);
+  w.put<float>(c.learning_rate);
+  w.put<uint64_t>(c.negative_sample_rate);
+  w.put<float>(c.repulsion_strength);
+}
+
+umap_config bc_read_config(Reader& r) {
+  auto tag = [&]() {
+    const uint8_t t = r.get<uint8_t>();
+    if (t > 1) throw Error(FORMAT, "invalid Option tag");
+    return (int32_t)t;
+  };
+  umap_config c{};
+  c.n_components = r.get<uint64_t>();
+  c.min_dist = r.get<float>();
+  c.spread = r.get<float>();
+  if ((c.has_a = tag())) c.a = r.get<float>();
+  if ((c.has_b = tag())) c.b = r.get<float>();
+  c.n_neighbors = r.get<uint64_t>();
+  c.local_connectivity = r.get<float>();
+  c.set_op_mix_ratio = r.get<float>();
+  if ((c.has_disconnection_distance = tag())) c.disconnection_distance = r.get<float>();
+  const uint8_t sym = r.get<uint8_t>();
+  if (sym > 1) throw Error(FORMAT, "invalid bool");
+  c.symmetrize = sym;
+  if ((c.has_n_epochs = tag())) c.n_epochs = r.get<uint64_t>();
+  c.learning_rate = r.get<float>();
+  c.negative_sample_rate = r.get<uint64_t>();
+  c.repulsion_strength = r.get<float>();
   return c;
 }
 
@@ -1462,22 +1639,7 @@ int umap_optimizer_deserialize(const uint8_t* buf, uint64_t len, umap_optimizer*
   o->threshold = r.get<float>();
   o->max_w = r.get<float>();
   if (r.off != len) throw Error(FORMAT, "trailing bytes after the optimizer");
-  if (o->current_epoch > o->total_epochs) throw Error(FORMAT, "current_epoch exceeds total_epochs");
-  if (o->metric_type != UMAP_METRIC_EUCLIDEAN) throw Error(UNSUPPORTED, "only Euclidean optimizers are supported");
-  // Validate the edge list (row-major by head, heads and tails < n) on the host.
-  std::vector<uint32_t> hh(E), tt(E);
-  d2h(hh.data(), head.p, E, s);
-  d2h(tt.data(), tail.p, E, s);
-  UB_CUDA(cudaStreamSynchronize(s));
-  for (uint64_t i = 0; i < E; ++i) {
-    if (hh[i] >= n || tt[i] >= n) throw Error(FORMAT, "edge index out of range");
-    if (i && hh[i] < hh[i - 1]) throw Error(FORMAT, "edges are not ordered by head");
-  }
-  DevBuf<uint64_t> ptr(n + 1, s);
-  segment_starts(head.p, E, n, ptr.p, s);
-  build_sgd_layout(ptr.p, tail.p, eps.p, n, 0, o->layout, s);
-  set_l2_window(*o, true);
-  UB_CUDA(cudaStreamSynchronize(s));
+  finish_loaded_optimizer(*o, head, tail, eps);
   *out = o.release();
   API_END
 }
@@ -1516,6 +1678,161 @@ int umap_fitted_deserialize(const uint8_t* buf, uint64_t len, umap_fitted** out)
   r.off += cnt * 4;
   f->manifold = read_manifold(r);
   f->config = read_config(r);
+  if (r.off != len) throw Error(FORMAT, "trailing bytes after the fitted model");
+  if (f->manifold->n_vertices != f->n) throw Error(FORMAT, "embedding rows do not match the manifold");
+  f->embedding.alloc(cnt, f->s());
+  std::vector<float> tmp(host_emb, host_emb + cnt);
+  h2d(f->embedding.p, tmp.data(), cnt, f->s());
+  UB_CUDA(cudaStreamSynchronize(f->s()));
+  *out = f.release();
+  API_END
+}
+
+// ---- checkpoints in the reference's own encoding (serde derive + bincode 1.3)
+int umap_manifold_serialize_bincode(const umap_manifold* m, uint8_t* buf, uint64_t cap, uint64_t* needed) {
+  API_BEGIN
+  need(m, "manifold");
+  m->stream->activate();
+  Writer w;
+  bc_manifold(w, *m);
+  int rc = copy_out(w, buf, cap, needed);
+  if (rc) throw Error(rc, "buffer too small for the serialized manifold");
+  API_END
+}
+
+int umap_manifold_deserialize_bincode(const uint8_t* buf, uint64_t len, umap_manifold** out) {
+  API_BEGIN
+  need(buf, "buf"); need(out, "out");
+  *out = nullptr;
+  Reader r{buf, len};
+  auto m = bc_read_manifold(r);
+  if (r.off != len) throw Error(FORMAT, "trailing bytes after the manifold");
+  *out = m.release();
+  API_END
+}
+
+// Optimizer (optimizer.rs:27-56): manifold, head, tail, epochs_per_sample, embedding,
+// epoch_of_next_sample, epoch_of_next_negative_sample, epochs_per_negative_sample,
+// current_epoch, total_epochs, gamma, initial_alpha, negative_sample_rate, metric_type.
+int umap_optimizer_serialize_bincode(const umap_optimizer* o, uint8_t* buf, uint64_t cap, uint64_t* needed) {
+  API_BEGIN
+  need(o, "optimizer");
+  if (o->n_seg) throw Error(UNSUPPORTED, "checkpoints of batched optimizers are not supported");
+  o->manifold->stream->activate();
+  cudaStream_t s = o->s();
+  Writer w;
+  bc_manifold(w, *o->manifold);
+  KeptEdges K;
+  compute_kept_edges(*o, K, true, true);
+  const uint64_t E = K.E;
+  {
+    DevBuf<uint32_t> h(E, s);
+    head_from_ptr(K.ptr.p, o->manifold->n_vertices, h.p, s);
+    bc_array1(w, h.p, E, s);
+  }
+  bc_array1(w, K.tail.p, E, s);
+  bc_array1(w, K.eps.p, E, s);
+  bc_array2(w, o->emb2.p, o->n, o->dim, s);
+  {
+    DevBuf<double> a(E, s), b(E, s), c(E, s);
+    export_state(K.eps.p, E, o->negative_sample_rate, o->current_epoch, a.p, b.p, c.p, s);
+    bc_array1(w, a.p, E, s);
+    bc_array1(w, b.p, E, s);
+    bc_array1(w, c.p, E, s);
+  }
+  w.put<uint64_t>(o->current_epoch);
+  w.put<uint64_t>(o->total_epochs);
+  w.put<float>(o->gamma);
+  w.put<float>(o->initial_alpha);
+  w.put<double>((double)o->negative_sample_rate);
+  w.put<uint32_t>((uint32_t)o->metric_type);
+  int rc = copy_out(w, buf, cap, needed);
+  if (rc) throw Error(rc, "buffer too small for the serialized optimizer");
+  API_END
+}
+
+int umap_optimizer_deserialize_bincode(const uint8_t* buf, uint64_t len, umap_optimizer** out) {
+  API_BEGIN
+  need(buf, "buf"); need(out, "out");
+  *out = nullptr;
+  Reader r{buf, len};
+  auto o = std::make_unique<umap_optimizer>();
+  o->manifold = bc_read_manifold(r);
+  cudaStream_t s = o->s();
+  const uint64_t n = o->manifold->n_vertices;
+  DevBuf<uint32_t> head, tail;
+  DevBuf<double> eps;
+  bc_get_array1(r, head, UINT64_MAX, s);
+  const uint64_t E = head.n;
+  bc_get_array1(r, tail, E, s);
+  bc_get_array1(r, eps, E, s);
+  {
+    uint64_t dims[2];
+    const uint64_t total = bc_array_header(r, 2, dims);
+    if (dims[0] != n || dims[1] < 1 || dims[1] > (1u << 20)) throw Error(FORMAT, "embedding shape mismatch");
+    o->n = dims[0];
+    o->dim = dims[1];
+    DevBuf<float> e;
+    get_device_array(r, e, total, s);
+    o->emb2.alloc(2 * n * o->dim, s);
+    d2d(o->emb2.p, e.p, n * o->dim, s);
+  }
+  for (int t = 0; t < 3; ++t) {  // schedule state: recomputed from epochs_per_sample
+    uint64_t d;
+    const uint64_t total = bc_array_header(r, 1, &d);
+    if (total != E || r.count(8) != E) throw Error(FORMAT, "schedule array length mismatch");
+    r.off += E * 8;
+  }
+  o->current_epoch = r.get<uint64_t>();
+  o->total_epochs = r.get<uint64_t>();
+  o->gamma = r.get<float>();
+  o->initial_alpha = r.get<float>();
+  const double nsr = r.get<double>();
+  if (!(nsr >= 0.0 && nsr < 4294967296.0) || nsr != (double)(uint64_t)nsr)
+    throw Error(FORMAT, "negative_sample_rate is not a whole number");
+  o->negative_sample_rate = (uint64_t)nsr;
+  const uint32_t mt = r.get<uint32_t>();
+  if (mt > 1) throw Error(FORMAT, "invalid MetricType");
+  o->metric_type = (int)mt;
+  if (r.off != len) throw Error(FORMAT, "trailing bytes after the optimizer");
+  compute_thresholds(*o);
+  finish_loaded_optimizer(*o, head, tail, eps);
+  *out = o.release();
+  API_END
+}
+
+// FittedUmap (embedding.rs:438-443): embedding, manifold, config.
+int umap_fitted_serialize_bincode(const umap_fitted* f, uint8_t* buf, uint64_t cap, uint64_t* needed) {
+  API_BEGIN
+  need(f, "fitted");
+  f->manifold->stream->activate();
+  Writer w;
+  bc_array2(w, f->embedding.p, f->n, f->dim, f->s());
+  bc_manifold(w, *f->manifold);
+  bc_config(w, f->config);
+  int rc = copy_out(w, buf, cap, needed);
+  if (rc) throw Error(rc, "buffer too small for the serialized fitted model");
+  API_END
+}
+
+int umap_fitted_deserialize_bincode(const uint8_t* buf, uint64_t len, umap_fitted** out) {
+  API_BEGIN
+  need(buf, "buf"); need(out, "out");
+  *out = nullptr;
+  Reader r{buf, len};
+  auto f = std::make_unique<umap_fitted>();
+  uint64_t dims[2];
+  const uint64_t total = bc_array_header(r, 2, dims);
+  if (dims[1] > (1u << 20)) throw Error(FORMAT, "embedding shape mismatch");
+  f->n = dims[0];
+  f->dim = dims[1];
+  // The embedding precedes the manifold (which owns the stream): stage it on the host.
+  const uint64_t cnt = r.count(4);
+  if (cnt != total) throw Error(FORMAT, "embedding length mismatch");
+  const float* host_emb = (const float*)(r.p + r.off);
+  r.off += cnt * 4;
+  f->manifold = bc_read_manifold(r);
+  f->config = bc_read_config(r);
   if (r.off != len) throw Error(FORMAT, "trailing bytes after the fitted model");
   if (f->manifold->n_vertices != f->n) throw Error(FORMAT, "embedding rows do not match the manifold");
   f->embedding.alloc(cnt, f->s());

@@ -323,6 +323,14 @@ class LearnedManifold(_Handle):
     def from_bytes(b: bytes) -> "LearnedManifold":
         return LearnedManifold(_deserialize("umap_manifold_deserialize", b))
 
+    def to_bincode(self) -> bytes:
+        """The reference's own bytes: bincode::serialize(&manifold)."""
+        return _serialize("umap_manifold_serialize_bincode", self._get())
+
+    @staticmethod
+    def from_bincode(b: bytes) -> "LearnedManifold":
+        return LearnedManifold(_deserialize("umap_manifold_deserialize_bincode", b))
+
 
 def _serialize(fn, h) -> bytes:
     L = _lib.load()
@@ -577,6 +585,14 @@ class Optimizer(_Handle):
     def from_bytes(b: bytes) -> "Optimizer":
         return Optimizer(None, _handle=_deserialize("umap_optimizer_deserialize", b))
 
+    def to_bincode(self) -> bytes:
+        """The reference's own bytes: bincode::serialize(&optimizer)."""
+        return _serialize("umap_optimizer_serialize_bincode", self._get())
+
+    @staticmethod
+    def from_bincode(b: bytes) -> "Optimizer":
+        return Optimizer(None, _handle=_deserialize("umap_optimizer_deserialize_bincode", b))
+
 
 # ------------------------------------------------------------------ FittedUmap
 class FittedUmap(_Handle):
@@ -620,6 +636,14 @@ class FittedUmap(_Handle):
     @staticmethod
     def from_bytes(b: bytes) -> "FittedUmap":
         return FittedUmap(_deserialize("umap_fitted_deserialize", b))
+
+    def to_bincode(self) -> bytes:
+        """The reference's own bytes: bincode::serialize(&fitted)."""
+        return _serialize("umap_fitted_serialize_bincode", self._get())
+
+    @staticmethod
+    def from_bincode(b: bytes) -> "FittedUmap":
+        return FittedUmap(_deserialize("umap_fitted_deserialize_bincode", b))
 
 
 # ------------------------------------------------------------------ learned warm start

@@ -81,6 +81,12 @@ SIGNATURES = {
     "umap_optimizer_deserialize": [P, u64, PP],
     "umap_fitted_serialize": [P, P, u64, C.POINTER(u64)],
     "umap_fitted_deserialize": [P, u64, PP],
+    "umap_manifold_serialize_bincode": [P, P, u64, C.POINTER(u64)],
+    "umap_manifold_deserialize_bincode": [P, u64, PP],
+    "umap_optimizer_serialize_bincode": [P, P, u64, C.POINTER(u64)],
+    "umap_optimizer_deserialize_bincode": [P, u64, PP],
+    "umap_fitted_serialize_bincode": [P, P, u64, C.POINTER(u64)],
+    "umap_fitted_deserialize_bincode": [P, u64, PP],
     "umap_smooth_knn_dist_device": [P, u64, u64, u64, f32, f32, P, P],
     "umap_radix_sort_pairs_device": [P, P, P, P, u64, i32],
     "umap_radix_sort_pairs_device_noalloc": [P, P, P, P, u64, i32, P],

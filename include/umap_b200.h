@@ -40,12 +40,22 @@ enum umap_status {
   UMAP_ERR_FORMAT = 5,           /* checkpoint bytes truncated / corrupt / wrong kind */
   UMAP_ERR_IO = 6,
   UMAP_ERR_NULL = 7,             /* NULL handle or pointer                           */
-  UMAP_ERR_UNSUPPORTED = 8       /* e.g. MetricType::Generic output metric           */
+  UMAP_ERR_UNSUPPORTED = 8       /* e.g. an output metric with no device implementation */
 };
 
-enum umap_metric_type { /* umap-rs/src/metric.rs:6-12 */
+/* MetricType (umap-rs/src/metric.rs:6-12) selects the SGD update rule: the Euclidean
+ * specialisation (layout/optimize_layout_euclidean.rs) or the generic-metric rule
+ * (layout/optimize_layout_generic.rs), which calls the output metric's distance and gradient. */
+enum umap_metric_type {
   UMAP_METRIC_EUCLIDEAN = 0,
   UMAP_METRIC_GENERIC = 1
+};
+
+/* Output metrics with a device implementation, for the generic rule (the reference's
+ * `output_metric: &dyn Metric`).  The reference ships one Metric, EuclideanMetric
+ * (distances.rs:197-236): distance sqrt(sum (x-y)^2), gradient (x-y) / (distance + 1e-6). */
+enum umap_output_metric {
+  UMAP_OUTPUT_METRIC_EUCLIDEAN = 0
 };
 
 /* UmapConfig (umap-rs/src/config.rs:205-235).  Option<T> fields are a has_* flag plus a
@@ -124,8 +134,12 @@ int umap_optimizer_new_device(umap_manifold* manifold, const float* dev_init, ui
                               uint64_t dims, uint64_t total_epochs, const umap_config* cfg,
                               int metric_type, umap_optimizer** out);
 /* Optimizer::step_epochs (optimizer.rs:297-366).  UMAP_ERR_OVERSTEP with the reference's
- * message when current_epoch + n > total_epochs. */
+ * message when current_epoch + n > total_epochs.  A MetricType::Generic optimizer steps with
+ * the Euclidean output metric; _metric names the output metric (umap_output_metric) and
+ * returns UMAP_ERR_UNSUPPORTED for one without a device implementation.  A Euclidean
+ * optimizer ignores it, as the reference does. */
 int umap_optimizer_step_epochs(umap_optimizer* opt, uint64_t n);
+int umap_optimizer_step_epochs_metric(umap_optimizer* opt, uint64_t n, int output_metric);
 int umap_optimizer_current_epoch(const umap_optimizer* opt, uint64_t* out);   /* :369 */
 int umap_optimizer_total_epochs(const umap_optimizer* opt, uint64_t* out);    /* :374 */
 int umap_optimizer_remaining_epochs(const umap_optimizer* opt, uint64_t* out);/* :379 */
@@ -191,6 +205,14 @@ int umap_fit_manifold(umap_manifold* manifold, const umap_config* cfg, const flo
                       uint64_t init_rows, uint64_t init_cols, umap_fitted** out);
 int umap_fit_manifold_device(umap_manifold* manifold, const umap_config* cfg, const float* dev_init,
                              uint64_t init_rows, uint64_t init_cols, umap_fitted** out);
+/* The same with the Umap's output metric (embedding.rs:311-321): its MetricType picks the
+ * update rule and `output_metric` (umap_output_metric) is passed to step_epochs. */
+int umap_fit_manifold_metric(umap_manifold* manifold, const umap_config* cfg, const float* host_init,
+                             uint64_t init_rows, uint64_t init_cols, int metric_type, int output_metric,
+                             umap_fitted** out);
+int umap_fit_manifold_metric_device(umap_manifold* manifold, const umap_config* cfg, const float* dev_init,
+                                    uint64_t init_rows, uint64_t init_cols, int metric_type,
+                                    int output_metric, umap_fitted** out);
 
 /* ---- batched instances (no counterpart in the reference: a fit per dataset) --------
  * n_instances independent fits in one problem.  Instance s owns points

@@ -66,6 +66,7 @@ def lib():
         L.orc_optimizer_state.argtypes = [P, P, P, P]
         L.orc_optimizer_embedding.argtypes = [P, P]
         L.orc_optimizer_set_embedding.argtypes = [P, P]
+        L.orc_optimizer_set_metric_type.argtypes = [P, i32]
         L.orc_optimizer_step_epochs.argtypes = [P, u64, P, P]
         L.orc_optimizer_step_epochs.restype = i32
         _lib = L
@@ -196,7 +197,10 @@ def learn_manifold(knn_idx: np.ndarray, knn_dist: np.ndarray, cfg: OracleConfig 
 
 class Optimizer:
     def __init__(self, manifold: Manifold, init: np.ndarray, total_epochs: int,
-                 cfg: OracleConfig | None = None, seed: int = 0):
+                 cfg: OracleConfig | None = None, seed: int = 0, metric_type: int = 0):
+        """metric_type 0 = Euclidean specialisation (optimize_layout_euclidean.rs), 1 = the
+        generic-metric rule with the built-in Euclidean output metric
+        (optimize_layout_generic.rs + distances.rs)."""
         cfg = cfg or OracleConfig()
         x = np.ascontiguousarray(init, dtype=np.float32)
         self.n, self.dim = x.shape
@@ -205,6 +209,7 @@ class Optimizer:
                                          cfg.negative_sample_rate, seed)
         if not self.h:
             raise OracleError(lib().orc_last_error().decode())
+        lib().orc_optimizer_set_metric_type(self.h, int(metric_type))
 
     def __del__(self):
         if getattr(self, "h", None):
@@ -261,14 +266,14 @@ class Optimizer:
             return fires[:n], negs[:n]
 
 
-def fit(knn_idx, knn_dist, init, cfg: OracleConfig | None = None, seed: int = 0):
+def fit(knn_idx, knn_dist, init, cfg: OracleConfig | None = None, seed: int = 0, metric_type: int = 0):
     """embedding.rs:274-337: learn_manifold -> Optimizer::new -> one step_epochs call ->
     rows whose graph row sums to zero become NaN."""
     cfg = cfg or OracleConfig()
     n = knn_idx.shape[0]
     m = learn_manifold(knn_idx, knn_dist, cfg)
     total = cfg.n_epochs if cfg.n_epochs is not None else (500 if n <= 10000 else 200)
-    opt = Optimizer(m, init, total, cfg, seed=seed)
+    opt = Optimizer(m, init, total, cfg, seed=seed, metric_type=metric_type)
     opt.step_epochs(total)
     emb = opt.embedding()
     ip, _, _ = m.graph()

@@ -471,6 +471,7 @@ struct OrcOptimizer {
   double negative_sample_rate = 5;
   float max_val = 0, threshold = 0;
   uint64_t seed = 0;
+  int metric_type = 0;  // metric.rs:6-12: 0 Euclidean specialisation, 1 Generic
 };
 
 extern "C" {
@@ -687,8 +688,67 @@ void orc_optimizer_state(const OrcOptimizer* o, double* eons, double* eonns, dou
 void orc_optimizer_embedding(const OrcOptimizer* o, float* out) {
   memcpy(out, o->embedding.data(), o->embedding.size() * 4);
 }
+// MetricType of the optimizer (optimizer.rs:318-359 dispatch): 0 Euclidean, 1 Generic.
+void orc_optimizer_set_metric_type(OrcOptimizer* o, int metric_type) { o->metric_type = metric_type; }
 void orc_optimizer_set_embedding(OrcOptimizer* o, const float* in) {
   memcpy(o->embedding.data(), in, o->embedding.size() * 4);
+}
+
+// distances.rs:208-223 EuclideanMetric::distance: (sqrt(sum diff^2), (x - y) / (dist + 1e-6)).
+static float euclidean_distance(const float* x, const float* y, uint64_t dim, float* grad) {
+  float sum_sq = 0.0f;
+  for (uint64_t i = 0; i < dim; ++i) {
+    float diff = x[i] - y[i];
+    sum_sq = sum_sq + diff * diff;
+  }
+  float dist = sqrtf(sum_sq);
+  float denom = dist + 1e-6f;
+  for (uint64_t i = 0; i < dim; ++i) grad[i] = (x[i] - y[i]) / denom;
+  return dist;
+}
+
+// layout/optimize_layout_generic.rs:35-124 (move_other = true) with the built-in output
+// metric EuclideanMetric, the only Metric the reference ships.  Sequential over the edges
+// with one RNG, as the reference's generic loop is (it has no parallel variant).
+static void generic_epoch(OrcOptimizer* o, float* headp, float* tailp, uint64_t epoch, float alpha,
+                   uint64_t* fired, uint64_t* negs) {
+  const uint64_t nv = o->manifold.n_vertices, dim = o->dim, E = o->head.size();
+  const float a = o->manifold.a, b = o->manifold.b, gamma = o->gamma;
+  const double nd = (double)epoch;
+  Xoshiro256ss rng(o->seed ^ (0x9E3779B97F4A7C15ull * (epoch + 1)));
+  std::vector<float> grad(dim), rev(dim);
+  uint64_t lf = 0, ln = 0;
+  for (uint64_t i = 0; i < E; ++i) {
+    if (!(o->epoch_of_next_sample[i] <= nd)) continue;                 // :57
+    const uint64_t j = o->head[i], k = o->tail[i];
+    float* cur = headp + j * dim;
+    float* oth = tailp + k * dim;
+    float dist = euclidean_distance(cur, oth, dim, grad.data());        // :65
+    euclidean_distance(oth, cur, dim, rev.data());                      // :66
+    float w_l = dist > 0.0f ? 1.0f / (1.0f + a * powf(dist, 2.0f * b)) : 1.0f;   // :71-75
+    float grad_coeff = ((2.0f * b) * (w_l - 1.0f)) / (dist + 1e-6f);   // :76
+    for (uint64_t d = 0; d < dim; ++d) {                                // :78-86
+      cur[d] += rust_clamp(grad_coeff * grad[d], -4.0f, 4.0f) * alpha;
+      oth[d] += rust_clamp(grad_coeff * rev[d], -4.0f, 4.0f) * alpha;
+    }
+    o->epoch_of_next_sample[i] += o->epochs_per_sample[i];              // :88
+    uint64_t n_neg = rust_f64_to_usize((nd - o->epoch_of_next_negative_sample[i]) /
+                                       o->epochs_per_negative_sample[i]);   // :91-92
+    lf++;
+    ln += n_neg;
+    for (uint64_t p = 0; p < n_neg; ++p) {                              // :94-119
+      uint64_t kk = rng.below(nv);
+      if (j == kk) continue;
+      float* ob = tailp + kk * dim;
+      float dn = euclidean_distance(cur, ob, dim, grad.data());
+      float wn = dn > 0.0f ? 1.0f / (1.0f + a * powf(dn, 2.0f * b)) : 1.0f;
+      float gc = (((gamma * 2.0f) * b) * wn) / (dn + 1e-6f);            // :113
+      for (uint64_t d = 0; d < dim; ++d) cur[d] += rust_clamp(gc * grad[d], -4.0f, 4.0f) * alpha;
+    }
+    o->epoch_of_next_negative_sample[i] += (double)n_neg * o->epochs_per_negative_sample[i];  // :121
+  }
+  *fired = lf;
+  *negs = ln;
 }
 
 // optimizer.rs:297-366 + layout/optimize_layout_euclidean.rs:236-347 (parallel=true,
@@ -715,6 +775,13 @@ int orc_optimizer_step_epochs(OrcOptimizer* o, uint64_t n_ep, uint64_t* fires, u
   for (uint64_t epoch = start; epoch < end; ++epoch) {
     const float alpha = o->initial_alpha * (1.0f - ((float)epoch / (float)o->total_epochs));  // :317
     const double nd = (double)epoch;
+    if (o->metric_type == 1) {                                          // optimizer.rs:340-358
+      uint64_t F = 0, N = 0;
+      generic_epoch(o, headp, tailp, epoch, alpha, &F, &N);
+      if (fires) fires[epoch - start] = F;
+      if (negs) negs[epoch - start] = N;
+      continue;
+    }
     std::vector<uint64_t> tf(nt + 1, 0), tn(nt + 1, 0);
     parallel_for(E, [&](uint64_t bgn, uint64_t e, int tid) {
       Xoshiro256ss rng(o->seed ^ (0x9E3779B97F4A7C15ull * (epoch + 1)) ^ (bgn * 0xD1B54A32D192ED03ull));

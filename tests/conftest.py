@@ -62,6 +62,23 @@ def ring_fixture(seed=0, n=50, k=10, dim=2):
     return idx, dist, init
 
 
+def pairs_fixture(n_pairs=300, dim=2, seed=0):
+    """Disjoint pairs (2m, 2m+1): each row's kNN is [self (0), partner (d > 0)], so after
+    the prune every vertex has one edge of weight 1 (epochs_per_sample 1) to its partner.
+    With negative_sample_rate = 0 an epoch's result does not depend on the order of the
+    edge updates (each snapshot row is read and moved by one edge only), so every
+    implementation of the SGD rule must agree up to rounding."""
+    g = np.random.Generator(np.random.PCG64(seed))
+    n = 2 * n_pairs
+    idx = np.empty((n, 2), np.uint32)
+    idx[:, 0] = np.arange(n)
+    idx[:, 1] = np.arange(n) ^ 1
+    dist = np.zeros((n, 2), np.float32)
+    dist[:, 1] = (g.random(n, dtype=np.float32) + 0.5).astype(np.float32)
+    init = (g.random((n, dim), dtype=np.float32) * 10.0).astype(np.float32)
+    return idx, dist, init
+
+
 @pytest.fixture(scope="session")
 def ring():
     return ring_fixture()

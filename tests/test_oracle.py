@@ -227,3 +227,82 @@ def test_schedule_closed_form_matches_state_arrays(oracle):
     gF, gN = fixed_point_schedule(eps, total, 5)
     assert np.abs(gF - F.astype(np.int64)).sum() <= 1e-5 * F.sum() + 1
     assert np.abs(gN - N.astype(np.int64)).sum() <= 1e-5 * N.sum() + 5
+
+
+# ---------------------------------------------------------------- SGD update rules, known answers
+def np_pairs_epochs(x0, a, b, gamma, lr, total, n_ep, generic):
+    """One step_epochs(n_ep) call on the pairs graph (conftest.pairs_fixture) with
+    negative_sample_rate = 0, in numpy float32: live buffer `x`, snapshot `c` cloned once
+    (optimizer.rs:314), every edge (j -> j^1) fires at every epoch >= 1.  Euclidean rule:
+    optimize_layout_euclidean.rs:284-306; generic rule with EuclideanMetric:
+    optimize_layout_generic.rs:62-86 + distances.rs:208-223."""
+    f = np.float32
+    x = x0.astype(np.float32).copy()
+    c = x.copy()
+    n, dim = x.shape
+    part = np.arange(n) ^ 1
+    a, b = f(a), f(b)
+    for e in range(n_ep):
+        alpha = f(f(lr) * f(f(1) - f(f(e) / f(total))))
+        if e == 0:
+            continue                      # epoch_of_next_sample starts at 1
+        y = c[part]
+        diff = x - y
+        ds = np.zeros(n, np.float32)
+        for d in range(dim):
+            ds = (ds + diff[:, d] * diff[:, d]).astype(np.float32)
+        if generic:
+            dist = np.sqrt(ds)
+            den = (dist + f(1e-6)).astype(np.float32)
+            grad = (diff / den[:, None]).astype(np.float32)
+            rev = ((y - x) / den[:, None]).astype(np.float32)
+            with np.errstate(divide="ignore"):
+                pw = np.power(dist, f(f(2) * b)).astype(np.float32)
+            w = np.where(dist > 0, f(1) / (f(1) + a * pw), f(1)).astype(np.float32)
+            gc = ((f(2) * b) * (w - f(1)) / den).astype(np.float32)
+            x = (x + np.clip(gc[:, None] * grad, -4, 4) * alpha).astype(np.float32)
+            c[part] = (y + np.clip(gc[:, None] * rev, -4, 4) * alpha).astype(np.float32)
+        else:
+            with np.errstate(divide="ignore", invalid="ignore"):
+                pb = np.power(ds, b).astype(np.float32)
+                gc = ((((f(-2) * a) * b) * pb) / ds).astype(np.float32)
+                gc = (gc / ((a * pb) * ds + f(1))).astype(np.float32)
+            gc = np.where(ds > 0, gc, f(0)).astype(np.float32)
+            g = np.clip(gc[:, None] * diff, -4, 4).astype(np.float32)
+            x = (x + g * alpha).astype(np.float32)
+            c[part] = (y - g * alpha).astype(np.float32)
+    return x
+
+
+@pytest.mark.parametrize("generic", [False, True])
+@pytest.mark.parametrize("dim", [1, 2, 3, 5])
+def test_update_rules_known_answer(oracle, generic, dim):
+    """Both SGD rules of the oracle against a numpy restatement on an order-independent case."""
+    from conftest import pairs_fixture
+    idx, dist, init = pairs_fixture(200, dim, seed=dim)
+    cfg = oracle.OracleConfig(n_neighbors=2, negative_sample_rate=0, n_epochs=12)
+    m = oracle.learn_manifold(idx, dist, cfg)
+    ip, ix, dt = m.graph()
+    assert np.array_equal(np.diff(ip), np.ones(len(idx), np.int64)) and (dt == 1).all()
+    opt = oracle.Optimizer(m, init, 12, cfg, seed=3, metric_type=int(generic))
+    x0 = opt.embedding()
+    opt.step_epochs(12)
+    a, b = m.info()["a"], m.info()["b"]
+    expect = np_pairs_epochs(x0, a, b, cfg.repulsion_strength, cfg.learning_rate, 12, 12, generic)
+    got = opt.embedding()
+    assert np.array_equal(got, expect) or np.allclose(got, expect, rtol=2e-6, atol=2e-6)
+    assert not np.allclose(got, x0)
+
+
+def test_generic_rule_schedule_matches_euclidean(oracle):
+    """The generic rule changes the force law only: the same edges fire and draw the same
+    number of negatives (optimize_layout_generic.rs:57-121 vs optimize_layout_euclidean.rs)."""
+    idx, dist, init = small_gauss(600, 10, seed=5)
+    cfg = oracle.OracleConfig(n_neighbors=10)
+    m = oracle.learn_manifold(idx, dist, cfg)
+    F0, N0 = oracle.Optimizer(m, init, 40, cfg, seed=1).step_epochs(40, counts=True)
+    og = oracle.Optimizer(m, init, 40, cfg, seed=1, metric_type=1)
+    F1, N1 = og.step_epochs(40, counts=True)
+    assert np.array_equal(F0, F1) and np.array_equal(N0, N1)
+    e = og.embedding()
+    assert np.isfinite(e).all()

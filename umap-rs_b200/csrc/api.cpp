@@ -399,11 +399,8 @@ std::unique_ptr<umap_optimizer> optimizer_new_impl(std::unique_ptr<umap_manifold
                                                    bool init_on_host, uint64_t rows, uint64_t dims,
                                                    uint64_t total_epochs, const umap_config& c,
                                                    int metric_type) {
-  if (metric_type == UMAP_METRIC_GENERIC)
-    throw Error(UNSUPPORTED,
-                "MetricType::Generic output metrics are not implemented on the GPU path "
-                "(only the Euclidean specialisation, optimize_layout_euclidean.rs)");
-  if (metric_type != UMAP_METRIC_EUCLIDEAN) throw Error(INVALID_ARGUMENT, "unknown metric_type");
+  if (metric_type != UMAP_METRIC_EUCLIDEAN && metric_type != UMAP_METRIC_GENERIC)
+    throw Error(INVALID_ARGUMENT, "unknown metric_type");
   if (rows != man->n_vertices)
     throw Error(INVALID_ARGUMENT, "init has " + std::to_string(rows) + " samples but data has " +
                                       std::to_string(man->n_vertices) + " samples");
@@ -465,15 +462,22 @@ SgdParams sgd_params(const umap_optimizer& o) {
   p.seed = o.seed;
   p.row_seg = o.n_seg ? o.row_seg.p : nullptr;
   p.seg_off = o.n_seg ? o.seg_off.p : nullptr;
+  p.generic_metric = o.metric_type == UMAP_METRIC_GENERIC ? 1u : 0u;
+  p.two_b = 2.0f * p.b;                 // optimize_layout_generic.rs:72, :76
   return p;
 }
 
-// optimizer.rs:297-366.
-void step_epochs_impl(umap_optimizer& o, uint64_t n_ep) {
+// optimizer.rs:297-366.  `output_metric` is the device id of the metric the reference passes
+// to step_epochs; like the reference, the Euclidean specialisation ignores it, and the generic
+// path needs one with a device implementation.
+void step_epochs_impl(umap_optimizer& o, uint64_t n_ep, int output_metric = UMAP_OUTPUT_METRIC_EUCLIDEAN) {
   if (o.current_epoch + n_ep > o.total_epochs)
     throw Error(OVERSTEP, "Cannot step " + std::to_string(n_ep) + " epochs: would exceed total_epochs " +
                               std::to_string(o.total_epochs) + " (current: " +
                               std::to_string(o.current_epoch) + ")");
+  if (o.metric_type == UMAP_METRIC_GENERIC && output_metric != UMAP_OUTPUT_METRIC_EUCLIDEAN)
+    throw Error(UNSUPPORTED, "output metric " + std::to_string(output_metric) +
+                                 " has no device implementation (built in: 0 = Euclidean)");
   cudaStream_t s = o.s();
   const uint64_t nd = o.n * o.dim;
   float* live = o.emb2.p;
@@ -557,7 +561,9 @@ std::unique_ptr<umap_fitted> into_fitted_impl(std::unique_ptr<umap_optimizer> o,
 
 // embedding.rs:299-337: the rest of Umap::fit once the manifold is learned.
 std::unique_ptr<umap_fitted> fit_manifold_impl(const umap_config& c, std::unique_ptr<umap_manifold> m,
-                                               const float* init, uint64_t irows, uint64_t icols, bool host) {
+                                               const float* init, uint64_t irows, uint64_t icols, bool host,
+                                               int metric_type = UMAP_METRIC_EUCLIDEAN,
+                                               int output_metric = UMAP_OUTPUT_METRIC_EUCLIDEAN) {
   const uint64_t n_samples = m->n_vertices;
   if (icols != c.n_components)
     throw Error(INVALID_ARGUMENT, "init has " + std::to_string(icols) + " components but n_components is " +
@@ -566,8 +572,11 @@ std::unique_ptr<umap_fitted> fit_manifold_impl(const umap_config& c, std::unique
     throw Error(INVALID_ARGUMENT, "init has " + std::to_string(irows) + " samples but data has " +
                                       std::to_string(n_samples) + " samples");
   const uint64_t total = c.has_n_epochs ? c.n_epochs : (n_samples <= 10000 ? 500 : 200);  // :304-308
-  auto o = optimizer_new_impl(std::move(m), init, host, irows, icols, total, c, UMAP_METRIC_EUCLIDEAN);
-  step_epochs_impl(*o, total);  // :321
+  if (metric_type == UMAP_METRIC_GENERIC && output_metric != UMAP_OUTPUT_METRIC_EUCLIDEAN)
+    throw Error(UNSUPPORTED, "output metric " + std::to_string(output_metric) +
+                                 " has no device implementation (built in: 0 = Euclidean)");
+  auto o = optimizer_new_impl(std::move(m), init, host, irows, icols, total, c, metric_type);  // :311-319
+  step_epochs_impl(*o, total, output_metric);  // :321
   auto f = into_fitted_impl(std::move(o), c);
   nan_empty_rows(f->manifold->indptr.p, f->n, (uint32_t)f->dim, f->embedding.p, f->s());  // :327-334
   UB_CUDA(cudaStreamSynchronize(f->s()));
@@ -954,7 +963,8 @@ void finish_loaded_optimizer(umap_optimizer& o, const DevBuf<uint32_t>& head, co
   cudaStream_t s = o.s();
   const uint64_t n = o.manifold->n_vertices, E = head.n;
   if (o.current_epoch > o.total_epochs) throw Error(FORMAT, "current_epoch exceeds total_epochs");
-  if (o.metric_type != UMAP_METRIC_EUCLIDEAN) throw Error(UNSUPPORTED, "only Euclidean optimizers are supported");
+  if (o.metric_type != UMAP_METRIC_EUCLIDEAN && o.metric_type != UMAP_METRIC_GENERIC)
+    throw Error(FORMAT, "invalid MetricType");
   std::vector<uint32_t> hh(E), tt(E);
   d2h(hh.data(), head.p, E, s);
   d2h(tt.data(), tail.p, E, s);
@@ -1292,6 +1302,14 @@ int umap_optimizer_step_epochs(umap_optimizer* opt, uint64_t n) {
   API_END
 }
 
+int umap_optimizer_step_epochs_metric(umap_optimizer* opt, uint64_t n, int output_metric) {
+  API_BEGIN
+  need(opt, "optimizer");
+  opt->manifold->stream->activate();
+  step_epochs_impl(*opt, n, output_metric);
+  API_END
+}
+
 int umap_optimizer_current_epoch(const umap_optimizer* opt, uint64_t* out) {
   API_BEGIN
   need(opt, "optimizer"); need(out, "out");
@@ -1524,6 +1542,34 @@ int umap_fit_manifold_device(umap_manifold* manifold, const umap_config* cfg, co
   owned->stream->activate();
   wait_for_inputs();
   *out = fit_manifold_impl(*cfg, std::move(owned), init, irows, icols, false).release();
+  API_END
+}
+
+int umap_fit_manifold_metric(umap_manifold* manifold, const umap_config* cfg, const float* init, uint64_t irows,
+                             uint64_t icols, int metric_type, int output_metric, umap_fitted** out) {
+  std::unique_ptr<umap_manifold> owned(manifold);
+  API_BEGIN
+  need(manifold, "manifold"); need(cfg, "cfg"); need(init, "init"); need(out, "out");
+  *out = nullptr;
+  if (metric_type != UMAP_METRIC_EUCLIDEAN && metric_type != UMAP_METRIC_GENERIC)
+    throw Error(INVALID_ARGUMENT, "unknown metric_type");
+  owned->stream->activate();
+  *out = fit_manifold_impl(*cfg, std::move(owned), init, irows, icols, true, metric_type, output_metric).release();
+  API_END
+}
+
+int umap_fit_manifold_metric_device(umap_manifold* manifold, const umap_config* cfg, const float* init,
+                                    uint64_t irows, uint64_t icols, int metric_type, int output_metric,
+                                    umap_fitted** out) {
+  std::unique_ptr<umap_manifold> owned(manifold);
+  API_BEGIN
+  need(manifold, "manifold"); need(cfg, "cfg"); need(init, "init"); need(out, "out");
+  *out = nullptr;
+  if (metric_type != UMAP_METRIC_EUCLIDEAN && metric_type != UMAP_METRIC_GENERIC)
+    throw Error(INVALID_ARGUMENT, "unknown metric_type");
+  owned->stream->activate();
+  wait_for_inputs();
+  *out = fit_manifold_impl(*cfg, std::move(owned), init, irows, icols, false, metric_type, output_metric).release();
   API_END
 }
 

@@ -22,7 +22,6 @@
 // backward (CUDA cores) -> { dH1 GEMM (GELU derivative, db1) -> dW1 GEMM } || dW2 GEMM on a
 // second stream -> Adam.  The dW GEMMs contract over the batch in K splits whose partial sums
 // are stored to separate slices and summed by the Adam kernel.
-#include <cuda.h>  // CUtensorMap and its enums; the encoder is fetched from the runtime
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -33,9 +32,31 @@
 #include <vector>
 
 #include "ub_internal.hpp"
+#include "umma.cuh"
 
 namespace ub {
 namespace {
+
+using namespace umma;
+
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_tiled() {
+  static std::mutex mu;
+  static EncodeTiledFn fn = nullptr;
+  std::lock_guard<std::mutex> lock(mu);
+  if (!fn) {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    UB_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q));
+    if (q != cudaDriverEntryPointSuccess || !f) throw Error(CUDA, "cuTensorMapEncodeTiled is not available");
+    fn = reinterpret_cast<EncodeTiledFn>(f);
+  }
+  return fn;
+}
+
 
 using bf16 = __nv_bfloat16;
 
@@ -76,25 +97,6 @@ struct GatherA {
   int64_t ldt;
 };
 
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-// Shared-memory matrix descriptor: K-major, no swizzle (layout type 0), descriptor version 1.
-__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
-  uint64_t d = 0;
-  d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
-  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
-  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
-  d |= (uint64_t)1u << 46;
-  return d;
-}
-
-// Instruction descriptor, kind::f16: D F32 (bits 4-5 = 1), A and B BF16 (bits 7-9 and 10-12
-// = 1), both K-major (bits 15, 16 = 0), N >> 3 at bit 17, M >> 4 at bit 24.
-__host__ __device__ constexpr uint32_t instr_desc(int M, int N) {
-  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
-}
 
 __device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
 __device__ __forceinline__ float gelu_grad(float x) {
@@ -103,29 +105,6 @@ __device__ __forceinline__ float gelu_grad(float x) {
   return cdf + x * pdf;
 }
 
-__device__ __forceinline__ uint64_t global_ns() {
-  uint64_t t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-
-// Waits for an mbarrier phase; gives up after about two seconds.
-__device__ __forceinline__ bool mbar_wait(uint32_t addr, uint32_t phase) {
-  const uint64_t t0 = global_ns();
-  for (uint32_t it = 0; it < (1u << 30); ++it) {
-    uint32_t done;
-    asm volatile(
-        "{\n\t.reg .pred P;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2;\n\t"
-        "selp.b32 %0, 1, 0, P;\n\t}"
-        : "=r"(done)
-        : "r"(addr), "r"(phase)
-        : "memory");
-    if (done) return true;
-    if ((it & 255u) == 255u && global_ns() - t0 > 2000000000ull) return false;
-  }
-  return false;
-}
 
 __device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
   const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
@@ -366,19 +345,6 @@ __global__ void __launch_bounds__(GT) umma_gemm_kernel(const bf16* __restrict__ 
 }
 
 
-// K-major, 128-byte-swizzled shared-memory matrix descriptor (layout type 2): rows of 128 B
-// (64 bf16) with 16-byte chunks XOR-swizzled by row % 8, 8-row atoms 1024 B apart (stride
-// byte offset), leading byte offset unused (16 B); the tile starts 1024-byte aligned and
-// K step s (16 bf16 = 32 B) is addressed by advancing the start address 32 B.
-__device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t saddr) {
-  uint64_t d = 0;
-  d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
-  d |= (uint64_t)1u << 16;
-  d |= (uint64_t)(1024u >> 4) << 32;
-  d |= (uint64_t)1u << 46;
-  d |= (uint64_t)2u << 61;
-  return d;
-}
 
 constexpr int TS = 4;  // TMA pipeline stages
 
@@ -530,42 +496,6 @@ void launch_gemm(const bf16* A, int64_t lda, const bf16* B, int64_t ldb, int64_t
   UB_LAUNCH_CHECK();
 }
 
-
-// ------------------------------------------------------------------------------ TMA tensor maps
-using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
-                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
-                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-EncodeTiledFn encode_tiled() {
-  static std::mutex mu;
-  static EncodeTiledFn fn = nullptr;
-  std::lock_guard<std::mutex> lock(mu);
-  if (!fn) {
-    void* f = nullptr;
-    cudaDriverEntryPointQueryResult q{};
-    UB_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q));
-    if (q != cudaDriverEntryPointSuccess || !f) throw Error(CUDA, "cuTensorMapEncodeTiled is not available");
-    fn = reinterpret_cast<EncodeTiledFn>(f);
-  }
-  return fn;
-}
-
-// Tensor map of a row-major bf16 matrix [rows, cols] (row stride ld elements) read in boxes of
-// box_rows x 64 with 128-byte swizzle.
-CUtensorMap bf16_tile_map(const void* base, int64_t rows, int64_t cols, int64_t ld, int box_rows) {
-  if (reinterpret_cast<uintptr_t>(base) % 16 || (ld * 2) % 16 || cols < KC || rows < box_rows)
-    throw Error(INVALID_ARGUMENT, "TMA operand must be 16-byte aligned with 16-byte rows");
-  CUtensorMap m;
-  const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
-  const cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
-  const cuuint32_t box[2] = {(cuuint32_t)KC, (cuuint32_t)box_rows};
-  const cuuint32_t estr[2] = {1, 1};
-  const CUresult r = encode_tiled()(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides,
-                                    box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
-                                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (r != CUDA_SUCCESS) throw Error(CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
-  return m;
-}
 
 template <int BN, int EPI>
 void prepare_tma_gemm() {
@@ -891,6 +821,25 @@ void prepare_all_gemms() {
 }  // namespace
 
 // ------------------------------------------------------------------------------ model
+// ------------------------------------------------------------------------------ TMA tensor maps
+// Tensor map of a row-major bf16 matrix [rows, cols] (row stride ld elements) read in boxes of
+// box_rows x 64 with 128-byte swizzle.
+CUtensorMap bf16_tile_map(const void* base, int64_t rows, int64_t cols, int64_t ld, int box_rows) {
+  if (reinterpret_cast<uintptr_t>(base) % 16 || (ld * 2) % 16 || cols < 64 || rows < box_rows)
+    throw Error(INVALID_ARGUMENT, "TMA operand must be 16-byte aligned with 16-byte rows");
+  CUtensorMap m;
+  const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
+  const cuuint32_t box[2] = {64u, (cuuint32_t)box_rows};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r = encode_tiled()(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides,
+                                    box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) throw Error(CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+  return m;
+}
+
+
 struct Mlp::Impl {
   int in_dim = 0, out_dim = 0;
   cudaStream_t s = nullptr;   // owner's stream

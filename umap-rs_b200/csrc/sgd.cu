@@ -32,17 +32,11 @@ namespace {
 constexpr uint32_t PAD_ROW = 0xFFFFFFFFu;
 
 // Tuning knobs (compile-time).
-#ifndef UB_SGD_PF
-#define UB_SGD_PF 8          // entries loaded per lane per batch
-#endif
 #ifndef UB_SGD_NEG_BATCH
 #define UB_SGD_NEG_BATCH 4   // negative-sample rows fetched together
 #endif
 #ifndef UB_SGD_MIN_BLOCKS
 #define UB_SGD_MIN_BLOCKS 5  // resident 256-thread blocks per SM the register budget targets
-#endif
-#ifndef UB_SGD_KERNEL
-#define UB_SGD_KERNEL 2      // 1: warp-batched entries, 2: independent lane progress
 #endif
 
 // ------------------------------------------------------------------------------ negatives' RNG
@@ -129,7 +123,6 @@ __device__ __forceinline__ float clip4(float v) {
 }
 
 // ------------------------------------------------------------------------------ K7
-constexpr int PF = UB_SGD_PF;               // entries per lane per batch (coalesced across the warp)
 constexpr int NEG_BATCH = UB_SGD_NEG_BATCH; // negative-sample rows fetched together
 static_assert(NEG_BATCH >= 1 && NEG_BATCH <= 16, "negative batch size");
 
@@ -176,10 +169,24 @@ __device__ __forceinline__ void sub_row(float* p, const float (&g)[DIM]) {
   }
 }
 
-// One fired edge (optimize_layout_euclidean.rs:278-343): attractive step on (head, tail),
-// then `nneg` negative samples, all reading the snapshot buffer.  The tail row and a batch
-// of negative rows are fetched together before the (sequential) updates of `cur`.
-template <int DIM>
+// Force law of the generic-metric path (layout/optimize_layout_generic.rs:65-119) with the
+// built-in output metric EuclideanMetric (distances.rs:208-223): distance d = sqrt(sum diff^2),
+// gradient diff / (d + 1e-6), w = 1 / (1 + a d^(2b)).  Returns the coefficient c that
+// multiplies the gradient: 2b (w - 1) / (d + 1e-6) for an attraction, 2 gamma b w / (d + 1e-6)
+// for a repulsion (`scale` = 2b or 2 gamma b, `bias` = -1 or 0); *den receives d + 1e-6.
+__device__ __forceinline__ float metric_coeff(float ds, float a, float two_b, float scale, float bias,
+                                              float* den) {
+  const float dist = sqrtf(ds);
+  *den = dist + 1e-6f;
+  const float w = dist > 0.0f ? 1.0f / (1.0f + a * __powf(dist, two_b)) : 1.0f;
+  return __fdividef(scale * (w + bias), *den);
+}
+
+// One fired edge (optimize_layout_euclidean.rs:278-343, or with GEN the generic-metric rule
+// of optimize_layout_generic.rs:57-121): attractive step on (head, tail), then `nneg`
+// negative samples, all reading the snapshot buffer.  The tail row and a batch of negative
+// rows are fetched together before the (sequential) updates of `cur`.
+template <int DIM, bool GEN>
 __device__ __forceinline__ void fired_edge(float (&cur)[DIM], uint32_t r, uint32_t k, uint32_t nneg,
                                            float* snap, const SgdParams& p, float alpha, uint64_t idx,
                                            uint32_t epoch, uint64_t seed, uint32_t seg_lo, uint32_t seg_n) {
@@ -213,16 +220,27 @@ __device__ __forceinline__ void fired_edge(float (&cur)[DIM], uint32_t r, uint32
   float ds = 0.0f;
 #pragma unroll
   for (int d = 0; d < DIM; ++d) { const float df = cur[d] - o[d]; ds += df * df; }
-  float gc = 0.0f;
-  if (ds > 0.0f) {
-    const float pb = __powf(ds, b);
-    gc = __fdividef(p.neg_attr * pb, ds * (a * pb * ds + 1.0f));
-  }
   float g[DIM];
+  if constexpr (GEN) {
+    // head += clip(c * grad) alpha; tail += clip(c * rev_grad) alpha with rev_grad = -grad
+    float den;
+    const float gc = metric_coeff(ds, a, p.two_b, p.two_b, -1.0f, &den);
 #pragma unroll
-  for (int d = 0; d < DIM; ++d) {
-    g[d] = clip4(gc * (cur[d] - o[d])) * alpha;
-    cur[d] += g[d];
+    for (int d = 0; d < DIM; ++d) {
+      g[d] = clip4(gc * __fdividef(cur[d] - o[d], den)) * alpha;
+      cur[d] += g[d];
+    }
+  } else {
+    float gc = 0.0f;
+    if (ds > 0.0f) {
+      const float pb = __powf(ds, b);
+      gc = __fdividef(p.neg_attr * pb, ds * (a * pb * ds + 1.0f));
+    }
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      g[d] = clip4(gc * (cur[d] - o[d])) * alpha;
+      cur[d] += g[d];
+    }
   }
   sub_row<DIM>(oth, g);
   // negative samples (:313-341)
@@ -235,77 +253,22 @@ __device__ __forceinline__ void fired_edge(float (&cur)[DIM], uint32_t r, uint32
       float dsn = 0.0f;
 #pragma unroll
       for (int d = 0; d < DIM; ++d) { const float df = cur[d] - ob[q][d]; dsn += df * df; }
-      float gr = 0.0f;
-      if (dsn > 0.0f) {
-        const float pb = __powf(dsn, b);
-        gr = __fdividef(p.pos_rep, (0.001f + dsn) * (a * pb * dsn + 1.0f));
+      if constexpr (GEN) {
+        float den;
+        const float gr = metric_coeff(dsn, a, p.two_b, p.pos_rep, 0.0f, &den);
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) cur[d] += clip4(gr * __fdividef(cur[d] - ob[q][d], den)) * alpha;
+      } else {
+        float gr = 0.0f;
+        if (dsn > 0.0f) {
+          const float pb = __powf(dsn, b);
+          gr = __fdividef(p.pos_rep, (0.001f + dsn) * (a * pb * dsn + 1.0f));
+        }
+        if (gr > 0.0f) {
+#pragma unroll
+          for (int d = 0; d < DIM; ++d) cur[d] += clip4(gr * (cur[d] - ob[q][d])) * alpha;
+        }
       }
-      if (gr > 0.0f) {
-#pragma unroll
-        for (int d = 0; d < DIM; ++d) cur[d] += clip4(gr * (cur[d] - ob[q][d])) * alpha;
-      }
-    }
-  }
-}
-
-template <int DIM>
-__global__ void __launch_bounds__(256, UB_SGD_MIN_BLOCKS) sgd_epoch_kernel(
-    const uint64_t* __restrict__ slice_base, const uint32_t* __restrict__ slice_width,
-    const uint32_t* __restrict__ split_mask, const uint32_t* __restrict__ rowid,
-    const uint2* __restrict__ entry, uint64_t n_slices, float* __restrict__ live, float* snap,
-    SgdParams p, uint32_t epoch, float alpha) {
-  const uint64_t slice = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const uint32_t lane = threadIdx.x & 31;
-  if (slice >= n_slices) return;
-  const uint32_t r = rowid[slice * 32 + lane];
-  const uint32_t width = slice_width[slice];
-  const uint64_t base = slice_base[slice];
-  const bool split = (split_mask[slice] >> lane) & 1u;
-  const bool active = r != PAD_ROW;
-  uint32_t seg_lo = 0, seg_n = p.n_vertices;
-  if (p.row_seg && active) {
-    const uint32_t sg = p.row_seg[r];
-    seg_lo = (uint32_t)p.seg_off[sg];
-    seg_n = (uint32_t)(p.seg_off[sg + 1] - p.seg_off[sg]);
-  }
-  float cur[DIM], start[DIM];
-  float* hrow = live + (uint64_t)(active ? r : 0) * DIM;
-  if (active) load_row<DIM>(cur, hrow);
-  else
-#pragma unroll
-    for (int d = 0; d < DIM; ++d) cur[d] = 0.0f;
-#pragma unroll
-  for (int d = 0; d < DIM; ++d) start[d] = cur[d];
-  const uint32_t n = epoch;
-  const uint64_t seed = p.seed;
-
-  for (uint32_t e0 = 0; e0 < width; e0 += PF) {
-    uint2 ent[PF];
-    uint32_t mask = 0;
-#pragma unroll
-    for (int j = 0; j < PF; ++j) {
-      const uint32_t e = e0 + j;
-      ent[j] = e < width ? __ldcs(entry + base + (uint64_t)e * 32 + lane) : make_uint2(0u, 0u);
-      if (fires_at(n, ent[j].y)) mask |= 1u << j;
-    }
-    while (mask) {
-      const int j = __ffs(mask) - 1;
-      mask &= mask - 1;
-      uint2 en = ent[0];
-#pragma unroll
-      for (int t = 1; t < PF; ++t)
-        if (t == j) en = ent[t];
-      const uint32_t nneg = negatives_at(n, en.y, p.neg_rate);
-      const uint64_t idx = base + (uint64_t)(e0 + j) * 32 + lane;
-      fired_edge<DIM>(cur, r, en.x, nneg, snap, p, alpha, idx, epoch, seed, seg_lo, seg_n);
-    }
-  }
-  if (active) {
-    if (split) {
-#pragma unroll
-      for (int d = 0; d < DIM; ++d) atomicAdd(hrow + d, cur[d] - start[d]);
-    } else {
-      store_row<DIM>(hrow, cur);
     }
   }
 }
@@ -316,7 +279,7 @@ __global__ void __launch_bounds__(256, UB_SGD_MIN_BLOCKS) sgd_epoch_kernel(
 #ifndef UB_SGD2_W
 #define UB_SGD2_W 4
 #endif
-template <int DIM>
+template <int DIM, bool GEN>
 __global__ void __launch_bounds__(256, UB_SGD_MIN_BLOCKS) sgd_epoch_kernel2(
     const uint64_t* __restrict__ slice_base, const uint32_t* __restrict__ slice_width,
     const uint32_t* __restrict__ split_mask, const uint32_t* __restrict__ rowid,
@@ -372,7 +335,7 @@ __global__ void __launch_bounds__(256, UB_SGD_MIN_BLOCKS) sgd_epoch_kernel2(
         if (t == j) en = win[t];
       const uint32_t nneg = negatives_at(n, en.y, p.neg_rate);
       const uint64_t idx = base + (uint64_t)(ebase + j) * 32 + lane;
-      fired_edge<DIM>(cur, r, en.x, nneg, snap, p, alpha, idx, epoch, seed, seg_lo, seg_n);
+      fired_edge<DIM, GEN>(cur, r, en.x, nneg, snap, p, alpha, idx, epoch, seed, seg_lo, seg_n);
     }
   }
   if (active) {
@@ -385,10 +348,11 @@ __global__ void __launch_bounds__(256, UB_SGD_MIN_BLOCKS) sgd_epoch_kernel2(
   }
 }
 
-// Generic dimension (any n_components): same algorithm, head row in global memory (owned
-// by this lane for whole-row tasks; split tasks accumulate their delta in place with
-// atomics).
-__global__ void __launch_bounds__(256) sgd_epoch_generic(
+// Any dimension (n_components > 4): same algorithm, head row in global memory (owned by this
+// lane for whole-row tasks; split tasks accumulate their delta in place with atomics).  GEN
+// selects the generic-metric rule as in fired_edge.
+template <bool GEN>
+__global__ void __launch_bounds__(256) sgd_epoch_anydim(
     const uint64_t* __restrict__ slice_base, const uint32_t* __restrict__ slice_width,
     const uint32_t* __restrict__ split_mask, const uint32_t* __restrict__ rowid,
     const uint2* __restrict__ entry, uint64_t n_slices, float* __restrict__ live, float* snap,
@@ -423,14 +387,16 @@ __global__ void __launch_bounds__(256) sgd_epoch_generic(
     float* oth = snap + (uint64_t)en.x * dim;
     float ds = 0.0f;
     for (uint32_t d = 0; d < dim; ++d) { const float df = cur[d] - oth[d]; ds += df * df; }
-    float gc = 0.0f;
-    if (ds > 0.0f) {
+    float gc = 0.0f, den = 1.0f;
+    if constexpr (GEN) {
+      gc = metric_coeff(ds, a, p.two_b, p.two_b, -1.0f, &den);
+    } else if (ds > 0.0f) {
       const float pb = __powf(ds, b);
       gc = __fdividef(p.neg_attr * pb, ds * (a * pb * ds + 1.0f));
     }
     for (uint32_t d = 0; d < dim; ++d) {
       const float cd = cur[d], od = oth[d];
-      const float g = clip4(gc * (cd - od)) * alpha;
+      const float g = clip4(gc * (GEN ? __fdividef(cd - od, den) : cd - od)) * alpha;
       add(d, g);
       atomicAdd(oth + d, -g);
     }
@@ -445,13 +411,19 @@ __global__ void __launch_bounds__(256) sgd_epoch_generic(
       const float* ob = snap + (uint64_t)kk * dim;
       float dsn = 0.0f;
       for (uint32_t d = 0; d < dim; ++d) { const float df = cur[d] - ob[d]; dsn += df * df; }
-      float gr = 0.0f;
-      if (dsn > 0.0f) {
-        const float pb = __powf(dsn, b);
-        gr = __fdividef(p.pos_rep, (0.001f + dsn) * (a * pb * dsn + 1.0f));
+      if constexpr (GEN) {
+        float dn;
+        const float gr = metric_coeff(dsn, a, p.two_b, p.pos_rep, 0.0f, &dn);
+        for (uint32_t d = 0; d < dim; ++d) add(d, clip4(gr * __fdividef(cur[d] - ob[d], dn)) * alpha);
+      } else {
+        float gr = 0.0f;
+        if (dsn > 0.0f) {
+          const float pb = __powf(dsn, b);
+          gr = __fdividef(p.pos_rep, (0.001f + dsn) * (a * pb * dsn + 1.0f));
+        }
+        if (gr > 0.0f)
+          for (uint32_t d = 0; d < dim; ++d) add(d, clip4(gr * (cur[d] - ob[d])) * alpha);
       }
-      if (gr > 0.0f)
-        for (uint32_t d = 0; d < dim; ++d) add(d, clip4(gr * (cur[d] - ob[d])) * alpha);
     }
   }
 }
@@ -840,20 +812,21 @@ void sgd_epoch(const SgdLayout& L, float* live, float* snap, const SgdParams& p,
   const unsigned grid = grid_for(L.n_slices * 32, bt);
 #define UB_SGD_ARGS L.slice_base.p, L.slice_width.p, L.split_mask.p, L.rowid.p, L.entry.p, L.n_slices, live, snap, \
                     p, epoch, alpha
-#if UB_SGD_KERNEL == 2
-#define UB_SGD_K sgd_epoch_kernel2
-#else
-#define UB_SGD_K sgd_epoch_kernel
-#endif
-  switch (p.dim) {
-    case 1: UB_SGD_K<1><<<grid, bt, 0, s>>>(UB_SGD_ARGS); break;
-    case 2: UB_SGD_K<2><<<grid, bt, 0, s>>>(UB_SGD_ARGS); break;
-    case 3: UB_SGD_K<3><<<grid, bt, 0, s>>>(UB_SGD_ARGS); break;
-    case 4: UB_SGD_K<4><<<grid, bt, 0, s>>>(UB_SGD_ARGS); break;
-    default: sgd_epoch_generic<<<grid, bt, 0, s>>>(UB_SGD_ARGS); break;
+#define UB_SGD_DISPATCH(GEN)                                                          \
+  switch (p.dim) {                                                                    \
+    case 1: sgd_epoch_kernel2<1, GEN><<<grid, bt, 0, s>>>(UB_SGD_ARGS); break;        \
+    case 2: sgd_epoch_kernel2<2, GEN><<<grid, bt, 0, s>>>(UB_SGD_ARGS); break;        \
+    case 3: sgd_epoch_kernel2<3, GEN><<<grid, bt, 0, s>>>(UB_SGD_ARGS); break;        \
+    case 4: sgd_epoch_kernel2<4, GEN><<<grid, bt, 0, s>>>(UB_SGD_ARGS); break;        \
+    default: sgd_epoch_anydim<GEN><<<grid, bt, 0, s>>>(UB_SGD_ARGS); break;           \
   }
+  if (p.generic_metric) {
+    UB_SGD_DISPATCH(true)
+  } else {
+    UB_SGD_DISPATCH(false)
+  }
+#undef UB_SGD_DISPATCH
 #undef UB_SGD_ARGS
-#undef UB_SGD_K
   UB_LAUNCH_CHECK();
 }
 

@@ -196,6 +196,10 @@ struct SgdParams {
   const uint64_t* seg_off;
   uint32_t dim;
   uint64_t seed;
+  // MetricType::Generic (optimizer.rs:340-358): the generic-metric update rule with the
+  // built-in Euclidean output metric instead of the Euclidean specialisation.
+  uint32_t generic_metric;
+  float two_b;      // 2 b
 };
 
 // Batched instances: per-instance prune threshold and max kept weight (device arrays).

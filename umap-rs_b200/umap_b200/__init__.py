@@ -29,7 +29,7 @@ from . import _lib
 
 __all__ = [
     "ManifoldParams", "GraphParams", "OptimizationParams", "UmapConfig", "MetricType",
-    "EuclideanMetric", "Metric", "Umap", "LearnedManifold", "Optimizer", "FittedUmap",
+    "EuclideanMetric", "GenericEuclideanMetric", "Metric", "OUTPUT_METRIC_EUCLIDEAN", "Umap", "LearnedManifold", "Optimizer", "FittedUmap",
     "SparseMat", "UmapError", "find_ab_params", "lib",
 ]
 
@@ -135,9 +135,15 @@ class MetricType(enum.IntEnum):
     Generic = 1
 
 
+OUTPUT_METRIC_EUCLIDEAN = 0   # umap_output_metric (include/umap_b200.h)
+
+
 class Metric:
-    """Output-space metric (metric.rs:19-62).  Only the Euclidean specialisation runs on
-    the GPU; a Generic metric is rejected by Optimizer (UMAP_ERR_UNSUPPORTED)."""
+    """Output-space metric (metric.rs:19-62).  `metric_type()` picks the SGD rule: the
+    Euclidean specialisation or the generic rule (layout/optimize_layout_generic.rs), which
+    needs the metric's distance and gradient on the device.  `device_metric()` names that
+    device implementation (an umap_output_metric id), or None for a metric that has none:
+    a Generic optimizer stepped with such a metric raises UMAP_ERR_UNSUPPORTED."""
 
     def metric_type(self) -> MetricType:
         return MetricType.Generic
@@ -145,10 +151,37 @@ class Metric:
     def disconnection_threshold(self) -> float:
         return float("inf")
 
+    def device_metric(self) -> int | None:
+        return None
+
 
 class EuclideanMetric(Metric):
+    """distances.rs:197-236."""
+
     def metric_type(self) -> MetricType:
         return MetricType.Euclidean
+
+    def device_metric(self) -> int | None:
+        return OUTPUT_METRIC_EUCLIDEAN
+
+    def distance(self, x, y):
+        """(sqrt(sum (x - y)^2), (x - y) / (distance + 1e-6)) in f32 (distances.rs:208-223)."""
+        x = np.asarray(x, np.float32)
+        y = np.asarray(y, np.float32)
+        s = np.float32(0)
+        for v in x - y:
+            s = np.float32(s + v * v)
+        d = np.sqrt(s)
+        return d, (x - y) / np.float32(d + np.float32(1e-6))
+
+
+class GenericEuclideanMetric(EuclideanMetric):
+    """EuclideanMetric's distance and gradient through the generic rule: what a Rust caller
+    gets from a Metric impl that computes the Euclidean distance but keeps the trait's default
+    `metric_type()` (Generic), so Optimizer::step_epochs takes optimize_layout_generic.rs."""
+
+    def metric_type(self) -> MetricType:
+        return MetricType.Generic
 
 
 def kernel_launches() -> int:
@@ -393,12 +426,27 @@ class Umap:
             _check(L.umap_learn_manifold(C.byref(cfg), n, pi, pd, rows, cols, C.byref(out)))
         return LearnedManifold(out.value)
 
+    def _output_metric_ids(self):
+        mt = self.output_metric.metric_type()
+        dm = self.output_metric.device_metric()
+        if mt == MetricType.Generic and dm is None:
+            raise UmapError(ERR_UNSUPPORTED, f"output metric {type(self.output_metric).__name__} has no "
+                                             "device implementation")
+        return int(mt), OUTPUT_METRIC_EUCLIDEAN if dm is None else int(dm)
+
     def fit(self, data, knn_indices, knn_dists, init) -> "FittedUmap":
         """embedding.rs:274-337."""
         L = _lib.load()
-        if self.output_metric.metric_type() != MetricType.Euclidean:
-            raise UmapError(ERR_UNSUPPORTED, "MetricType::Generic output metrics are not implemented "
-                                             "on the GPU path")
+        if self._output_metric_ids()[0] != MetricType.Euclidean:
+            # generic rule: learn_manifold, then the rest of fit with the metric's device id
+            irows, icols = int(init.shape[0]), int(init.shape[1])
+            n = _n_samples(data)
+            if icols != self.config.n_components:
+                raise UmapError(ERR_INVALID_ARGUMENT, f"init has {icols} components but n_components is "
+                                                      f"{self.config.n_components}")
+            if irows != n:
+                raise UmapError(ERR_INVALID_ARGUMENT, f"init has {irows} samples but data has {n} samples")
+            return self.fit_manifold(self.learn_manifold(data, knn_indices, knn_dists), init)
         n = _n_samples(data)
         rows, cols = int(knn_dists.shape[0]), int(knn_dists.shape[1])
         if tuple(knn_indices.shape) != tuple(knn_dists.shape):
@@ -425,9 +473,7 @@ class Umap:
     def fit_manifold(self, manifold: "LearnedManifold", init) -> "FittedUmap":
         """embedding.rs:299-337: `fit` after its learn_manifold step.  Consumes `manifold`."""
         L = _lib.load()
-        if self.output_metric.metric_type() != MetricType.Euclidean:
-            raise UmapError(ERR_UNSUPPORTED, "MetricType::Generic output metrics are not implemented "
-                                             "on the GPU path")
+        mt, dm = self._output_metric_ids()
         cfg = self._cfg()
         irows, icols = int(init.shape[0]), int(init.shape[1])
         mh = manifold._take()
@@ -435,10 +481,10 @@ class Umap:
         if _is_cuda_tensor(init):
             import torch
             tn, pn = _device(init, torch.float32)
-            _check(L.umap_fit_manifold_device(mh, C.byref(cfg), pn, irows, icols, C.byref(out)))
+            _check(L.umap_fit_manifold_metric_device(mh, C.byref(cfg), pn, irows, icols, mt, dm, C.byref(out)))
         else:
             an, pn = _host(init, np.float32)
-            _check(L.umap_fit_manifold(mh, C.byref(cfg), pn, irows, icols, C.byref(out)))
+            _check(L.umap_fit_manifold_metric(mh, C.byref(cfg), pn, irows, icols, mt, dm, C.byref(out)))
         return FittedUmap(out.value)
 
 
@@ -472,8 +518,10 @@ class Optimizer(_Handle):
         _check(rc)
 
     def step_epochs(self, n: int, output_metric: Metric | None = None):
-        """optimizer.rs:297-366."""
-        _check(_lib.load().umap_optimizer_step_epochs(self._get(), n))
+        """optimizer.rs:297-366.  A Generic optimizer uses `output_metric` (Euclidean when
+        omitted); one without a device implementation raises UMAP_ERR_UNSUPPORTED."""
+        dm = OUTPUT_METRIC_EUCLIDEAN if output_metric is None else output_metric.device_metric()
+        _check(_lib.load().umap_optimizer_step_epochs_metric(self._get(), n, -1 if dm is None else int(dm)))
 
     def _u64(self, fn):
         v = C.c_uint64()

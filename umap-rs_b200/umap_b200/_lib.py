@@ -47,6 +47,7 @@ SIGNATURES = {
     "umap_optimizer_new": [P, P, u64, u64, u64, C.POINTER(UmapConfigC), i32, PP],
     "umap_optimizer_new_device": [P, P, u64, u64, u64, C.POINTER(UmapConfigC), i32, PP],
     "umap_optimizer_step_epochs": [P, u64],
+    "umap_optimizer_step_epochs_metric": [P, u64, i32],
     "umap_optimizer_current_epoch": [P, C.POINTER(u64)],
     "umap_optimizer_total_epochs": [P, C.POINTER(u64)],
     "umap_optimizer_remaining_epochs": [P, C.POINTER(u64)],
@@ -93,6 +94,8 @@ SIGNATURES = {
     "umap_radix_sort_noalloc_max_pairs": [C.POINTER(u64)],
     "umap_fit_manifold": [P, C.POINTER(UmapConfigC), P, u64, u64, PP],
     "umap_fit_manifold_device": [P, C.POINTER(UmapConfigC), P, u64, u64, PP],
+    "umap_fit_manifold_metric": [P, C.POINTER(UmapConfigC), P, u64, u64, i32, i32, PP],
+    "umap_fit_manifold_metric_device": [P, C.POINTER(UmapConfigC), P, u64, u64, i32, i32, PP],
     "umap_mlp_param_count": [u64, u64, C.POINTER(u64)],
     "umap_mlp_new": [u64, u64, P, PP],
     "umap_mlp_dims": [P, C.POINTER(u64), C.POINTER(u64)],

@@ -214,6 +214,21 @@ int umap_fit_manifold_metric_device(umap_manifold* manifold, const umap_config* 
                                     uint64_t init_rows, uint64_t init_cols, int metric_type,
                                     int output_metric, umap_fitted** out);
 
+/* ---- kNN producer (the step before the fit; the reference takes kNN as input) ---------
+ * Exact brute-force k nearest neighbours as the reference's example computes them
+ * (examples/src/bin/mnist_demo.rs:203-229): for each row of data [n, dim] (row-major f32) the
+ * k other rows with the smallest sqrt(sum_i (x_i - y_i)^2) (f32, summed in coordinate order),
+ * ordered by distance then index, the row itself excluded; with fewer than k other rows the
+ * remaining slots are 0 / 0.0.  Outputs [n, k] row-major.  1 <= k <= 32.  Candidates come
+ * from a BF16 tensor-core distance pass; every row is then either certified exact against an
+ * error bound or recomputed exactly, so the result equals the f32 brute force.
+ * `rows_recomputed` (nullable) receives the number of rows that needed the exact recompute.
+ * UMAP_ERR_INVALID_ARGUMENT for NaN or infinite inputs (the reference's sort panics). */
+int umap_knn_bruteforce(const float* host_data, uint64_t n, uint64_t dim, uint64_t k,
+                        uint32_t* host_knn_indices, float* host_knn_dists, uint64_t* rows_recomputed);
+int umap_knn_bruteforce_device(const float* dev_data, uint64_t n, uint64_t dim, uint64_t k,
+                               uint32_t* dev_knn_indices, float* dev_knn_dists, uint64_t* rows_recomputed);
+
 /* ---- batched instances (no counterpart in the reference: a fit per dataset) --------
  * n_instances independent fits in one problem.  Instance s owns points
  * [offsets[s], offsets[s+1]) of the concatenated arrays (host offsets, u64[n_instances+1],

@@ -67,6 +67,10 @@ def lib():
         L.orc_optimizer_embedding.argtypes = [P, P]
         L.orc_optimizer_set_embedding.argtypes = [P, P]
         L.orc_optimizer_set_metric_type.argtypes = [P, i32]
+        L.orc_knn_bruteforce.argtypes = [P, u64, u64, u64, P, P]
+        L.orc_knn_bruteforce.restype = None
+        L.orc_knn_bruteforce_rows.argtypes = [P, u64, u64, u64, u64, u64, P, P]
+        L.orc_knn_bruteforce_rows.restype = None
         L.orc_optimizer_step_epochs.argtypes = [P, u64, P, P]
         L.orc_optimizer_step_epochs.restype = i32
         _lib = L
@@ -280,3 +284,16 @@ def fit(knn_idx, knn_dist, init, cfg: OracleConfig | None = None, seed: int = 0,
     empty = (ip[1:] - ip[:-1]) == 0
     emb[empty] = np.nan
     return emb, m, opt
+
+
+def knn_bruteforce(X, k: int, rows=None):
+    """examples/src/bin/mnist_demo.rs:203-229 (brute force, self excluded, stable by distance).
+    `rows` = (r0, r1) computes only those query rows (against all points)."""
+    x = np.ascontiguousarray(X, dtype=np.float32)
+    n, d = x.shape
+    r0, r1 = (0, n) if rows is None else rows
+    idx = np.zeros((r1 - r0, k), np.uint32)
+    dist = np.zeros((r1 - r0, k), np.float32)
+    if r1 > r0:
+        lib().orc_knn_bruteforce_rows(_ptr(x), n, d, k, r0, r1, _ptr(idx), _ptr(dist))
+    return idx, dist

@@ -853,4 +853,42 @@ int orc_optimizer_step_epochs(OrcOptimizer* o, uint64_t n_ep, uint64_t* fires, u
   return 0;
 }
 
+// examples/src/bin/mnist_demo.rs:203-239 compute_knn: for each row, the distances to every
+// other row (f32, (x - y)^2 summed in coordinate order, then sqrt), stably sorted by distance
+// (ties in index order), the first k kept; slots beyond n - 1 stay 0 / 0.0.
+// Rows [r0, r1) only (outputs [r1 - r0, k]): a sample of the workload for timing and spot checks.
+void orc_knn_bruteforce_rows(const float* X, uint64_t n, uint64_t d, uint64_t k, uint64_t r0, uint64_t r1,
+                             uint32_t* idx, float* dist) {
+  memset(idx, 0, (r1 - r0) * k * 4);
+  memset(dist, 0, (r1 - r0) * k * 4);
+  parallel_for(r1 - r0, [&](uint64_t b, uint64_t e, int) {
+    std::vector<std::pair<float, uint32_t>> cand;
+    cand.reserve(n);
+    for (uint64_t i = r0 + b; i < r0 + e; ++i) {
+      cand.clear();
+      const float* x = X + i * d;
+      for (uint64_t j = 0; j < n; ++j) {
+        if (j == i) continue;
+        const float* y = X + j * d;
+        float acc = -0.0f;
+        for (uint64_t c = 0; c < d; ++c) {
+          float df = x[c] - y[c];
+          acc = acc + df * df;
+        }
+        cand.emplace_back(sqrtf(acc), (uint32_t)j);
+      }
+      const uint64_t m = std::min<uint64_t>(k, cand.size());
+      std::partial_sort(cand.begin(), cand.begin() + m, cand.end());  // (distance, index) order
+      for (uint64_t t = 0; t < m; ++t) {
+        idx[(i - r0) * k + t] = cand[t].second;
+        dist[(i - r0) * k + t] = cand[t].first;
+      }
+    }
+  }, 16);
+}
+
+void orc_knn_bruteforce(const float* X, uint64_t n, uint64_t d, uint64_t k, uint32_t* idx, float* dist) {
+  orc_knn_bruteforce_rows(X, n, d, k, 0, n, idx, dist);
+}
+
 }  // extern "C"

@@ -306,3 +306,36 @@ def test_generic_rule_schedule_matches_euclidean(oracle):
     assert np.array_equal(F0, F1) and np.array_equal(N0, N1)
     e = og.embedding()
     assert np.isfinite(e).all()
+
+
+# ---------------------------------------------------------------- kNN producer
+def np_knn_bruteforce(X, k):
+    """mnist_demo.rs:203-239 in numpy float32: per row, (x - y)^2 summed column by column, sqrt,
+    a stable sort by distance (ties in index order), self excluded, zeros past n - 1."""
+    X = np.asarray(X, np.float32)
+    n, d = X.shape
+    idx = np.zeros((n, k), np.uint32)
+    dist = np.zeros((n, k), np.float32)
+    for i in range(n):
+        acc = np.zeros(n, np.float32)
+        for c in range(d):
+            df = (X[i, c] - X[:, c]).astype(np.float32)
+            acc = (acc + df * df).astype(np.float32)
+        dd = np.sqrt(acc)
+        others = np.delete(np.arange(n), i)
+        order = others[np.argsort(dd[others], kind="stable")][:k]
+        idx[i, :len(order)] = order
+        dist[i, :len(order)] = dd[order]
+    return idx, dist
+
+
+@pytest.mark.parametrize("n,d,k", [(1, 3, 4), (2, 1, 3), (7, 3, 10), (60, 5, 15), (300, 17, 32)])
+def test_knn_oracle_matches_numpy(oracle, n, d, k):
+    g = np.random.Generator(np.random.PCG64(n * 31 + d))
+    X = g.normal(0, 1, (n, d)).astype(np.float32)
+    if n >= 60:
+        X[::3] = np.round(X[::3])       # exact ties and duplicate rows
+        X[5] = X[2]
+    i1, d1 = oracle.knn_bruteforce(X, k)
+    i2, d2 = np_knn_bruteforce(X, k)
+    assert np.array_equal(i1, i2) and np.array_equal(d1, d2)

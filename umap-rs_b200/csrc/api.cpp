@@ -1966,6 +1966,46 @@ int umap_smooth_knn_dist_device(const float* dists, uint64_t n, uint64_t k, uint
   API_END
 }
 
+// Exact brute-force kNN (examples/src/bin/mnist_demo.rs:203-229) on the tensor cores.
+static void knn_entry(const float* X, uint64_t n, uint64_t dim, uint64_t k, uint32_t* idx, float* dist,
+                      uint64_t* rows_recomputed, bool host) {
+  cudaStream_t s;
+  UB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  struct SGuard { cudaStream_t s; ~SGuard() { (void)cudaStreamSynchronize(s); (void)cudaStreamDestroy(s); } } g{s};
+  if (!host) wait_for_inputs();
+  if (n && dim && n > UINT64_MAX / dim) throw Error(INVALID_ARGUMENT, "n * dim overflows");
+  KnnStats st;
+  if (host) {
+    DevBuf<float> dx(n * dim, s);
+    DevBuf<uint32_t> di(n * k, s);
+    DevBuf<float> dd(n * k, s);
+    h2d(dx.p, X, n * dim, s);
+    st = knn_bruteforce(dx.p, n, dim, k, di.p, dd.p, s);
+    d2h(idx, di.p, n * k, s);
+    d2h(dist, dd.p, n * k, s);
+    UB_CUDA(cudaStreamSynchronize(s));
+  } else {
+    st = knn_bruteforce(X, n, dim, k, idx, dist, s);
+  }
+  if (rows_recomputed) *rows_recomputed = st.fallback_rows;
+}
+
+int umap_knn_bruteforce(const float* data, uint64_t n, uint64_t dim, uint64_t k, uint32_t* knn_indices,
+                        float* knn_dists, uint64_t* rows_recomputed) {
+  API_BEGIN
+  need(data, "data"); need(knn_indices, "knn_indices"); need(knn_dists, "knn_dists");
+  knn_entry(data, n, dim, k, knn_indices, knn_dists, rows_recomputed, true);
+  API_END
+}
+
+int umap_knn_bruteforce_device(const float* data, uint64_t n, uint64_t dim, uint64_t k, uint32_t* knn_indices,
+                               float* knn_dists, uint64_t* rows_recomputed) {
+  API_BEGIN
+  need(data, "data"); need(knn_indices, "knn_indices"); need(knn_dists, "knn_dists");
+  knn_entry(data, n, dim, k, knn_indices, knn_dists, rows_recomputed, false);
+  API_END
+}
+
 int umap_radix_sort_pairs_device(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
                                  uint32_t* vals_out, uint64_t n, int end_bit) {
   API_BEGIN

@@ -824,7 +824,7 @@ void prepare_all_gemms() {
 // ------------------------------------------------------------------------------ TMA tensor maps
 // Tensor map of a row-major bf16 matrix [rows, cols] (row stride ld elements) read in boxes of
 // box_rows x 64 with 128-byte swizzle.
-CUtensorMap bf16_tile_map(const void* base, int64_t rows, int64_t cols, int64_t ld, int box_rows) {
+CUtensorMap bf16_tile_map(const void* base, int64_t rows, int64_t cols, int64_t ld, int box_rows, bool f16) {
   if (reinterpret_cast<uintptr_t>(base) % 16 || (ld * 2) % 16 || cols < 64 || rows < box_rows)
     throw Error(INVALID_ARGUMENT, "TMA operand must be 16-byte aligned with 16-byte rows");
   CUtensorMap m;
@@ -832,7 +832,7 @@ CUtensorMap bf16_tile_map(const void* base, int64_t rows, int64_t cols, int64_t 
   const cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
   const cuuint32_t box[2] = {64u, (cuuint32_t)box_rows};
   const cuuint32_t estr[2] = {1, 1};
-  const CUresult r = encode_tiled()(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides,
+  const CUresult r = encode_tiled()(&m, f16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides,
                                     box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) throw Error(CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");

@@ -286,4 +286,17 @@ class Mlp {
 void umma_gemm_f32(const void* A, const void* B, float* C, int64_t M, int64_t N, int64_t K, int ksplit,
                    cudaStream_t s);
 
+// Exact brute-force kNN (knn.cu): for each of the n rows of X [n, d] (f32, device), the k
+// nearest other rows by the reference example's f32 Euclidean distance, ordered by (distance,
+// index); out_idx / out_dist [n, k] on the device.  Synchronises `s`.
+constexpr int KNN_MAX_K = 32;
+struct KnnStats {
+  uint32_t splits = 0;         // database splits of the candidate pass
+  uint32_t fallback_rows = 0;  // rows whose certificate failed and were recomputed exactly
+  float scale = 1.0f;          // power of two applied to the centred rows before FP16 rounding
+  uint32_t reordered = 0;      // 1 when the scan ran in pivot (locality) order
+};
+KnnStats knn_bruteforce(const float* X, uint64_t n, uint64_t d, uint64_t k, uint32_t* out_idx, float* out_dist,
+                        cudaStream_t s);
+
 }  // namespace ub

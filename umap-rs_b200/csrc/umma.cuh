@@ -44,6 +44,10 @@ __device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t saddr) {
 __host__ __device__ constexpr uint32_t instr_desc(int M, int N) {
   return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
+// The same with A and B FP16 (format 0 in bits 7-9 and 10-12).
+__host__ __device__ constexpr uint32_t instr_desc_f16(int M, int N) {
+  return (1u << 4) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
 
 __device__ __forceinline__ uint64_t global_ns() {
   uint64_t t;
@@ -71,8 +75,8 @@ __device__ __forceinline__ bool mbar_wait(uint32_t addr, uint32_t phase) {
 
 }  // namespace umma
 
-// Tensor map of a row-major bf16 matrix [rows, cols] (row stride ld elements) read in boxes of
-// box_rows x 64 with 128-byte swizzle (defined in mlp.cu).
-CUtensorMap bf16_tile_map(const void* base, int64_t rows, int64_t cols, int64_t ld, int box_rows);
+// Tensor map of a row-major bf16 (or, with f16, fp16) matrix [rows, cols] (row stride ld
+// elements) read in boxes of box_rows x 64 with 128-byte swizzle (defined in mlp.cu).
+CUtensorMap bf16_tile_map(const void* base, int64_t rows, int64_t cols, int64_t ld, int box_rows, bool f16 = false);
 
 }  // namespace ub

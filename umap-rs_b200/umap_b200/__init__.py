@@ -30,7 +30,7 @@ from . import _lib
 __all__ = [
     "ManifoldParams", "GraphParams", "OptimizationParams", "UmapConfig", "MetricType",
     "EuclideanMetric", "GenericEuclideanMetric", "Metric", "OUTPUT_METRIC_EUCLIDEAN", "Umap", "LearnedManifold", "Optimizer", "FittedUmap",
-    "SparseMat", "UmapError", "find_ab_params", "lib",
+    "SparseMat", "UmapError", "find_ab_params", "lib", "knn_bruteforce", "KNN_MAX_K",
 ]
 
 lib = _lib.load
@@ -217,6 +217,35 @@ def batch_fit(config: UmapConfig, offsets, knn_indices, knn_dists, init):
     _check(L.umap_batch_fit(C.byref(cfg), n_inst, off.ctypes.data_as(C.c_void_p), pi, pd, k, pn, d,
                             out.ctypes.data_as(C.c_void_p)))
     return out
+
+
+KNN_MAX_K = 32
+
+
+def knn_bruteforce(data, k: int, return_stats: bool = False):
+    """Exact k nearest neighbours of every row of `data` [n, dim] (numpy f32 or a CUDA
+    tensor), as the reference's example computes them (examples/src/bin/mnist_demo.rs:203-229):
+    f32 Euclidean distance summed in coordinate order, self excluded, ordered by distance then
+    index, missing slots 0 / 0.0 when n - 1 < k.  Returns (indices u32 [n, k], distances f32
+    [n, k]) of the input's kind (numpy, or int32/float32 CUDA tensors), plus the number of rows
+    recomputed exactly after a failed certificate when `return_stats`."""
+    L = _lib.load()
+    n, dim = int(data.shape[0]), int(data.shape[1])
+    rec = C.c_uint64()
+    if _is_cuda_tensor(data):
+        import torch
+        t, p = _device(data, torch.float32)
+        idx = torch.empty((n, k), dtype=torch.int32, device=t.device)
+        dist = torch.empty((n, k), dtype=torch.float32, device=t.device)
+        _check(L.umap_knn_bruteforce_device(p, n, dim, k, C.c_void_p(idx.data_ptr() if n else 1),
+                                            C.c_void_p(dist.data_ptr() if n else 1), C.byref(rec)))
+    else:
+        a, p = _host(data, np.float32)
+        idx = np.zeros((n, k), np.uint32)
+        dist = np.zeros((n, k), np.float32)
+        _check(L.umap_knn_bruteforce(p, n, dim, k, idx.ctypes.data_as(C.c_void_p) if n else C.c_void_p(1),
+                                     dist.ctypes.data_as(C.c_void_p) if n else C.c_void_p(1), C.byref(rec)))
+    return (idx, dist, rec.value) if return_stats else (idx, dist)
 
 
 def release_cached_memory() -> int:

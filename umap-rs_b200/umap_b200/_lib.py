@@ -89,6 +89,8 @@ SIGNATURES = {
     "umap_fitted_serialize_bincode": [P, P, u64, C.POINTER(u64)],
     "umap_fitted_deserialize_bincode": [P, u64, PP],
     "umap_smooth_knn_dist_device": [P, u64, u64, u64, f32, f32, P, P],
+    "umap_knn_bruteforce": [P, u64, u64, u64, P, P, C.POINTER(u64)],
+    "umap_knn_bruteforce_device": [P, u64, u64, u64, P, P, C.POINTER(u64)],
     "umap_radix_sort_pairs_device": [P, P, P, P, u64, i32],
     "umap_radix_sort_pairs_device_noalloc": [P, P, P, P, u64, i32, P],
     "umap_radix_sort_noalloc_max_pairs": [C.POINTER(u64)],

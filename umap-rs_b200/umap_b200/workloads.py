@@ -62,6 +62,39 @@ def gaussians_2m(n: int = 2_000_000):
     return gaussian_mixture(n, 64, 50, 8.0, seed=1, anisotropic=True, dirichlet=True)
 
 
+def digits_like(n: int = 70_000, side: int = 28, n_classes: int = 10, seed: int = 5):
+    """Synthetic stand-in with MNIST's shape and value distribution (no dataset is read):
+    n images of side x side pixels in [0, 1], mostly zero.  Each class is a prototype of a few
+    Gaussian strokes; a sample is its prototype shifted by up to 2 pixels, scaled in
+    intensity, with pixel noise, clipped to [0, 1] and zeroed below 0.2.  Returns
+    (X f32[n, side * side], labels i32[n])."""
+    g = _rng(seed)
+    yy, xx = np.mgrid[0:side, 0:side].astype(np.float32)
+    protos = np.zeros((n_classes, side, side), np.float32)
+    for c in range(n_classes):
+        for _ in range(g.integers(3, 7)):
+            cy, cx = g.uniform(6, side - 6, 2)
+            sy, sx = g.uniform(1.0, 4.0, 2)
+            protos[c] += np.exp(-((yy - cy) ** 2 / (2 * sy * sy) + (xx - cx) ** 2 / (2 * sx * sx)))
+        protos[c] /= protos[c].max()
+    labels = g.integers(0, n_classes, n).astype(np.int32)
+    X = np.empty((n, side * side), np.float32)
+    chunk = 8192
+    for s in range(0, n, chunk):
+        e = min(n, s + chunk)
+        m = e - s
+        sh = g.integers(-2, 3, (m, 2))
+        img = np.empty((m, side, side), np.float32)
+        for i in range(m):
+            img[i] = np.roll(protos[labels[s + i]], (sh[i, 0], sh[i, 1]), axis=(0, 1))
+        img *= g.uniform(0.6, 1.0, (m, 1, 1)).astype(np.float32)
+        img += g.normal(0, 0.1, img.shape).astype(np.float32)
+        np.clip(img, 0.0, 1.0, out=img)
+        img[img < 0.2] = 0.0
+        X[s:e] = img.reshape(m, -1)
+    return X, labels
+
+
 def swiss_roll(n: int, seed: int = 2):
     g = _rng(seed)
     t = g.uniform(1.5 * math.pi, 4.5 * math.pi, size=n)

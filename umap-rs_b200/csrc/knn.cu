@@ -18,11 +18,13 @@
 //       256 rows: warp 0 issues TMA loads (128-byte swizzle, 3 stages of a 128 x 64 query chunk
 //       and a 256 x 64 database chunk), warp 1 issues tcgen05.mma (M=128, N=256, K=16, FP16,
 //       FP32 accumulation) into one of two 256-column tensor-memory accumulators, and warps
-//       2-5 read the other accumulator with tcgen05.ld (thread = query row).  For a dot product
+//       2-9 read the other accumulator with tcgen05.ld (thread = query row; warps 2-5 take
+//       the first 128 columns of a tile, warps 6-9 the rest).  For a dot product
 //       s with database row y the approximate squared distance is |q|^2 + |y|^2 - 2s; the
 //       epilogue tests v = 2s - |y|^2 against the row's threshold |q|^2 - tau in registers and
-//       only on a hit inserts into the row's list of the C = 64 smallest (a max-heap in shared
-//       memory whose root is tau), so the common path costs two instructions per candidate.
+//       only on a hit inserts into its half's list of the 32 smallest (a max-heap in shared
+//       memory whose root is tau), so the common path costs two instructions per candidate;
+//       the two halves' lists together are the row's C = 64 candidates.
 //       The scan takes 16 tiles around the query block's own tile first, then the rest in the
 //       order all CTAs share; the producer warp also bulk-copies each tile's row norms into a
 //       ring of shared-memory slots.
@@ -60,10 +62,11 @@ constexpr int DBN = 256;     // database rows per tile (UMMA N)
 constexpr int KC = 64;       // K per staged chunk (128 bytes of bf16)
 constexpr int TS = 3;        // pipeline stages
 constexpr int NCAND = 64;    // candidates kept per row and database split
-constexpr int KNN_THREADS = 192;
+constexpr int HC = NCAND / 2;  // per epilogue warpgroup (each takes half of a tile's columns)
+constexpr int KNN_THREADS = 320;
 constexpr uint32_t Q_BYTES = QM * 128, D_BYTES = DBN * 128, STAGE = Q_BYTES + D_BYTES;
 constexpr int NBS = 4;      // slots of the ring of per-tile row norms
-constexpr size_t KNN_SMEM = (size_t)TS * STAGE + (size_t)NCAND * QM * 8 + (size_t)16 * QM * 4 + NBS * DBN * 4 + 1024;
+constexpr size_t KNN_SMEM = (size_t)TS * STAGE + (size_t)NCAND * QM * 8 + (size_t)2 * 8 * QM * 4 + NBS * DBN * 4 + 1024;
 static_assert(STAGE % 1024 == 0, "stages stay 1024-byte aligned");
 constexpr float PAD_NORM = 3.0e38f;  // |y|^2 of padding rows: never a candidate
 constexpr uint64_t KNN_REORDER_MIN = 16384;  // scan in locality order from this many points
@@ -237,10 +240,10 @@ __global__ void __launch_bounds__(KNN_THREADS, 1) knn_candidates_kernel(
   __shared__ uint32_t tmem_base;
   __shared__ volatile int s_fail;
   uint8_t* smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
-  float* cd = reinterpret_cast<float*>(smem + TS * STAGE);  // [NCAND][QM]
+  float* cd = reinterpret_cast<float*>(smem + TS * STAGE);  // [2][HC][QM] heaps of the two halves
   uint32_t* ci = reinterpret_cast<uint32_t*>(cd + NCAND * QM);
-  float* vst = reinterpret_cast<float*>(ci + NCAND * QM);  // [16][QM]
-  float* nbuf = vst + 16 * QM;                             // [NBS][DBN] norms of the tile's rows
+  float* vst = reinterpret_cast<float*>(ci + NCAND * QM);  // [2][8][QM]
+  float* nbuf = vst + 2 * 8 * QM;                          // [NBS][DBN] norms of the tile's rows
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int64_t m0 = (int64_t)blockIdx.x * QM;
   const int split = blockIdx.y, n_splits = gridDim.y;
@@ -276,11 +279,11 @@ __global__ void __launch_bounds__(KNN_THREADS, 1) knn_candidates_kernel(
     }
     for (int i = 0; i < 2; ++i) {
       asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(&tfull[i])), "r"(1) : "memory");
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(&tempty[i])), "r"(QM) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(&tempty[i])), "r"(2 * QM) : "memory");
     }
     for (int i = 0; i < NBS; ++i) {
       asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(&nfull[i])), "r"(1) : "memory");
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(&nempty[i])), "r"(QM) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(&nempty[i])), "r"(2 * QM) : "memory");
     }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     s_fail = 0;
@@ -375,15 +378,20 @@ __global__ void __launch_bounds__(KNN_THREADS, 1) knn_candidates_kernel(
       // the last MMAs must have completed before tensor memory is freed
       if (g > 0) (void)mbar_wait(smem_u32(&empty[(g - 1) % TS]), (uint32_t)(((g - 1) / TS) & 1));
     }
-  } else {  // epilogue: warps 2..5 own tensor-memory lane quarters 2, 3, 0, 1
-    const int q = warp & 3;
+  } else {
+    // epilogue: warps 2..9; warp w owns tensor-memory lane quarter w % 4 (query rows) and half
+    // (w - 2) / 4 of each tile's columns, with its own heap of HC candidates per row
+    const int q = warp & 3, half = (warp - 2) >> 2;
     const int trow = q * 32 + lane;
     const int64_t row = m0 + trow;
     const bool live = row < n;
     const float nq = live ? nb[row] : 0.0f;
-    for (int s = 0; s < NCAND; ++s) {
-      cd[s * QM + trow] = INFINITY;
-      ci[s * QM + trow] = 0xFFFFFFFFu;
+    float* hd = cd + half * HC * QM;
+    uint32_t* hi = ci + half * HC * QM;
+    float* vs = vst + half * 8 * QM;
+    for (int s = 0; s < HC; ++s) {
+      hd[s * QM + trow] = INFINITY;
+      hi[s * QM + trow] = 0xFFFFFFFFu;
     }
     float tau = INFINITY, thr = live ? -INFINITY : INFINITY;
     // 32 columns of the accumulator: v = 2 s - |y|^2; a column enters the heap when
@@ -402,41 +410,42 @@ __global__ void __launch_bounds__(KNN_THREADS, 1) knn_candidates_kernel(
       }
       if (!(vmax > thr)) return;
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        // stage 16 values (dynamic index below) and mark those above the threshold
+      for (int h = 0; h < 4; ++h) {
+        // stage 8 values (dynamic index below) and mark those above the threshold
         uint32_t hits = 0;
 #pragma unroll
-        for (int i = 0; i < 16; ++i) {
-          vst[i * QM + trow] = v[16 * h + i];
-          hits |= (v[16 * h + i] > thr ? 1u : 0u) << i;
+        for (int i = 0; i < 8; ++i) {
+          vs[i * QM + trow] = v[8 * h + i];
+          hits |= (v[8 * h + i] > thr ? 1u : 0u) << i;
         }
         while (hits) {
           const int i = __ffs(hits) - 1;
           hits &= hits - 1;
-          const int64_t col = c0 + 16 * h + i;
-          const float a = nq - vst[i * QM + trow];
+          const int64_t col = c0 + 8 * h + i;
+          const float a = nq - vs[i * QM + trow];
           if (!(a < tau) || col >= n || col == row) continue;
           // max-heap on the approximate distance: replace the root, sift down
           int pos = 0;
           for (;;) {
             const int l = 2 * pos + 1;
-            if (l >= NCAND) break;
-            const float dl = cd[l * QM + trow];
-            const float dr = l + 1 < NCAND ? cd[(l + 1) * QM + trow] : -INFINITY;
+            if (l >= HC) break;
+            const float dl = hd[l * QM + trow];
+            const float dr = l + 1 < HC ? hd[(l + 1) * QM + trow] : -INFINITY;
             const int c = dr > dl ? l + 1 : l;
             const float dc = dr > dl ? dr : dl;
             if (!(dc > a)) break;
-            cd[pos * QM + trow] = dc;
-            ci[pos * QM + trow] = ci[c * QM + trow];
+            hd[pos * QM + trow] = dc;
+            hi[pos * QM + trow] = hi[c * QM + trow];
             pos = c;
           }
-          cd[pos * QM + trow] = a;
-          ci[pos * QM + trow] = (uint32_t)col;
-          tau = cd[trow];
+          hd[pos * QM + trow] = a;
+          hi[pos * QM + trow] = (uint32_t)col;
+          tau = hd[trow];
           thr = nq - tau;
         }
       }
     };
+    constexpr int CH = DBN / 64;  // 32-column chunks per half tile
     for (int t = 0; t < T; ++t) {
       const int buf = t & 1;
       const int slot = t % NBS;
@@ -446,23 +455,23 @@ __global__ void __launch_bounds__(KNN_THREADS, 1) knn_candidates_kernel(
         break;
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const int64_t cb0 = tile_of(t) * DBN;
-      const float* nrm = nbuf + slot * DBN;
-      const uint32_t ta = tbase + ((uint32_t)(q * 32) << 16) + (uint32_t)(buf * DBN);
+      const int64_t cb0 = tile_of(t) * DBN + half * (DBN / 2);
+      const float* nrm = nbuf + slot * DBN + half * (DBN / 2);
+      const uint32_t ta = tbase + ((uint32_t)(q * 32) << 16) + (uint32_t)(buf * DBN + half * (DBN / 2));
       // tensor-memory loads run one 32-column chunk ahead of the arithmetic
       uint32_t ra[32], rb[32];
       tmem_ld32(ra, ta);
       tmem_wait32(ra);
 #pragma unroll 1
-      for (int jj = 0; jj < DBN / 32; jj += 2) {
+      for (int jj = 0; jj < CH; jj += 2) {
         tmem_ld32(rb, ta + (uint32_t)(jj + 1) * 32);
         process(ra, nrm + jj * 32, cb0 + jj * 32);
         __syncwarp();
         tmem_wait32(rb);
-        if (jj + 2 < DBN / 32) tmem_ld32(ra, ta + (uint32_t)(jj + 2) * 32);
+        if (jj + 2 < CH) tmem_ld32(ra, ta + (uint32_t)(jj + 2) * 32);
         process(rb, nrm + (jj + 1) * 32, cb0 + (jj + 1) * 32);
         __syncwarp();
-        if (jj + 2 < DBN / 32) tmem_wait32(ra);
+        if (jj + 2 < CH) tmem_wait32(ra);
       }
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" :: "r"(smem_u32(&tempty[buf])) : "memory");
@@ -471,13 +480,13 @@ __global__ void __launch_bounds__(KNN_THREADS, 1) knn_candidates_kernel(
     }
     if (live && !s_fail) {  // outputs by original row index, candidates as original indices
       const int64_t orow = perm ? (int64_t)perm[row] : row;
-      const int64_t base = (orow * n_splits + split) * NCAND;
-      for (int s = 0; s < NCAND; ++s) {
-        const uint32_t c = ci[s * QM + trow];
+      const int64_t base = (orow * n_splits + split) * NCAND + half * HC;
+      for (int s = 0; s < HC; ++s) {
+        const uint32_t c = hi[s * QM + trow];
         cand_idx[base + s] = (perm && c < (uint64_t)n) ? perm[c] : c;
-        cand_d[base + s] = cd[s * QM + trow];
+        cand_d[base + s] = hd[s * QM + trow];
       }
-      tau_out[orow * n_splits + split] = tau;
+      tau_out[(orow * n_splits + split) * 2 + half] = tau;
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -575,7 +584,7 @@ __global__ void __launch_bounds__(256) knn_rerank_kernel(
     }
     if (lane == 0 && last != ~0ull) {
       float tau = INFINITY;
-      for (int s = 0; s < S; ++s) tau = fminf(tau, tau_in[row * S + s]);
+      for (int s = 0; s < 2 * S; ++s) tau = fminf(tau, tau_in[row * 2 * S + s]);  // (split, half)
       if (tau < INFINITY) {
         const float lb = distance_lower_bound(tau, rn[row], __uint_as_float(*rmax_bits), gamma, scale, d, dp);
         if (!(__uint_as_float((uint32_t)(last >> 32)) < lb)) fail_rows[atomicAdd(fail_count, 1u)] = (uint32_t)row;
@@ -815,7 +824,7 @@ KnnStats knn_bruteforce(const float* X, uint64_t n, uint64_t d, uint64_t k, uint
   }
 
   DevBuf<uint32_t> cidx(n * S * NCAND, s);
-  DevBuf<float> cdist(n * S * NCAND, s), tau(n * S, s);
+  DevBuf<float> cdist(n * S * NCAND, s), tau(n * S * 2, s);
   const CUtensorMap tq = bf16_tile_map(xh.p, n_pad, dp, dp, QM, true);
   const CUtensorMap tdb = bf16_tile_map(xh.p, n_pad, dp, dp, DBN, true);
   knn_candidates_kernel<<<dim3((unsigned)q_blocks, (unsigned)S), KNN_THREADS, KNN_SMEM, s>>>(

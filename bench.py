@@ -46,7 +46,7 @@ def parse():
                     help="profiling run: build one optimizer, run --profile-epochs epochs, exit")
     ap.add_argument("--profile-epochs", type=int, default=24)
     ap.add_argument("--workload", default="gaussians_2m",
-                    choices=["gaussians_2m", "batched", "warm_start", "swiss_roll", "mlp"],
+                    choices=["gaussians_2m", "batched", "warm_start", "swiss_roll", "mlp", "knn"],
                     help="batched: 4096 independent instances, 200 epochs, vs a per-instance loop; "
                          "warm_start: learned initial embedding + a shortened fit vs the plain fit")
     ap.add_argument("--sub", type=int, default=100_000, help="warm_start: subsample size")
@@ -55,6 +55,9 @@ def parse():
     ap.add_argument("--n-swiss", type=int, default=100_000_000, help="swiss_roll: points")
     ap.add_argument("--swiss-epochs", type=int, default=200, help="swiss_roll: epochs")
     ap.add_argument("--instances", type=int, default=4096)
+    ap.add_argument("--knn-n", type=int, default=70_000, help="knn: points")
+    ap.add_argument("--knn-k", type=int, default=15, help="knn: neighbours")
+    ap.add_argument("--knn-cpu-rows", type=int, default=600, help="knn: query rows the oracle times")
     ap.add_argument("--loop-sample", type=int, default=8,
                     help="per-instance loop timed on every n-th instance, scaled by n")
     return ap.parse_args()
@@ -551,6 +554,96 @@ def run_mlp(a):
                       "gpu_launches": ub.kernel_launches() - launches0, "clocks": clk.summary()}), flush=True)
 
 
+def run_knn(a):
+    """The kNN producer (the step before the fit path; the reference's example computes it by
+    brute force, examples/src/bin/mnist_demo.rs:203-229): exact k=15 neighbours of all rows of
+    an MNIST-shaped synthetic set (70,000 x 784, values in [0, 1], ~22% non-zero; no dataset is
+    read).  value = query rows per second from inputs resident in HBM (220 MB of inputs, more
+    than L2); e2e = the host-pointer call (H2D of the data, D2H of indices and distances).
+    Roofline: the tensor-core candidate pass, 2 n^2 D algorithmic FLOPs per call over its
+    CUDA-event time, against the measured dense BF16 peak (FP16 runs at the same rate).
+    cpu_baseline: the oracle's brute force (all host threads) on the first --knn-cpu-rows query
+    rows against all points, scaled to rows/s.  --profile: one call after one warm-up."""
+    import torch
+    import umap_b200 as ub
+    from umap_b200 import workloads as W
+    torch.cuda.set_device(0)
+    n, k = a.knn_n, a.knn_k
+    X, _ = W.digits_like(n)
+    d = X.shape[1]
+    t = torch.from_numpy(X).cuda()
+    torch.cuda.synchronize()
+    if a.profile:
+        ub.knn_bruteforce(t, k)
+        ub.knn_bruteforce(t, k)
+        torch.cuda.synchronize()
+        print(json.dumps({"profile": True, "workload": "knn", "n": n}), flush=True)
+        return
+    for _ in range(max(1, a.warmup)):
+        ub.knn_bruteforce(t, k)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0 = ub.kernel_launches()
+    cand_ms, recomputed = [], 0
+    with Clocks(0) as clk:
+        ev0.record()
+        for _ in range(a.steps):
+            ub.knn_bruteforce(t, k)
+            ms, rec, _ = ub.knn_last_profile()
+            cand_ms.append(ms)
+            recomputed += rec
+        ev1.record()
+        torch.cuda.synchronize()
+    launches = ub.kernel_launches() - launches0
+    ms_step = ev0.elapsed_time(ev1) / a.steps
+    value = n / (ms_step / 1e3)
+    # e2e: numpy in, numpy out through the host-pointer C ABI
+    e2e = []
+    for _ in range(max(1, a.e2e_steps)):
+        t0 = time.perf_counter()
+        ub.knn_bruteforce(X, k)
+        e2e.append(time.perf_counter() - t0)
+    e2e_s = min(e2e)
+    flops = 2.0 * n * n * d
+    cms = float(np.mean(cand_ms))
+    achieved = flops / (cms / 1e3) / 1e12
+    pk = peaks().get("bf16_tflops")
+    traffic = None
+    try:
+        for line in open(os.path.join(ROOT, "profiles", "knn_candidates_digits70k.md")):
+            if line.startswith("traffic_bytes_per_launch:"):
+                traffic = float(line.split(":", 1)[1].split()[0])
+    except OSError:
+        pass
+    cpu = None
+    if not a.no_cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        O.build()
+        cores = os.cpu_count() or 1
+        O.set_threads(cores)
+        rows = min(a.knn_cpu_rows, n)
+        t0 = time.perf_counter()
+        O.knn_bruteforce(X, k, rows=(0, rows))
+        dt = time.perf_counter() - t0
+        cpu = {"value": rows / dt, "unit": "rows/s", "cores": cores, "kind": "port",
+               "sample": f"oracle brute force (mnist_demo.rs:203-239 restated) for query rows 0..{rows} "
+                         f"against all {n} points in {dt:.2f} s"}
+    print(json.dumps({
+        "metric": "exact kNN query rows/s", "value": value, "unit": "rows/s", "n_gpus": 1, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f16 candidates, f32 exact distances", "data": "synthetic",
+        "config": {"workload": f"knn digits-like {n}x{d} k={k}", "n_points": n, "dim": d, "k": k,
+                   "l2": "inputs exceed L2 (220 MB)"},
+        "rows_recomputed_exactly": recomputed,
+        "e2e": {"value": n / e2e_s, "unit": "rows/s", "ms_per_step": e2e_s * 1e3,
+                "h2d_bytes_per_step": int(X.nbytes), "d2h_bytes_per_step": int(n * k * 8)},
+        "roofline": {"bound": "tensor", "kernel": "knn_candidates_kernel", "achieved": achieved, "peak": pk,
+                     "unit": "TFLOP/s", "frac": achieved / pk if pk else None, "peak_source": "measured",
+                     "traffic": traffic, "algorithmic_flops_per_launch": flops, "avg_launch_ms": cms},
+        "gpu_launches": launches, "clocks": clk.summary(), "cpu_baseline": cpu}), flush=True)
+
+
 def main():
     a = parse()
     if a.impl == "reference":
@@ -563,6 +656,8 @@ def main():
         return run_swiss_roll(a)
     if a.workload == "mlp":
         return run_mlp(a)
+    if a.workload == "knn":
+        return run_knn(a)
     import torch
     import umap_b200 as ub
     from umap_b200 import replicas as R

@@ -228,6 +228,9 @@ int umap_knn_bruteforce(const float* host_data, uint64_t n, uint64_t dim, uint64
                         uint32_t* host_knn_indices, float* host_knn_dists, uint64_t* rows_recomputed);
 int umap_knn_bruteforce_device(const float* dev_data, uint64_t n, uint64_t dim, uint64_t k,
                                uint32_t* dev_knn_indices, float* dev_knn_dists, uint64_t* rows_recomputed);
+/* Profile of this thread's last kNN call: CUDA-event time of the tensor-core candidate pass,
+ * rows recomputed exactly, and whether the scan ran in pivot (locality) order.  Nullable. */
+int umap_knn_last_profile(float* candidate_pass_ms, uint64_t* rows_recomputed, uint32_t* reordered);
 
 /* ---- batched instances (no counterpart in the reference: a fit per dataset) --------
  * n_instances independent fits in one problem.  Instance s owns points

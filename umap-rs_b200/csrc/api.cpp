@@ -1967,6 +1967,7 @@ int umap_smooth_knn_dist_device(const float* dists, uint64_t n, uint64_t k, uint
 }
 
 // Exact brute-force kNN (examples/src/bin/mnist_demo.rs:203-229) on the tensor cores.
+thread_local KnnStats g_knn_last;
 static void knn_entry(const float* X, uint64_t n, uint64_t dim, uint64_t k, uint32_t* idx, float* dist,
                       uint64_t* rows_recomputed, bool host) {
   cudaStream_t s;
@@ -1988,6 +1989,15 @@ static void knn_entry(const float* X, uint64_t n, uint64_t dim, uint64_t k, uint
     st = knn_bruteforce(X, n, dim, k, idx, dist, s);
   }
   if (rows_recomputed) *rows_recomputed = st.fallback_rows;
+  g_knn_last = st;
+}
+
+int umap_knn_last_profile(float* candidate_pass_ms, uint64_t* rows_recomputed, uint32_t* reordered) {
+  API_BEGIN
+  if (candidate_pass_ms) *candidate_pass_ms = g_knn_last.candidate_ms;
+  if (rows_recomputed) *rows_recomputed = g_knn_last.fallback_rows;
+  if (reordered) *reordered = g_knn_last.reordered;
+  API_END
 }
 
 int umap_knn_bruteforce(const float* data, uint64_t n, uint64_t dim, uint64_t k, uint32_t* knn_indices,

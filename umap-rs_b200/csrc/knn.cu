@@ -78,40 +78,56 @@ __device__ __forceinline__ uint64_t dist_key(float dist, uint32_t idx) {
 
 // ---------------------------------------------------------------------------- K-a
 __global__ void col_sums_kernel(const float* __restrict__ X, int64_t n, int d, double* __restrict__ sums,
+                                unsigned* __restrict__ cmin, unsigned* __restrict__ cmax,
                                 unsigned* __restrict__ bad) {
   __shared__ double part[8][33];
+  __shared__ float lo[8][33], hi[8][33];
   const int col = blockIdx.x * 32 + threadIdx.x;
   double acc = 0.0;
+  float mn = INFINITY, mx = -INFINITY;
   bool finite = true;
   if (col < d)
     for (int64_t r = (int64_t)blockIdx.y * 8 + threadIdx.y; r < n; r += (int64_t)gridDim.y * 8) {
       const float v = X[r * d + col];
       finite &= isfinite(v);
       acc += (double)v;
+      mn = fminf(mn, v);
+      mx = fmaxf(mx, v);
     }
   if (!finite) atomicOr(bad, 1u);
   part[threadIdx.y][threadIdx.x] = acc;
+  lo[threadIdx.y][threadIdx.x] = mn;
+  hi[threadIdx.y][threadIdx.x] = mx;
   __syncthreads();
   if (threadIdx.y == 0 && col < d) {
-    for (int i = 1; i < 8; ++i) acc += part[i][threadIdx.x];
+    for (int i = 1; i < 8; ++i) {
+      acc += part[i][threadIdx.x];
+      mn = fminf(mn, lo[i][threadIdx.x]);
+      mx = fmaxf(mx, hi[i][threadIdx.x]);
+    }
     atomicAdd(sums + col, acc);
+    // order-preserving integer images of the floats for atomicMin / atomicMax
+    const unsigned umn = __float_as_uint(mn), umx = __float_as_uint(mx);
+    atomicMin(cmin + col, (umn & 0x80000000u) ? ~umn : (umn | 0x80000000u));
+    atomicMax(cmax + col, (umx & 0x80000000u) ? ~umx : (umx | 0x80000000u));
   }
 }
 
-__global__ void col_means_kernel(const double* __restrict__ sums, int64_t n, int d, float* __restrict__ mean) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c < d) mean[c] = (float)(sums[c] / (double)n);
+__device__ __forceinline__ float from_ordered(unsigned u) {
+  return __uint_as_float((u & 0x80000000u) ? (u & 0x7FFFFFFFu) : ~u);
 }
 
-// Largest |x - mean| over all elements (bit pattern of a non-negative float, atomicMax).
-__global__ void max_abs_kernel(const float* __restrict__ X, int64_t total, int d, const float* __restrict__ mean,
-                               unsigned* __restrict__ out) {
-  float m = 0.0f;
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x)
-    m = fmaxf(m, fabsf(X[e] - mean[e % d]));
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xFFFFFFFFu, m, o));
-  if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(m));
+// Column means and the largest centred magnitude max_c max(max_c - mean_c, mean_c - min_c)
+// (bit pattern of a non-negative float, atomicMax).
+__global__ void col_means_kernel(const double* __restrict__ sums, const unsigned* __restrict__ cmin,
+                                 const unsigned* __restrict__ cmax, int64_t n, int d, float* __restrict__ mean,
+                                 unsigned* __restrict__ maxabs) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d) return;
+  const float m = (float)(sums[c] / (double)n);
+  mean[c] = m;
+  const float a = fmaxf(fabsf(from_ordered(cmax[c]) - m), fabsf(m - from_ordered(cmin[c])));
+  atomicMax(maxabs, __float_as_uint(a * (1.0f + 1e-6f)));
 }
 
 // One warp per output row r (source row src = perm ? perm[r] : r, rows >= n are padding):
@@ -544,15 +560,17 @@ template <int E>  // candidates per lane = splits * NCAND / 32
 __global__ void __launch_bounds__(256) knn_rerank_kernel(
     const float* __restrict__ X, int64_t n, int d, int dp, int k, const uint32_t* __restrict__ cand_idx,
     const float* __restrict__ tau_in, const float* __restrict__ rn, const unsigned* __restrict__ rmax_bits,
-    float gamma, float scale, uint32_t* __restrict__ out_idx, float* __restrict__ out_d,
-    uint32_t* __restrict__ fail_rows, unsigned* __restrict__ fail_count) {
+    float gamma, float scale, const uint32_t* __restrict__ order, uint32_t* __restrict__ out_idx,
+    float* __restrict__ out_d, uint32_t* __restrict__ fail_rows, unsigned* __restrict__ fail_count) {
   constexpr int S = E * 32 / NCAND;
   __shared__ float tiles[8][33][33];
   const int lane = threadIdx.x & 31;
   float (*tile)[33] = tiles[threadIdx.x >> 5];
   const int64_t w0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t row = w0; row < n; row += nw) {
+  for (int64_t w = w0; w < n; w += nw) {
+    // rows in locality order when there is one: neighbouring warps share candidate rows in L2
+    const int64_t row = order ? (int64_t)order[w] : w;
     uint64_t keys[E];
 #pragma unroll
     for (int e = 0; e < E; ++e) {
@@ -622,10 +640,14 @@ __global__ void __launch_bounds__(EX_THREADS) knn_exact_part_kernel(const float*
       for (int i0 = 0; i0 < d; i0 += 32) {
         __syncthreads();
         // 256 columns x 32 coordinates: warp w loads rows j0 + 32 w' .. as 128-byte pieces
-        for (int q = warp; q < EX_THREADS; q += EX_THREADS / 32) {
-          const int64_t jj = j0 + q;
-          xt[lane][q] = (jj < j_end && i0 + lane < d) ? __ldg(X + jj * d + i0 + lane) : 0.0f;
+        float ld[EX_THREADS / 8];  // all loads of this warp in flight before the stores
+#pragma unroll
+        for (int u = 0; u < EX_THREADS / 8; ++u) {
+          const int64_t jj = j0 + warp + 8 * u;
+          ld[u] = (jj < j_end && i0 + lane < d) ? __ldg(X + jj * d + i0 + lane) : 0.0f;
         }
+#pragma unroll
+        for (int u = 0; u < EX_THREADS / 8; ++u) xt[lane][warp + 8 * u] = ld[u];
         if (tid < 32) xs[tid] = i0 + tid < d ? __ldg(X + row * d + i0 + tid) : 0.0f;
         __syncthreads();
         const int m = min(32, d - i0);
@@ -722,10 +744,10 @@ inline unsigned blocks_for(int64_t n, unsigned bt) { return (unsigned)std::min<i
 
 template <int E>
 void launch_rerank(const float* X, int64_t n, int d, int dp, int k, const uint32_t* ci, const float* tau,
-                   const float* rn, const unsigned* rmax, float gamma, float scale, uint32_t* oi, float* od,
-                   uint32_t* fr, unsigned* fc, cudaStream_t s) {
-  knn_rerank_kernel<E><<<blocks_for(n * 32, 256), 256, 0, s>>>(X, n, d, dp, k, ci, tau, rn, rmax, gamma, scale, oi,
-                                                               od, fr, fc);
+                   const float* rn, const unsigned* rmax, float gamma, float scale, const uint32_t* order,
+                   uint32_t* oi, float* od, uint32_t* fr, unsigned* fc, cudaStream_t s) {
+  knn_rerank_kernel<E><<<blocks_for(n * 32, 256), 256, 0, s>>>(X, n, d, dp, k, ci, tau, rn, rmax, gamma, scale,
+                                                               order, oi, od, fr, fc);
   UB_LAUNCH_CHECK();
 }
 
@@ -766,11 +788,14 @@ KnnStats knn_bruteforce(const float* X, uint64_t n, uint64_t d, uint64_t k, uint
   UB_CUDA(cudaMemsetAsync(flags.p, 0, 20, s));
   {
     const unsigned gy = (unsigned)std::min<int64_t>(1024, std::max<int64_t>(1, (int64_t)n / 256));
-    col_sums_kernel<<<dim3((unsigned)((d + 31) / 32), gy), dim3(32, 8), 0, s>>>(X, (int64_t)n, di, sums.p, flags.p);
+    DevBuf<unsigned> cmm(2 * d, s);
+    UB_CUDA(cudaMemsetAsync(cmm.p, 0xFF, d * 4, s));  // min of ordered images starts at the top
+    UB_CUDA(cudaMemsetAsync(cmm.p + d, 0, d * 4, s));
+    col_sums_kernel<<<dim3((unsigned)((d + 31) / 32), gy), dim3(32, 8), 0, s>>>(X, (int64_t)n, di, sums.p, cmm.p,
+                                                                               cmm.p + d, flags.p);
     UB_LAUNCH_CHECK();
-    col_means_kernel<<<(unsigned)((d + 255) / 256), 256, 0, s>>>(sums.p, (int64_t)n, di, mean.p);
-    UB_LAUNCH_CHECK();
-    max_abs_kernel<<<blocks_for((int64_t)(n * d), 256), 256, 0, s>>>(X, (int64_t)(n * d), di, mean.p, flags.p + 4);
+    col_means_kernel<<<(unsigned)((d + 255) / 256), 256, 0, s>>>(sums.p, cmm.p, cmm.p + d, (int64_t)n, di, mean.p,
+                                                                 flags.p + 4);
     UB_LAUNCH_CHECK();
   }
   unsigned pre[5] = {0, 0, 0, 0, 0};
@@ -827,31 +852,39 @@ KnnStats knn_bruteforce(const float* X, uint64_t n, uint64_t d, uint64_t k, uint
   DevBuf<float> cdist(n * S * NCAND, s), tau(n * S * 2, s);
   const CUtensorMap tq = bf16_tile_map(xh.p, n_pad, dp, dp, QM, true);
   const CUtensorMap tdb = bf16_tile_map(xh.p, n_pad, dp, dp, DBN, true);
+  cudaEvent_t ev[2];
+  UB_CUDA(cudaEventCreate(&ev[0]));
+  UB_CUDA(cudaEventCreate(&ev[1]));
+  UB_CUDA(cudaEventRecord(ev[0], s));
   knn_candidates_kernel<<<dim3((unsigned)q_blocks, (unsigned)S), KNN_THREADS, KNN_SMEM, s>>>(
       tq, tdb, nb.p, (int64_t)n, (int)(dp / KC), tiles, perm.p, cidx.p, cdist.p, tau.p, flags.p + 2);
   UB_LAUNCH_CHECK();
+  UB_CUDA(cudaEventRecord(ev[1], s));
   unsigned kerr = 0;
   UB_CUDA(cudaMemcpyAsync(&kerr, flags.p + 2, 4, cudaMemcpyDeviceToHost, s));
   UB_CUDA(cudaStreamSynchronize(s));
+  (void)cudaEventElapsedTime(&st.candidate_ms, ev[0], ev[1]);
+  (void)cudaEventDestroy(ev[0]);
+  (void)cudaEventDestroy(ev[1]);
   if (kerr) throw Error(CUDA, "kNN candidate pass: a pipeline wait timed out");
 
   DevBuf<uint32_t> fail_rows(n, s);
   const float gamma = (float)(dp + 8) * 9.5367432e-7f;  // (Dp + 8) 2^-20
   const int ki = (int)k, dpi = (int)dp;
   switch (S) {
-    case 1: launch_rerank<2>(X, n, di, dpi, ki, cidx.p, tau.p, rn.p, flags.p + 1, gamma, scale, out_idx, out_dist, fail_rows.p, flags.p + 3, s); break;
-    case 2: launch_rerank<4>(X, n, di, dpi, ki, cidx.p, tau.p, rn.p, flags.p + 1, gamma, scale, out_idx, out_dist, fail_rows.p, flags.p + 3, s); break;
-    case 4: launch_rerank<8>(X, n, di, dpi, ki, cidx.p, tau.p, rn.p, flags.p + 1, gamma, scale, out_idx, out_dist, fail_rows.p, flags.p + 3, s); break;
-    default: launch_rerank<16>(X, n, di, dpi, ki, cidx.p, tau.p, rn.p, flags.p + 1, gamma, scale, out_idx, out_dist, fail_rows.p, flags.p + 3, s); break;
+    case 1: launch_rerank<2>(X, n, di, dpi, ki, cidx.p, tau.p, rn.p, flags.p + 1, gamma, scale, perm.p, out_idx, out_dist, fail_rows.p, flags.p + 3, s); break;
+    case 2: launch_rerank<4>(X, n, di, dpi, ki, cidx.p, tau.p, rn.p, flags.p + 1, gamma, scale, perm.p, out_idx, out_dist, fail_rows.p, flags.p + 3, s); break;
+    case 4: launch_rerank<8>(X, n, di, dpi, ki, cidx.p, tau.p, rn.p, flags.p + 1, gamma, scale, perm.p, out_idx, out_dist, fail_rows.p, flags.p + 3, s); break;
+    default: launch_rerank<16>(X, n, di, dpi, ki, cidx.p, tau.p, rn.p, flags.p + 1, gamma, scale, perm.p, out_idx, out_dist, fail_rows.p, flags.p + 3, s); break;
   }
   unsigned n_fail = 0;
   UB_CUDA(cudaMemcpyAsync(&n_fail, flags.p + 3, 4, cudaMemcpyDeviceToHost, s));
   UB_CUDA(cudaStreamSynchronize(s));
   st.fallback_rows = n_fail;
   if (n_fail) {
-    // enough CTAs to fill the GPU: split each row's columns into ranges of >= 4096
+    // enough CTAs to fill the GPU: split each row's columns into ranges of >= 1024
     const int64_t want = std::max<int64_t>(1, (4 * 148 + (int64_t)n_fail - 1) / (int64_t)n_fail);
-    const int ranges = (int)std::max<int64_t>(1, std::min<int64_t>({want, (int64_t)n / 4096 + 1, 256}));
+    const int ranges = (int)std::max<int64_t>(1, std::min<int64_t>({want, (int64_t)n / 1024 + 1, 256}));
     const unsigned gx = std::min<unsigned>(n_fail, 65535u);
     DevBuf<uint64_t> part((uint64_t)n_fail * ranges * k, s);
     knn_exact_part_kernel<<<dim3(gx, (unsigned)ranges), EX_THREADS, (size_t)k * EX_THREADS * 8, s>>>(

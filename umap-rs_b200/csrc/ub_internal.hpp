@@ -295,6 +295,7 @@ struct KnnStats {
   uint32_t fallback_rows = 0;  // rows whose certificate failed and were recomputed exactly
   float scale = 1.0f;          // power of two applied to the centred rows before FP16 rounding
   uint32_t reordered = 0;      // 1 when the scan ran in pivot (locality) order
+  float candidate_ms = 0.0f;   // CUDA-event time of the tensor-core candidate pass
 };
 KnnStats knn_bruteforce(const float* X, uint64_t n, uint64_t d, uint64_t k, uint32_t* out_idx, float* out_dist,
                         cudaStream_t s);

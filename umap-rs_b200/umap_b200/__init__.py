@@ -30,7 +30,7 @@ from . import _lib
 __all__ = [
     "ManifoldParams", "GraphParams", "OptimizationParams", "UmapConfig", "MetricType",
     "EuclideanMetric", "GenericEuclideanMetric", "Metric", "OUTPUT_METRIC_EUCLIDEAN", "Umap", "LearnedManifold", "Optimizer", "FittedUmap",
-    "SparseMat", "UmapError", "find_ab_params", "lib", "knn_bruteforce", "KNN_MAX_K",
+    "SparseMat", "UmapError", "find_ab_params", "lib", "knn_bruteforce", "knn_last_profile", "KNN_MAX_K",
 ]
 
 lib = _lib.load
@@ -246,6 +246,14 @@ def knn_bruteforce(data, k: int, return_stats: bool = False):
         _check(L.umap_knn_bruteforce(p, n, dim, k, idx.ctypes.data_as(C.c_void_p) if n else C.c_void_p(1),
                                      dist.ctypes.data_as(C.c_void_p) if n else C.c_void_p(1), C.byref(rec)))
     return (idx, dist, rec.value) if return_stats else (idx, dist)
+
+
+def knn_last_profile():
+    """(candidate-pass ms, rows recomputed, scanned in locality order) of this thread's last
+    knn_bruteforce call."""
+    ms, rec, ro = C.c_float(), C.c_uint64(), C.c_uint32()
+    _check(_lib.load().umap_knn_last_profile(C.byref(ms), C.byref(rec), C.byref(ro)))
+    return ms.value, rec.value, bool(ro.value)
 
 
 def release_cached_memory() -> int:

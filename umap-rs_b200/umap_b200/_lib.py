@@ -91,6 +91,7 @@ SIGNATURES = {
     "umap_smooth_knn_dist_device": [P, u64, u64, u64, f32, f32, P, P],
     "umap_knn_bruteforce": [P, u64, u64, u64, P, P, C.POINTER(u64)],
     "umap_knn_bruteforce_device": [P, u64, u64, u64, P, P, C.POINTER(u64)],
+    "umap_knn_last_profile": [C.POINTER(f32), C.POINTER(u64), C.POINTER(u32)],
     "umap_radix_sort_pairs_device": [P, P, P, P, u64, i32],
     "umap_radix_sort_pairs_device_noalloc": [P, P, P, P, u64, i32, P],
     "umap_radix_sort_noalloc_max_pairs": [C.POINTER(u64)],

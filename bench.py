@@ -2,7 +2,8 @@
 
 Workload (default): n=2,000,000 points, D=64, 50 anisotropic Gaussians (centres ~N(0,8^2 I),
 per-cluster diagonal std ~U[0.5,2], Dirichlet(1) weights), seed 1; exact kNN k=15 (self
-first); init U[-10,10]^2; 500 epochs; min_dist 0.1, spread 1, local_connectivity 1,
+first, from the library's tensor-core brute force); init U[-10,10]^2; 500 epochs; min_dist
+0.1, spread 1, local_connectivity 1,
 set_op_mix_ratio 1, symmetrize, negative_sample_rate 5.  Synthetic data of that shape.
 
 One step = one complete fit (Umap::learn_manifold -> Optimizer::new -> step_epochs(500) ->
@@ -132,10 +133,11 @@ def make_workload(n, seed_note=True):
     else:
         X, lab = W.gaussian_mixture(n, 64, 50, 8.0, seed=1, anisotropic=True, dirichlet=True)
     t = time.time()
-    idx, dist, redo = W.knn_exact_clustered_torch(X, lab, 15)
+    idx, dist, redo = W.knn_exact_gpu(X, 15)
     knn_s = time.time() - t
     init = W.uniform_init(n)
-    return idx, dist, init, {"knn_seconds": round(knn_s, 1), "knn_rows_recomputed": redo}
+    return idx, dist, init, {"knn": "exact, self first (umap_knn_bruteforce)", "knn_seconds": round(knn_s, 2),
+                             "knn_rows_recomputed": redo}
 
 
 def dist_info():
@@ -276,13 +278,13 @@ def run_warm_start(a):
     n = a.n
     X, lab = W.gaussians_2m() if n == 2_000_000 else W.gaussian_mixture(n, 64, 50, 8.0, seed=1, anisotropic=True,
                                                                          dirichlet=True)
-    idx, dist, _ = W.knn_exact_clustered_torch(X, lab, 15)
+    idx, dist, _ = W.knn_exact_gpu(X, 15)
     init = W.uniform_init(n)
     n_sub = min(a.sub, n)
     sub = np.sort(np.random.Generator(np.random.PCG64(3)).choice(n, n_sub, replace=False))
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    sidx, sdist, _ = W.knn_exact_clustered_torch(X[sub], lab[sub], 15)
+    sidx, sdist, _ = W.knn_exact_gpu(X[sub], 15)
     torch.cuda.synchronize()
     sub_knn_ms = (time.perf_counter() - t0) * 1e3
     x = torch.from_numpy(X).cuda()
@@ -330,7 +332,7 @@ def run_warm_start(a):
             if name == "plain":
                 ab = f.manifold().curve_params()
                 edges = quality.pruned_edges(f.manifold(), a.epochs)
-            res[name] = {"ms": float(np.median(ms))}
+            res[name] = {"ms": float(np.median(ms)), "all_ms": [round(v, 1) for v in ms]}
             del f
     launches = ub.kernel_launches() - launches0
     for name, emb in embs.items():
@@ -357,6 +359,7 @@ def run_warm_start(a):
             "random_short_ce": res["random_short"]["ce"],
             "ce_scored_on": f"{len(edges[0])} edges of the plain fit's {a.epochs}-epoch pruned graph + 5x random pairs",
             "time_ratio_warm_over_plain": res["warm"]["ms"] / res["plain"]["ms"],
+            "step_ms": {k: v["all_ms"] for k, v in res.items()},
             "recall_gap_plain_minus_warm": res["plain"]["recall"] - res["warm"]["recall"],
             "warm_phase_ms": info["ms"], "mlp_losses": [info["mlp_losses"][0], info["mlp_losses"][-1]],
             "mlp": {"train_steps": 20 * steps_per_epoch, "train_tflops": train_tflops,

@@ -209,6 +209,23 @@ def knn_exact_torch(X: np.ndarray, k: int, device="cuda", margin: int = 8, chunk
     return idx.to(torch.int32).cpu().numpy().astype(np.uint32), dst.cpu().numpy(), len(bad_rows)
 
 
+def knn_exact_gpu(X: np.ndarray, k: int, device="cuda"):
+    """Exact kNN with the point itself first (self + k - 1 others), the others from the
+    library's tensor-core brute force (umap_knn_bruteforce: the reference example's f32
+    distance, ties in index order).  Returns (idx u32[n,k], dist f32[n,k], rows recomputed)."""
+    import torch
+    import umap_b200 as ub
+    n = X.shape[0]
+    t = torch.from_numpy(np.ascontiguousarray(X, dtype=np.float32)).to(device)
+    i, d, rec = ub.knn_bruteforce(t, k - 1, return_stats=True)
+    idx = np.empty((n, k), np.uint32)
+    dist = np.zeros((n, k), np.float32)
+    idx[:, 0] = np.arange(n, dtype=np.uint32)
+    idx[:, 1:] = i.cpu().numpy().view(np.uint32)
+    dist[:, 1:] = d.cpu().numpy()
+    return idx, dist, rec
+
+
 def _torch_knn_block(torch, Xq0, Xq, Xc0, Xc, sqq, sqc, k, kc, self_offset):
     """Top-(k) exact neighbours of query rows among candidate rows (both on the GPU).
     X*0 are the original coordinates (exact distances), X* the centred copies (search)."""

@@ -139,3 +139,25 @@ def test_batch_validation_names_the_instance(ub):
     init = np.zeros((110, 2), np.float32)
     with pytest.raises(ub.UmapError, match=r"^instance 1: Number of samples \(10\) must be > n_neighbors \(15\)$"):
         ub.Optimizer.batch(ub.UmapConfig(), off, idx, dist, init, 10)
+
+
+def test_rust_ffi_is_generated_from_the_header():
+    """include/umap_b200_ffi.rs (the Rust crate's extern "C" block) is current with the header:
+    regenerating it changes nothing, every header entry point has a declaration, and the
+    config struct lists the header's fields in order (the ctypes mirror's order too)."""
+    import importlib.util
+    import os
+    import re
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    spec = importlib.util.spec_from_file_location("gen_rust_ffi", os.path.join(root, "include", "gen_rust_ffi.py"))
+    gen = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(gen)
+    header = open(os.path.join(root, "include", "umap_b200.h")).read()
+    committed = open(os.path.join(root, "include", "umap_b200_ffi.rs")).read()
+    assert gen.render(header) == committed
+    decl = set(re.findall(r"^(?:int|const char\s*\*)\s*(umap_\w+)\s*\(", gen._strip_comments(header), re.M))
+    rust = set(re.findall(r"pub fn (umap_\w+)\(", committed))
+    assert decl == rust and len(rust) > 60
+    from umap_b200._lib import UmapConfigC
+    fields = re.findall(r"^    pub (\w+): ", committed.split("pub struct umap_config {")[1].split("}")[0], re.M)
+    assert fields == [f[0] for f in UmapConfigC._fields_]

@@ -250,7 +250,7 @@ __device__ __forceinline__ void tmem_wait32(uint32_t (&r)[32]) {
 __global__ void __launch_bounds__(KNN_THREADS, 1) knn_candidates_kernel(
     const __grid_constant__ CUtensorMap tq, const __grid_constant__ CUtensorMap tdb, const float* __restrict__ nb,
     int64_t n, int n_kchunks, int64_t tiles_total, const uint32_t* __restrict__ perm, uint32_t* __restrict__ cand_idx,
-    float* __restrict__ cand_d, float* __restrict__ tau_out, unsigned* __restrict__ err) {
+    float* __restrict__ tau_out, unsigned* __restrict__ err) {
   extern __shared__ uint8_t smem_raw[];
   __shared__ __align__(8) uint64_t full[TS], empty[TS], tfull[2], tempty[2], nfull[NBS], nempty[NBS];
   __shared__ uint32_t tmem_base;
@@ -500,7 +500,6 @@ __global__ void __launch_bounds__(KNN_THREADS, 1) knn_candidates_kernel(
       for (int s = 0; s < HC; ++s) {
         const uint32_t c = hi[s * QM + trow];
         cand_idx[base + s] = (perm && c < (uint64_t)n) ? perm[c] : c;
-        cand_d[base + s] = hd[s * QM + trow];
       }
       tau_out[(orow * n_splits + split) * 2 + half] = tau;
     }
@@ -849,7 +848,7 @@ KnnStats knn_bruteforce(const float* X, uint64_t n, uint64_t d, uint64_t k, uint
   }
 
   DevBuf<uint32_t> cidx(n * S * NCAND, s);
-  DevBuf<float> cdist(n * S * NCAND, s), tau(n * S * 2, s);
+  DevBuf<float> tau(n * S * 2, s);
   const CUtensorMap tq = bf16_tile_map(xh.p, n_pad, dp, dp, QM, true);
   const CUtensorMap tdb = bf16_tile_map(xh.p, n_pad, dp, dp, DBN, true);
   cudaEvent_t ev[2];
@@ -857,7 +856,7 @@ KnnStats knn_bruteforce(const float* X, uint64_t n, uint64_t d, uint64_t k, uint
   UB_CUDA(cudaEventCreate(&ev[1]));
   UB_CUDA(cudaEventRecord(ev[0], s));
   knn_candidates_kernel<<<dim3((unsigned)q_blocks, (unsigned)S), KNN_THREADS, KNN_SMEM, s>>>(
-      tq, tdb, nb.p, (int64_t)n, (int)(dp / KC), tiles, perm.p, cidx.p, cdist.p, tau.p, flags.p + 2);
+      tq, tdb, nb.p, (int64_t)n, (int)(dp / KC), tiles, perm.p, cidx.p, tau.p, flags.p + 2);
   UB_LAUNCH_CHECK();
   UB_CUDA(cudaEventRecord(ev[1], s));
   unsigned kerr = 0;

@@ -219,9 +219,10 @@ int umap_fit_manifold_metric_device(umap_manifold* manifold, const umap_config* 
  * (examples/src/bin/mnist_demo.rs:203-229): for each row of data [n, dim] (row-major f32) the
  * k other rows with the smallest sqrt(sum_i (x_i - y_i)^2) (f32, summed in coordinate order),
  * ordered by distance then index, the row itself excluded; with fewer than k other rows the
- * remaining slots are 0 / 0.0.  Outputs [n, k] row-major.  1 <= k <= 32.  Candidates come
- * from a BF16 tensor-core distance pass; every row is then either certified exact against an
- * error bound or recomputed exactly, so the result equals the f32 brute force.
+ * remaining slots are 0 / 0.0.  Outputs [n, k] row-major.  1 <= k <= 128.  For k <= 32
+ * candidates come from an FP16 tensor-core distance pass; every row is then either certified
+ * exact against an error bound or recomputed exactly, so the result equals the f32 brute
+ * force.  For 32 < k <= 128 every row is computed exactly on the CUDA cores (slower).
  * `rows_recomputed` (nullable) receives the number of rows that needed the exact recompute.
  * UMAP_ERR_INVALID_ARGUMENT for NaN or infinite inputs (the reference's sort panics). */
 int umap_knn_bruteforce(const float* host_data, uint64_t n, uint64_t dim, uint64_t k,

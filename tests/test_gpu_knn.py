@@ -45,6 +45,18 @@ def test_knn_matches_oracle(ub, oracle, n, d, k, kind):
     print(f"n={n} d={d} k={k} {kind}: rows recomputed {rec}")
 
 
+@pytest.mark.parametrize("n,d,k,kind", [(700, 16, 33, "gauss"), (1500, 40, 100, "clusters"),
+                                         (400, 8, 128, "ties"), (60, 5, 100, "gauss")])
+def test_knn_long_lists_exact_path(ub, oracle, n, d, k, kind):
+    """k above the candidate pass's 32: every row on the exact CUDA-core path, still equal to
+    the reference example's brute force (including zero padding when n - 1 < k)."""
+    X = _data(n, d, seed=n + k, kind=kind)
+    gi, gd, rec = ub.knn_bruteforce(X, k, return_stats=True)
+    oi, od = oracle.knn_bruteforce(X, k)
+    assert rec == n
+    assert np.array_equal(gi, oi) and np.array_equal(gd, od)
+
+
 def test_knn_device_matches_host_and_uses_fallback_only_when_needed(ub, oracle):
     import torch
     X = _data(4096, 48, seed=3, kind="gauss")

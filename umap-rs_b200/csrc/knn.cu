@@ -38,7 +38,8 @@
 //       point can enter the top k.
 //  K-d  rows whose certificate fails are recomputed exactly against all points: CTAs over
 //       (row, column range) keep the k smallest keys of their range, then a warp per row
-//       merges the ranges.
+//       merges the ranges.  For k > 32 (more than the candidate pass keeps) every row takes
+//       this path.
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
@@ -616,11 +617,12 @@ __global__ void __launch_bounds__(256) knn_rerank_kernel(
 // (coalesced), each thread sums its column's squared differences in coordinate order and
 // keeps its k smallest (distance, index) keys; k rounds of a block-wide minimum leave the
 // range's k smallest keys in part[b][s][0..k).
-constexpr int EX_THREADS = 256;
-__global__ void __launch_bounds__(EX_THREADS) knn_exact_part_kernel(const float* __restrict__ X, int64_t n, int d,
-                                                                    int k, const uint32_t* __restrict__ rows,
-                                                                    unsigned n_rows, int n_ranges,
-                                                                    uint64_t* __restrict__ part) {
+// TH threads per CTA: 256 for k <= 32, 128 for the longer lists of k <= 128.
+template <int TH>
+__global__ void __launch_bounds__(TH) knn_exact_part_kernel(const float* __restrict__ X, int64_t n, int d, int k,
+                                                            const uint32_t* __restrict__ rows, unsigned n_rows,
+                                                            int n_ranges, uint64_t* __restrict__ part) {
+  constexpr int EX_THREADS = TH, NW = TH / 32;
   extern __shared__ uint64_t lst[];  // [k][EX_THREADS]
   __shared__ float xt[32][EX_THREADS + 1];
   __shared__ float xs[32];
@@ -639,14 +641,14 @@ __global__ void __launch_bounds__(EX_THREADS) knn_exact_part_kernel(const float*
       for (int i0 = 0; i0 < d; i0 += 32) {
         __syncthreads();
         // 256 columns x 32 coordinates: warp w loads rows j0 + 32 w' .. as 128-byte pieces
-        float ld[EX_THREADS / 8];  // all loads of this warp in flight before the stores
+        float ld[32];  // this warp's 32 rows: all loads in flight before the stores
 #pragma unroll
-        for (int u = 0; u < EX_THREADS / 8; ++u) {
-          const int64_t jj = j0 + warp + 8 * u;
+        for (int u = 0; u < 32; ++u) {
+          const int64_t jj = j0 + warp + NW * u;
           ld[u] = (jj < j_end && i0 + lane < d) ? __ldg(X + jj * d + i0 + lane) : 0.0f;
         }
 #pragma unroll
-        for (int u = 0; u < EX_THREADS / 8; ++u) xt[lane][warp + 8 * u] = ld[u];
+        for (int u = 0; u < 32; ++u) xt[lane][warp + NW * u] = ld[u];
         if (tid < 32) xs[tid] = i0 + tid < d ? __ldg(X + row * d + i0 + tid) : 0.0f;
         __syncthreads();
         const int m = min(32, d - i0);
@@ -741,6 +743,32 @@ __global__ void knn_exact_merge_kernel(const uint64_t* __restrict__ part, const 
 
 inline unsigned blocks_for(int64_t n, unsigned bt) { return (unsigned)std::min<int64_t>((n + bt - 1) / bt, 1 << 20); }
 
+__global__ void iota_kernel(uint32_t* __restrict__ v, int64_t n) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) v[i] = (uint32_t)i;
+}
+
+// K-d for the listed rows: enough CTAs to fill the GPU (each row's columns split into ranges
+// of >= 1024), then the merge.  Synchronises `s`.
+void exact_rows(const float* X, int64_t n, int d, int k, const uint32_t* rows, unsigned n_rows, uint32_t* out_idx,
+                float* out_dist, cudaStream_t s) {
+  const int64_t want = std::max<int64_t>(1, (4 * 148 + (int64_t)n_rows - 1) / (int64_t)n_rows);
+  const int ranges = (int)std::max<int64_t>(1, std::min<int64_t>({want, n / 1024 + 1, 256}));
+  const unsigned gx = std::min<unsigned>(n_rows, 65535u);
+  DevBuf<uint64_t> part((uint64_t)n_rows * ranges * k, s);
+  if (k <= KNN_MAX_K)
+    knn_exact_part_kernel<256><<<dim3(gx, (unsigned)ranges), 256, (size_t)k * 256 * 8, s>>>(X, n, d, k, rows, n_rows,
+                                                                                            ranges, part.p);
+  else
+    knn_exact_part_kernel<128><<<dim3(gx, (unsigned)ranges), 128, (size_t)k * 128 * 8, s>>>(X, n, d, k, rows, n_rows,
+                                                                                            ranges, part.p);
+  UB_LAUNCH_CHECK();
+  knn_exact_merge_kernel<<<blocks_for((int64_t)n_rows * 32, 256), 256, 0, s>>>(part.p, rows, n_rows, ranges, k,
+                                                                               out_idx, out_dist);
+  UB_LAUNCH_CHECK();
+  UB_CUDA(cudaStreamSynchronize(s));
+}
+
 template <int E>
 void launch_rerank(const float* X, int64_t n, int d, int dp, int k, const uint32_t* ci, const float* tau,
                    const float* rn, const unsigned* rmax, float gamma, float scale, const uint32_t* order,
@@ -755,8 +783,8 @@ void launch_rerank(const float* X, int64_t n, int d, int dp, int k, const uint32
 KnnStats knn_bruteforce(const float* X, uint64_t n, uint64_t d, uint64_t k, uint32_t* out_idx, float* out_dist,
                         cudaStream_t s) {
   KnnStats st{};
-  if (k < 1 || k > (uint64_t)KNN_MAX_K)
-    throw Error(INVALID_ARGUMENT, "k must be in 1.." + std::to_string(KNN_MAX_K) + ", got " + std::to_string(k));
+  if (k < 1 || k > (uint64_t)KNN_MAX_K_EXACT)
+    throw Error(INVALID_ARGUMENT, "k must be in 1.." + std::to_string(KNN_MAX_K_EXACT) + ", got " + std::to_string(k));
   if (d < 1 || d > 65536) throw Error(INVALID_ARGUMENT, "dimension must be in 1..65536");
   if (n >= 0x7FFFFF00ull) throw Error(UNSUPPORTED, "n must be < 2^31 - 256");
   if (n == 0) return st;
@@ -769,8 +797,10 @@ KnnStats knn_bruteforce(const float* X, uint64_t n, uint64_t d, uint64_t k, uint
   static std::once_flag once;
   std::call_once(once, [] {
     UB_CUDA(cudaFuncSetAttribute(knn_candidates_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)KNN_SMEM));
-    UB_CUDA(cudaFuncSetAttribute(knn_exact_part_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)(KNN_MAX_K * EX_THREADS * 8)));
+    UB_CUDA(cudaFuncSetAttribute(knn_exact_part_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(KNN_MAX_K * 256 * 8)));
+    UB_CUDA(cudaFuncSetAttribute(knn_exact_part_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(KNN_MAX_K_EXACT * 128 * 8)));
   });
   const int di = (int)d;
   const int64_t dp = (int64_t)((d + KC - 1) / KC) * KC;
@@ -801,6 +831,16 @@ KnnStats knn_bruteforce(const float* X, uint64_t n, uint64_t d, uint64_t k, uint
   UB_CUDA(cudaMemcpyAsync(pre, flags.p, 20, cudaMemcpyDeviceToHost, s));
   UB_CUDA(cudaStreamSynchronize(s));
   if (pre[0]) throw Error(INVALID_ARGUMENT, "kNN input contains NaN or infinite values");
+  if (k > (uint64_t)KNN_MAX_K) {
+    // lists longer than the candidate pass keeps: every row on the exact CUDA-core path
+    DevBuf<uint32_t> all(n, s);
+    iota_kernel<<<blocks_for((int64_t)n, 256), 256, 0, s>>>(all.p, (int64_t)n);
+    UB_LAUNCH_CHECK();
+    exact_rows(X, (int64_t)n, (int)d, (int)k, all.p, (unsigned)n, out_idx, out_dist, s);
+    st.fallback_rows = (uint32_t)n;
+    st.all_exact = 1;
+    return st;
+  }
   // scale = 2^e with max |x~| * scale <= 2^14, so every scaled value is finite in FP16
   float maxabs;
   std::memcpy(&maxabs, &pre[4], 4);
@@ -880,20 +920,7 @@ KnnStats knn_bruteforce(const float* X, uint64_t n, uint64_t d, uint64_t k, uint
   UB_CUDA(cudaMemcpyAsync(&n_fail, flags.p + 3, 4, cudaMemcpyDeviceToHost, s));
   UB_CUDA(cudaStreamSynchronize(s));
   st.fallback_rows = n_fail;
-  if (n_fail) {
-    // enough CTAs to fill the GPU: split each row's columns into ranges of >= 1024
-    const int64_t want = std::max<int64_t>(1, (4 * 148 + (int64_t)n_fail - 1) / (int64_t)n_fail);
-    const int ranges = (int)std::max<int64_t>(1, std::min<int64_t>({want, (int64_t)n / 1024 + 1, 256}));
-    const unsigned gx = std::min<unsigned>(n_fail, 65535u);
-    DevBuf<uint64_t> part((uint64_t)n_fail * ranges * k, s);
-    knn_exact_part_kernel<<<dim3(gx, (unsigned)ranges), EX_THREADS, (size_t)k * EX_THREADS * 8, s>>>(
-        X, (int64_t)n, di, ki, fail_rows.p, n_fail, ranges, part.p);
-    UB_LAUNCH_CHECK();
-    knn_exact_merge_kernel<<<blocks_for((int64_t)n_fail * 32, 256), 256, 0, s>>>(part.p, fail_rows.p, n_fail, ranges,
-                                                                                 ki, out_idx, out_dist);
-    UB_LAUNCH_CHECK();
-    UB_CUDA(cudaStreamSynchronize(s));
-  }
+  if (n_fail) exact_rows(X, (int64_t)n, di, ki, fail_rows.p, n_fail, out_idx, out_dist, s);
   return st;
 }
 

@@ -289,13 +289,15 @@ void umma_gemm_f32(const void* A, const void* B, float* C, int64_t M, int64_t N,
 // Exact brute-force kNN (knn.cu): for each of the n rows of X [n, d] (f32, device), the k
 // nearest other rows by the reference example's f32 Euclidean distance, ordered by (distance,
 // index); out_idx / out_dist [n, k] on the device.  Synchronises `s`.
-constexpr int KNN_MAX_K = 32;
+constexpr int KNN_MAX_K = 32;         // through the tensor-core candidate pass
+constexpr int KNN_MAX_K_EXACT = 128;  // every row on the exact CUDA-core path
 struct KnnStats {
   uint32_t splits = 0;         // database splits of the candidate pass
   uint32_t fallback_rows = 0;  // rows whose certificate failed and were recomputed exactly
   float scale = 1.0f;          // power of two applied to the centred rows before FP16 rounding
   uint32_t reordered = 0;      // 1 when the scan ran in pivot (locality) order
   float candidate_ms = 0.0f;   // CUDA-event time of the tensor-core candidate pass
+  uint32_t all_exact = 0;      // 1 when k > KNN_MAX_K sent every row to the exact path
 };
 KnnStats knn_bruteforce(const float* X, uint64_t n, uint64_t d, uint64_t k, uint32_t* out_idx, float* out_dist,
                         cudaStream_t s);

@@ -30,7 +30,7 @@ from . import _lib
 __all__ = [
     "ManifoldParams", "GraphParams", "OptimizationParams", "UmapConfig", "MetricType",
     "EuclideanMetric", "GenericEuclideanMetric", "Metric", "OUTPUT_METRIC_EUCLIDEAN", "Umap", "LearnedManifold", "Optimizer", "FittedUmap",
-    "SparseMat", "UmapError", "find_ab_params", "lib", "knn_bruteforce", "knn_last_profile", "KNN_MAX_K",
+    "SparseMat", "UmapError", "find_ab_params", "lib", "knn_bruteforce", "knn_last_profile", "KNN_MAX_K", "KNN_MAX_K_TENSOR",
 ]
 
 lib = _lib.load
@@ -219,7 +219,8 @@ def batch_fit(config: UmapConfig, offsets, knn_indices, knn_dists, init):
     return out
 
 
-KNN_MAX_K = 32
+KNN_MAX_K = 128       # largest k; above 32 every row takes the exact CUDA-core path
+KNN_MAX_K_TENSOR = 32  # largest k through the tensor-core candidate pass
 
 
 def knn_bruteforce(data, k: int, return_stats: bool = False):

@@ -71,6 +71,16 @@ def peaks():
         return {}
 
 
+# Earlier measurements on this pool's B200s, used when MEASURED_PEAKS.json is absent.
+FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}
+
+
+def peak(key):
+    """(value, "measured" | "fallback") of a roofline denominator."""
+    v = peaks().get(key)
+    return (float(v), "measured") if v else (FALLBACK_PEAKS[key], "fallback")
+
+
 def traffic_per_epoch():
     """DRAM bytes per SGD launch from the committed ncu summary (None if absent)."""
     p = os.path.join(ROOT, "profiles", "sgd_epoch_2m.md")
@@ -350,8 +360,7 @@ def run_warm_start(a):
     train_ms = info["ms"]["mlp_train"]
     train_tflops = flop_step * 20 * steps_per_epoch / (train_ms / 1e3) / 1e12
     pred_tflops = 2 * n * (64 * 256 + 256 * 256 + 256 * 2) / (info["ms"]["mlp_predict"] / 1e3) / 1e12
-    pk = peaks()
-    tc = pk.get("bf16_tflops")
+    tc, tc_src = peak("bf16_tflops")
     line = {"metric": "warm-start fit wall time at equal 15-NN recall", "value": res["warm"]["ms"], "unit": "ms",
             "higher_is_better": False, "n_gpus": 1, "steps": a.steps, "warmup": a.warmup, "dtype": "bf16+f32",
             "data": "synthetic",
@@ -369,7 +378,7 @@ def run_warm_start(a):
             "recall_gap_plain_minus_warm": res["plain"]["recall"] - res["warm"]["recall"],
             "warm_phase_ms": info["ms"], "mlp_losses": [info["mlp_losses"][0], info["mlp_losses"][-1]],
             "mlp": {"train_steps": 20 * steps_per_epoch, "train_tflops": train_tflops,
-                    "predict_tflops": pred_tflops, "bf16_peak_tflops": tc,
+                    "predict_tflops": pred_tflops, "bf16_peak_tflops": tc, "peak_source": tc_src,
                     "train_frac": train_tflops / tc if tc else None,
                     "predict_frac": pred_tflops / tc if tc else None},
             "gpu_launches": launches, "clocks": clk.summary()}
@@ -463,8 +472,7 @@ def run_swiss_roll(a):
     F_tot, N_tot = stats["FN"]
     sgd_ms = float(np.median(sgd))
     alg = 4.0 * E * a.swiss_epochs + 40.0 * F_tot + 8.0 * N_tot
-    pk = peaks()
-    hbm = pk.get("hbm_gbs") or 6650.0
+    hbm, hbm_src = peak("hbm_gbs")
     achieved = alg / (sgd_ms / 1e3) / 1e9
     # spot check: sampled rows' rho (bit-exact) and sigma (1e-5 relative) against the oracle
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -493,7 +501,7 @@ def run_swiss_roll(a):
             "sgd_ms_per_fit": sgd_ms, "sgd_edge_updates_per_s": F_tot / (sgd_ms / 1e3),
             "graph_and_setup_ms": ms_step - sgd_ms,
             "roofline": {"bound": "hbm", "kernel": "sgd_epoch_kernel2<2>", "achieved": achieved, "peak": hbm,
-                         "unit": "GB/s", "frac": achieved / hbm, "traffic": swiss_traffic(E),
+                         "unit": "GB/s", "frac": achieved / hbm, "peak_source": hbm_src, "traffic": swiss_traffic(E),
                          "traffic_note": "DRAM bytes of one epoch-20 launch captured at 20M points "
                                          "(profiles/sgd_epoch_swiss_roll_20m.md), scaled by kept edges",
                          "algorithmic_bytes_per_launch": alg / a.swiss_epochs,
@@ -550,7 +558,7 @@ def run_mlp(a):
     flop_step = 2 * 4096 * (64 * 256 + 256 * 256 + 256 * 2) * 3 - 2 * 4096 * 64 * 256
     tflops = flop_step * steps / (train_ms / 1e3) / 1e12
     pflops = 2 * 2_000_000 * (64 * 256 + 256 * 256 + 256 * 2) / (pred_ms / 1e3) / 1e12
-    pk = peaks().get("bf16_tflops")
+    pk, pk_src = peak("bf16_tflops")
     print(json.dumps({"metric": "MLP training step time", "value": train_ms / steps * 1e3, "unit": "us/step",
                       "higher_is_better": False, "n_gpus": 1, "steps": a.steps, "warmup": a.warmup,
                       "dtype": "bf16", "data": "synthetic",
@@ -558,7 +566,7 @@ def run_mlp(a):
                                              "predict 2000000 rows"},
                       "train_ms": train_ms, "predict_ms": pred_ms,
                       "roofline": {"bound": "tensor", "achieved": tflops, "peak": pk, "unit": "TFLOP/s",
-                                   "frac": tflops / pk if pk else None, "traffic": None},
+                                   "frac": tflops / pk, "peak_source": pk_src, "traffic": None},
                       "predict_tflops": pflops,
                       "gpu_launches": ub.kernel_launches() - launches0, "clocks": clk.summary()}), flush=True)
 
@@ -616,7 +624,7 @@ def run_knn(a):
     flops = 2.0 * n * n * d
     cms = float(np.mean(cand_ms))
     achieved = flops / (cms / 1e3) / 1e12
-    pk = peaks().get("bf16_tflops")
+    pk, pk_src = peak("bf16_tflops")
     traffic = None
     try:
         for line in open(os.path.join(ROOT, "profiles", "knn_candidates_digits70k.md")):
@@ -648,7 +656,7 @@ def run_knn(a):
         "e2e": {"value": n / e2e_s, "unit": "rows/s", "ms_per_step": e2e_s * 1e3,
                 "h2d_bytes_per_step": int(X.nbytes), "d2h_bytes_per_step": int(n * k * 8)},
         "roofline": {"bound": "tensor", "kernel": "knn_candidates_kernel", "achieved": achieved, "peak": pk,
-                     "unit": "TFLOP/s", "frac": achieved / pk if pk else None, "peak_source": "measured",
+                     "unit": "TFLOP/s", "frac": achieved / pk, "peak_source": pk_src,
                      "traffic": traffic, "algorithmic_flops_per_launch": flops, "avg_launch_ms": cms},
         "gpu_launches": launches, "clocks": clk.summary(), "cpu_baseline": cpu}), flush=True)
 
@@ -758,10 +766,7 @@ def main():
     h2d = idx.nbytes + dist.nbytes + init.nbytes
     d2h = n * 2 * 4
 
-    pk = peaks()
-    hbm = pk.get("hbm_gbs")
-    peak_src = "measured" if hbm else "fallback"
-    hbm = hbm or 6650.0
+    hbm, peak_src = peak("hbm_gbs")
     sgd_kernel_ms = float(np.median(sgd_ms)) / a.epochs
     achieved = alg_bytes / a.epochs / (sgd_kernel_ms / 1e3) / 1e9
     tr = traffic_per_epoch()

@@ -85,7 +85,7 @@ def test_input_norm_applied_in_gradients(ub, torch):
     assert _rel(g, go) <= 1e-2
 
 
-@pytest.mark.parametrize("n", [128, 1000, 131072 + 77])
+@pytest.mark.parametrize("n", [128, 1000, 9000, 131072 + 77])
 def test_predict_matches_oracle_forward(ub, torch, n):
     rng = np.random.default_rng(n)
     X = rng.normal(0, 1, (n, 64)).astype(np.float32)

@@ -806,7 +806,9 @@ void prepare_all_gemms() {
   std::lock_guard<std::mutex> lock(mu);
   if (prepared) return;
   prepare_gemm<64, EPI_BIAS_GELU, true>();
+  prepare_gemm<256, EPI_BIAS_GELU, true>();
   prepare_tma_gemm<64, EPI_BIAS_GELU>();
+  prepare_tma_gemm<256, EPI_BIAS_GELU>();
   prepare_tma_gemm<64, EPI_GELU_GRAD>();
   prepare_tma_gemm<64, EPI_F32>();
   prepare_tma_gemm<256, EPI_F32>();
@@ -1027,13 +1029,23 @@ static void run_batch(Mlp::Impl& m, const float* X, const uint32_t* rows, int64_
   e1.out_t = train ? m.h1t.p : nullptr;
   e1.ldo = HID;
   e1.ldt = (int)B;
-  launch_gemm<64, EPI_BIAS_GELU, true>(nullptr, 8, m.w1b.p, m.in_dim, B, HID, m.in_dim, 1, e1, m.err.p, s, &ga);
+  // Inference on large batches: one CTA per 128 rows covers all 256 hidden units (the rows are
+  // gathered once instead of once per 64-column tile); training keeps 64-column tiles for
+  // parallelism at its batch of a few thousand rows.
+  const bool wide = !train && B >= 8192;
+  if (wide)
+    launch_gemm<256, EPI_BIAS_GELU, true>(nullptr, 8, m.w1b.p, m.in_dim, B, HID, m.in_dim, 1, e1, m.err.p, s, &ga);
+  else
+    launch_gemm<64, EPI_BIAS_GELU, true>(nullptr, 8, m.w1b.p, m.in_dim, B, HID, m.in_dim, 1, e1, m.err.p, s, &ga);
   EpiArgs e2{};
   e2.bias = m.w.p + m.o_b2;
   e2.out_f32 = train ? m.z2.p : nullptr;
   e2.out_bf16 = m.h2.p;
   e2.ldo = HID;
-  launch_tma_gemm<64, EPI_BIAS_GELU>(m.h1.p, HID, m.w2b.p, HID, B, HID, HID, 1, e2, m.err.p, s);
+  if (wide)
+    launch_tma_gemm<256, EPI_BIAS_GELU>(m.h1.p, HID, m.w2b.p, HID, B, HID, HID, 1, e2, m.err.p, s);
+  else
+    launch_tma_gemm<64, EPI_BIAS_GELU>(m.h1.p, HID, m.w2b.p, HID, B, HID, HID, 1, e2, m.err.p, s);
   const float inv = 1.0f / (float)(B * m.out_dim);
 #define UB_OUT_ARGS                                                                                                   \
   m.h2.p, m.z2.p, m.w3b.p, m.w.p + m.o_b3, train ? Y : nullptr, rows, n_valid, inv, y_out, m.dz2.p, m.dz2t.p, B, \

@@ -794,14 +794,22 @@ KnnStats knn_bruteforce(const float* X, uint64_t n, uint64_t d, uint64_t k, uint
     UB_CUDA(cudaStreamSynchronize(s));
     return st;
   }
-  static std::once_flag once;
-  std::call_once(once, [] {
-    UB_CUDA(cudaFuncSetAttribute(knn_candidates_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)KNN_SMEM));
-    UB_CUDA(cudaFuncSetAttribute(knn_exact_part_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)(KNN_MAX_K * 256 * 8)));
-    UB_CUDA(cudaFuncSetAttribute(knn_exact_part_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)(KNN_MAX_K_EXACT * 128 * 8)));
-  });
+  {
+    // kernel attributes belong to the device's context: set them once per device
+    static std::mutex mu;
+    static uint64_t done = 0;  // bit per device id < 64
+    int dev = 0;
+    UB_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(mu);
+    if (dev >= 64 || !((done >> dev) & 1u)) {
+      UB_CUDA(cudaFuncSetAttribute(knn_candidates_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)KNN_SMEM));
+      UB_CUDA(cudaFuncSetAttribute(knn_exact_part_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)(KNN_MAX_K * 256 * 8)));
+      UB_CUDA(cudaFuncSetAttribute(knn_exact_part_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)(KNN_MAX_K_EXACT * 128 * 8)));
+      if (dev < 64) done |= 1ull << dev;
+    }
+  }
   const int di = (int)d;
   const int64_t dp = (int64_t)((d + KC - 1) / KC) * KC;
   const int64_t n_pad = (int64_t)((n + DBN - 1) / DBN) * DBN;

@@ -802,9 +802,11 @@ int k_splits(int64_t K, int tiles) {
 
 void prepare_all_gemms() {
   static std::mutex mu;
-  static bool prepared = false;  // the attribute is per function and process-wide
+  static uint64_t prepared = 0;  // kernel attributes belong to a device's context: bit per device id < 64
+  int dev = 0;
+  UB_CUDA(cudaGetDevice(&dev));
   std::lock_guard<std::mutex> lock(mu);
-  if (prepared) return;
+  if (dev < 64 && ((prepared >> dev) & 1u)) return;
   prepare_gemm<64, EPI_BIAS_GELU, true>();
   prepare_gemm<256, EPI_BIAS_GELU, true>();
   prepare_tma_gemm<64, EPI_BIAS_GELU>();
@@ -817,7 +819,7 @@ void prepare_all_gemms() {
   prepare_tma_gemm<256, EPI_F32_ATOMIC>();
   prepare_tma_gemm<64, EPI_F32_ATOMIC>();
   (void)encode_tiled();
-  prepared = true;
+  if (dev < 64) prepared |= 1ull << dev;
 }
 
 }  // namespace

@@ -161,3 +161,25 @@ def test_rust_ffi_is_generated_from_the_header():
     from umap_b200._lib import UmapConfigC
     fields = re.findall(r"^    pub (\w+): ", committed.split("pub struct umap_config {")[1].split("}")[0], re.M)
     assert fields == [f[0] for f in UmapConfigC._fields_]
+
+
+def test_output_metric_checks_without_gpu(ub):
+    """metric.rs / distances.rs on the host side: EuclideanMetric's distance and gradient
+    (distances.rs:208-223, f32), the metric types and device ids that route Optimizer and
+    Umap.fit, and the refusal of a metric with no device form before any GPU work."""
+    import numpy as np
+    x = np.float32([1.5, -2.0, 0.25])
+    y = np.float32([0.5, 1.0, 0.25])
+    d, g = ub.EuclideanMetric().distance(x, y)
+    assert d == np.float32(np.sqrt(np.float32(1.0) + np.float32(9.0)))
+    assert np.array_equal(g, (x - y) / np.float32(d + np.float32(1e-6)))
+    assert ub.EuclideanMetric().metric_type() == ub.MetricType.Euclidean
+    assert ub.GenericEuclideanMetric().metric_type() == ub.MetricType.Generic
+    assert ub.GenericEuclideanMetric().device_metric() == ub.OUTPUT_METRIC_EUCLIDEAN
+    assert ub.Metric().metric_type() == ub.MetricType.Generic and ub.Metric().device_metric() is None
+    idx = np.zeros((20, 3), np.uint32)
+    dist = np.zeros((20, 3), np.float32)
+    init = np.zeros((20, 2), np.float32)
+    with pytest.raises(ub.UmapError) as e:
+        ub.Umap.with_metrics(ub.UmapConfig(), ub.EuclideanMetric(), ub.Metric()).fit(20, idx, dist, init)
+    assert e.value.code == ub.ERR_UNSUPPORTED

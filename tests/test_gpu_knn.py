@@ -31,6 +31,7 @@ def _data(n, d, seed, kind="gauss"):
     (2, 3, 1, "gauss"), (3, 2, 5, "gauss"), (17, 7, 16, "gauss"), (257, 1, 15, "gauss"),
     (300, 64, 15, "gauss"), (1000, 100, 32, "gauss"), (2049, 16, 15, "clusters"), (1500, 8, 20, "ties"),
     (1200, 784, 15, "pixels"), (900, 33, 10, "offset"), (5000, 64, 15, "clusters"),
+    (300, 1500, 15, "gauss"), (2000, 3, 1, "ties"), (700, 130, 31, "clusters"),
     # from 16,384 points the scan runs in pivot (locality) order
     (20000, 24, 15, "clusters"), (16400, 100, 32, "pixels"), (16384, 5, 15, "ties"),
 ])

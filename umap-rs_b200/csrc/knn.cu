@@ -410,22 +410,35 @@ __global__ void __launch_bounds__(KNN_THREADS, 1) knn_candidates_kernel(
       hd[s * QM + trow] = INFINITY;
       hi[s * QM + trow] = 0xFFFFFFFFu;
     }
-    float tau = INFINITY, thr = live ? -INFINITY : INFINITY;
+    float tau = INFINITY, thr_h = live ? -INFINITY : INFINITY;  // (|q|^2 - tau) / 2
     // 32 columns of the accumulator: v = 2 s - |y|^2; a column enters the heap when
     // |q|^2 - v < tau, i.e. v > thr.  The common case costs the FMAs and a running max.
     auto process = [&](const uint32_t (&r)[32], const float* nrm, int64_t c0) {
+      // u = s - |y|^2 / 2 = v / 2 exactly (halving commutes with rounding), two columns per
+      // packed FMA; u > thr / 2 is the same test as v > thr
       float v[32];
       float vmax = -INFINITY;
+      const uint64_t mhalf = 0xBF000000BF000000ull;  // (-0.5f, -0.5f)
 #pragma unroll
       for (int i = 0; i < 8; ++i) {
         const float4 w = reinterpret_cast<const float4*>(nrm)[i];
-        v[4 * i + 0] = fmaf(2.0f, __uint_as_float(r[4 * i + 0]), -w.x);
-        v[4 * i + 1] = fmaf(2.0f, __uint_as_float(r[4 * i + 1]), -w.y);
-        v[4 * i + 2] = fmaf(2.0f, __uint_as_float(r[4 * i + 2]), -w.z);
-        v[4 * i + 3] = fmaf(2.0f, __uint_as_float(r[4 * i + 3]), -w.w);
+        uint64_t s0, s1, n0, n1, d0, d1;
+        asm("mov.b64 %0, {%1, %2};" : "=l"(s0) : "r"(r[4 * i + 0]), "r"(r[4 * i + 1]));
+        asm("mov.b64 %0, {%1, %2};" : "=l"(s1) : "r"(r[4 * i + 2]), "r"(r[4 * i + 3]));
+        asm("mov.b64 %0, {%1, %2};" : "=l"(n0) : "r"(__float_as_uint(w.x)), "r"(__float_as_uint(w.y)));
+        asm("mov.b64 %0, {%1, %2};" : "=l"(n1) : "r"(__float_as_uint(w.z)), "r"(__float_as_uint(w.w)));
+        asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d0) : "l"(n0), "l"(mhalf), "l"(s0));
+        asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d1) : "l"(n1), "l"(mhalf), "l"(s1));
+        uint32_t a0, a1, a2, a3;
+        asm("mov.b64 {%0, %1}, %2;" : "=r"(a0), "=r"(a1) : "l"(d0));
+        asm("mov.b64 {%0, %1}, %2;" : "=r"(a2), "=r"(a3) : "l"(d1));
+        v[4 * i + 0] = __uint_as_float(a0);
+        v[4 * i + 1] = __uint_as_float(a1);
+        v[4 * i + 2] = __uint_as_float(a2);
+        v[4 * i + 3] = __uint_as_float(a3);
         vmax = fmaxf(vmax, fmaxf(fmaxf(v[4 * i], v[4 * i + 1]), fmaxf(v[4 * i + 2], v[4 * i + 3])));
       }
-      if (!(vmax > thr)) return;
+      if (!(vmax > thr_h)) return;
 #pragma unroll
       for (int h = 0; h < 4; ++h) {
         // stage 8 values (dynamic index below) and mark those above the threshold
@@ -433,13 +446,13 @@ __global__ void __launch_bounds__(KNN_THREADS, 1) knn_candidates_kernel(
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
           vs[i * QM + trow] = v[8 * h + i];
-          hits |= (v[8 * h + i] > thr ? 1u : 0u) << i;
+          hits |= (v[8 * h + i] > thr_h ? 1u : 0u) << i;
         }
         while (hits) {
           const int i = __ffs(hits) - 1;
           hits &= hits - 1;
           const int64_t col = c0 + 8 * h + i;
-          const float a = nq - vs[i * QM + trow];
+          const float a = nq - 2.0f * vs[i * QM + trow];
           if (!(a < tau) || col >= n || col == row) continue;
           // max-heap on the approximate distance: replace the root, sift down
           int pos = 0;
@@ -458,7 +471,7 @@ __global__ void __launch_bounds__(KNN_THREADS, 1) knn_candidates_kernel(
           hd[pos * QM + trow] = a;
           hi[pos * QM + trow] = (uint32_t)col;
           tau = hd[trow];
-          thr = nq - tau;
+          thr_h = 0.5f * (nq - tau);
         }
       }
     };

@@ -122,6 +122,34 @@ __device__ __forceinline__ float clip4(float v) {
   return x;
 }
 
+// Two-lane FP32 arithmetic on a 2-D row (each lane the same IEEE operation as the scalar one).
+__device__ __forceinline__ uint64_t pk2(float x, float y) {
+  uint64_t r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "r"(__float_as_uint(x)), "r"(__float_as_uint(y)));
+  return r;
+}
+__device__ __forceinline__ void up2(uint64_t v, float& x, float& y) {
+  uint32_t a, b;
+  asm("mov.b64 {%0, %1}, %2;" : "=r"(a), "=r"(b) : "l"(v));
+  x = __uint_as_float(a);
+  y = __uint_as_float(b);
+}
+__device__ __forceinline__ uint64_t sub2(uint64_t a, uint64_t b) {
+  uint64_t r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ uint64_t mul2(uint64_t a, uint64_t b) {
+  uint64_t r;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ uint64_t fma2(uint64_t a, uint64_t b, uint64_t c) {
+  uint64_t r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+  return r;
+}
+
 // ------------------------------------------------------------------------------ K7
 constexpr int NEG_BATCH = UB_SGD_NEG_BATCH; // negative-sample rows fetched together
 static_assert(NEG_BATCH >= 1 && NEG_BATCH <= 16, "negative batch size");
@@ -250,6 +278,25 @@ __device__ __forceinline__ void fired_edge(float (&cur)[DIM], uint32_t r, uint32
     for (int q = 0; q < NEG_BATCH; ++q) {
       if (q0 + q >= nneg) break;
       if (kk[q] == r) continue;
+      if constexpr (DIM == 2 && !GEN) {
+        // the same operations as the generic-DIM code below, two columns per instruction
+        const uint64_t c2 = pk2(cur[0], cur[1]);
+        const uint64_t df2 = sub2(c2, pk2(ob[q][0], ob[q][1]));
+        float df0, df1;
+        up2(df2, df0, df1);
+        const float dsn = df0 * df0 + df1 * df1;
+        float gr = 0.0f;
+        if (dsn > 0.0f) {
+          const float pb = __powf(dsn, b);
+          gr = __fdividef(p.pos_rep, (0.001f + dsn) * (a * pb * dsn + 1.0f));
+        }
+        if (gr > 0.0f) {
+          float t0, t1;
+          up2(mul2(pk2(gr, gr), df2), t0, t1);
+          up2(fma2(pk2(clip4(t0), clip4(t1)), pk2(alpha, alpha), c2), cur[0], cur[1]);
+        }
+        continue;
+      }
       float dsn = 0.0f;
 #pragma unroll
       for (int d = 0; d < DIM; ++d) { const float df = cur[d] - ob[q][d]; dsn += df * df; }

@@ -18,6 +18,7 @@ Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [-
 from __future__ import annotations
 
 import argparse
+import atexit
 import json
 import os
 import subprocess
@@ -93,47 +94,75 @@ def traffic_per_epoch():
     return None
 
 
-class Clocks:
-    """Samples SM clocks and throttle reasons with nvidia-smi during the timed region."""
+class _Sampler:
+    """One nvidia-smi process per bench run sampling SM clocks and throttle reasons every
+    200 ms.  It starts before the workload is built, so that its NVML start-up (which has
+    stalled a fit by ~200 ms when it fell inside the timed region) happens outside timing."""
     Q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, index: int):
         self.index, self.samples, self.proc = index, [], None
-
-    def __enter__(self):
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(index), "--query-gpu=" + self.Q,
                                           "--format=csv,noheader,nounits", "-lms", "200"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             threading.Thread(target=self._read, daemon=True).start()
+            atexit.register(self.stop)
         except Exception:
             self.proc = None
-        return self
 
     def _read(self):
         for line in self.proc.stdout:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) == 6:
-                self.samples.append(parts)
+                self.samples.append((time.time(), parts))
 
-    def __exit__(self, *a):
-        if self.proc:
+    def stop(self):
+        if self.proc and self.proc.poll() is None:
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except Exception:
                 self.proc.kill()
 
+
+_SAMPLERS = {}
+
+
+def start_clock_sampler(index: int):
+    if index not in _SAMPLERS:
+        _SAMPLERS[index] = _Sampler(index)
+    return _SAMPLERS[index]
+
+
+class Clocks:
+    """The clock samples of the timed region: `with Clocks(i) as clk:` around it, then
+    `clk.summary()`.  Samples within 0.25 s of the region count (a region shorter than the
+    sampling period still gets its nearest samples)."""
+
+    def __init__(self, index: int):
+        self.s = start_clock_sampler(index)
+        self.t0 = self.t1 = None
+
+    def __enter__(self):
+        self.t0 = time.time()
+        return self
+
+    def __exit__(self, *a):
+        self.t1 = time.time()
+
     def summary(self):
-        if not self.samples:
+        t1 = self.t1 if self.t1 is not None else time.time()
+        samples = [p for t, p in list(self.s.samples) if self.t0 - 0.25 <= t <= t1 + 0.25]
+        if not samples:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
-        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        sm = [float(x[0]) for x in samples if x[0].replace(".", "").isdigit()]
+        mx = [float(x[1]) for x in samples if x[1].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[2 + i].lower() == "active"})
+        reasons = sorted({names[i] for x in samples for i in range(4) if x[2 + i].lower() == "active"})
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.samples)}
+                "reasons": reasons, "samples": len(samples)}
 
 
 def make_workload(n, library_knn=True):
@@ -665,6 +694,8 @@ def main():
     a = parse()
     if a.impl == "reference":
         return run_reference(a)
+    # the clock sampler starts now, long before any timed region
+    start_clock_sampler(int(os.environ.get("LOCAL_RANK", "0")))
     if a.workload == "batched":
         return run_batched(a)
     if a.workload == "warm_start":
@@ -719,18 +750,23 @@ def main():
     dim = 2
     alg_bytes = 4.0 * E * a.epochs + F_tot * (8 + 16 * dim) + 4.0 * dim * N_tot
 
+    # warm-up in the timed loop's pattern (the previous fit's result stays alive while the
+    # next one runs), so that the device-memory cache reaches its steady size before timing
+    f = None
     for _ in range(a.warmup):
-        one_fit()
+        f, _ = one_fit()
     torch.cuda.synchronize()
     R.barrier(torch.device("cuda", local))
     torch.cuda.synchronize()
     launches0 = ub.kernel_launches()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    sgd_ms = []
+    sgd_ms, fit_wall = [], []
     with Clocks(local) as clk:
         ev0.record()
         for _ in range(a.steps):
+            t_fit = time.perf_counter()
             f, ms = one_fit()
+            fit_wall.append(round((time.perf_counter() - t_fit) * 1e3, 1))
             sgd_ms.append(ms)
         ev1.record()
         torch.cuda.synchronize()
@@ -779,7 +815,7 @@ def main():
                    "epochs": a.epochs, "n_components": 2, "kept_edges": E, "edge_updates_per_fit": F_tot,
                    "negatives_per_fit": N_tot, "l2": "inputs exceed L2 (kNN 240 MB + edge slices)",
                    "parallelism": "replicas" if world > 1 else "single", **winfo},
-        "fit_ms": ms_step,
+        "fit_ms": ms_step, "fit_wall_ms_each": fit_wall,
         "sgd_ms_per_fit": float(np.median(sgd_ms)),
         "sgd_edge_updates_per_s": F_tot / (float(np.median(sgd_ms)) / 1e3),
         "e2e": {"value": F_tot / (e2e_step / 1e3), "unit": "edge-updates/s", "ms_per_step": e2e_step,

@@ -29,6 +29,7 @@
 #include <cstdint>
 #include <cstdlib>
 #include <mutex>
+#include <utility>
 #include <vector>
 
 #include "ub_internal.hpp"
@@ -224,19 +225,23 @@ __global__ void __launch_bounds__(GT) umma_gemm_kernel(const bf16* __restrict__ 
   const int64_t k_begin = (int64_t)blockIdx.z * k_per_cta;
   const int n_chunks = k_per_cta / KC;
 
-  if (warp == 0) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
-                 :: "r"(smem_u32(&tmem_base)), "r"(TCOLS) : "memory");
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
-  }
   if (tid == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(&mbar[0])), "r"(1) : "memory");
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(&mbar[1])), "r"(1) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
+  // Everything above overlaps the previous kernel; its results are read below.  Tensor memory
+  // is taken only after it has finished, so a waiting CTA never holds any.
+  grid_wait();
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                 :: "r"(smem_u32(&tmem_base)), "r"(TCOLS) : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  grid_release();
   const uint32_t taddr = tmem_base;
 
   // A[m0:m0+128, k:k+64] and B[n0:n0+BN, k:k+64] of chunk c into stage `st`, 16-byte vectors.
@@ -373,22 +378,28 @@ __global__ void __launch_bounds__(GT) umma_tma_gemm_kernel(const __grid_constant
   const int64_t k_begin = (int64_t)blockIdx.z * k_per_cta;
   const int n_chunks = k_per_cta / KC;
 
-  if (warp == 0) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
-                 :: "r"(smem_u32(&tmem_base)), "r"(TCOLS) : "memory");
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
-  }
   if (tid == 0) {
     for (int i = 0; i < TS; ++i) {
       asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(&full[i])), "r"(1) : "memory");
       asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(&empty[i])), "r"(1) : "memory");
     }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("prefetch.tensormap [%0];" :: "l"(reinterpret_cast<uint64_t>(&ta)) : "memory");
+    asm volatile("prefetch.tensormap [%0];" :: "l"(reinterpret_cast<uint64_t>(&tb)) : "memory");
     s_fail = 0;
+  }
+  // As in umma_gemm_kernel: set-up overlaps the previous kernel, tensor memory and global
+  // memory are touched only after it has finished.
+  grid_wait();
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                 :: "r"(smem_u32(&tmem_base)), "r"(TCOLS) : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  grid_release();
   const uint32_t taddr = tmem_base;
 
   if (tid == 0) {
@@ -471,6 +482,25 @@ constexpr size_t gemm_smem() {
   return (size_t)2 * (GM + BN) * KC * 2;
 }
 
+// Launch of `k` on `s`; with `pdl` it carries the programmatic-stream-serialization attribute,
+// so it may be scheduled while the previous kernel on `s` still runs (the kernel orders its
+// memory accesses after that kernel's end with grid_wait()).
+template <typename... KArgs, typename... Args>
+void launch_k(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, bool pdl, Args&&... args) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = pdl ? 1 : 0;
+  UB_CUDA(cudaLaunchKernelEx(&cfg, k, std::forward<Args>(args)...));
+  count_launch();
+}
+
 template <int BN, int EPI, bool GATHER = false>
 void prepare_gemm() {
   UB_CUDA(cudaFuncSetAttribute(umma_gemm_kernel<BN, EPI, GATHER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -481,7 +511,8 @@ void prepare_gemm() {
 // part's sum to its own slice (ep.split_stride apart), EPI_F32_ATOMIC adds them up.
 template <int BN, int EPI, bool GATHER = false>
 void launch_gemm(const bf16* A, int64_t lda, const bf16* B, int64_t ldb, int64_t M, int64_t N, int64_t K,
-                 int ksplit, const EpiArgs& ep, unsigned* err, cudaStream_t s, const GatherA* ga = nullptr) {
+                 int ksplit, const EpiArgs& ep, unsigned* err, cudaStream_t s, const GatherA* ga = nullptr,
+                 bool pdl = false) {
   if (M <= 0 || M % GM || N % BN || K <= 0 || ksplit < 1 || K % ((int64_t)KC * ksplit) || lda % 8 || ldb % 8 ||
       M / GM > 0x7FFFFFFF || lda > 0x7FFFFFFF || ldb > 0x7FFFFFFF || ksplit > 65535)
     throw Error(INVALID_ARGUMENT, "tensor-core GEMM shape: M % 128, N % tile, K % (64 * splits), rows of 16 bytes");
@@ -491,9 +522,8 @@ void launch_gemm(const bf16* A, int64_t lda, const bf16* B, int64_t ldb, int64_t
   GatherA g{};
   if (ga) g = *ga;
   dim3 grid((unsigned)(M / GM), (unsigned)(N / BN), (unsigned)ksplit);
-  umma_gemm_kernel<BN, EPI, GATHER><<<grid, GT, gemm_smem<BN>(), s>>>(A, (int)lda, B, (int)ldb, (int)(K / ksplit),
-                                                                      ep, g, err);
-  UB_LAUNCH_CHECK();
+  launch_k(umma_gemm_kernel<BN, EPI, GATHER>, grid, dim3(GT), gemm_smem<BN>(), s, pdl, A, (int)lda, B, (int)ldb,
+           (int)(K / ksplit), ep, g, err);
 }
 
 
@@ -506,7 +536,7 @@ void prepare_tma_gemm() {
 // C = A[M,K] B[N,K]^T through the TMA-fed kernel; K split into `ksplit` parts as launch_gemm.
 template <int BN, int EPI>
 void launch_tma_gemm(const bf16* A, int64_t lda, const bf16* B, int64_t ldb, int64_t M, int64_t N, int64_t K,
-                     int ksplit, const EpiArgs& ep, unsigned* err, cudaStream_t s) {
+                     int ksplit, const EpiArgs& ep, unsigned* err, cudaStream_t s, bool pdl = false) {
   if (M <= 0 || M % GM || N <= 0 || N % BN || K <= 0 || ksplit < 1 || K % ((int64_t)KC * ksplit) ||
       M / GM > 0x7FFFFFFF || ksplit > 65535 || K > 0x7FFFFFFF || M > 0x7FFFFFFF || N > 0x7FFFFFFF)
     throw Error(INVALID_ARGUMENT, "tensor-core GEMM shape: M % 128, N % tile, K % (64 * splits), rows of 16 bytes");
@@ -515,8 +545,8 @@ void launch_tma_gemm(const bf16* A, int64_t lda, const bf16* B, int64_t ldb, int
   const CUtensorMap ta = bf16_tile_map(A, M, K, lda, GM);
   const CUtensorMap tb = bf16_tile_map(B, N, K, ldb, BN);
   dim3 grid((unsigned)(M / GM), (unsigned)(N / BN), (unsigned)ksplit);
-  umma_tma_gemm_kernel<BN, EPI><<<grid, GT, tma_gemm_smem<BN>(), s>>>(ta, tb, (int)(K / ksplit), ep, err);
-  UB_LAUNCH_CHECK();
+  launch_k(umma_tma_gemm_kernel<BN, EPI>, grid, dim3(GT), tma_gemm_smem<BN>(), s, pdl, ta, tb, (int)(K / ksplit), ep,
+           err);
 }
 
 // ------------------------------------------------------------------------------ CUDA-core parts
@@ -538,6 +568,8 @@ __global__ void __launch_bounds__(256) out_layer_kernel(
   __shared__ float s_gb2[HID];
   __shared__ float s_gb3[OUT];
   __shared__ float s_loss;
+  grid_wait();
+  grid_release();
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const bool train = Y != nullptr;
   if (train) {
@@ -693,6 +725,8 @@ __device__ __forceinline__ float slice_sum(const float* part, int ks, int64_t st
 }
 
 __global__ void adam_kernel(AdamArgs a) {
+  grid_wait();
+  grid_release();
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= a.n) return;
   const float t = (float)*a.step;
@@ -791,6 +825,13 @@ bool graphs_enabled() {
   return !(e && e[0] == '0');
 }
 
+// Programmatic dependent launch between the kernels of a network step (UMAP_B200_PDL=0 turns
+// it off).
+bool pdl_enabled() {
+  const char* e = std::getenv("UMAP_B200_PDL");
+  return !(e && e[0] == '0');
+}
+
 // Split of a batch-row contraction of length K over `tiles` output tiles: the largest power
 // of two that keeps about 64 CTAs and whole 64-row chunks per split (the TMA pipeline keeps
 // a CTA's chunks in flight, so fewer, longer splits cost less than more slices to sum).
@@ -854,6 +895,7 @@ struct Mlp::Impl {
   DevBuf<bf16> w1b, w2b, w2t, w3b;  // bf16 working copies (w2t = W2^T)
   DevBuf<float> shift, scale;       // input standardisation
   bool has_norm = false;
+  bool pdl = pdl_enabled();
   DevBuf<unsigned> err, step;
   DevBuf<float> loss;
   // per-batch activations, capacity `cap` rows
@@ -1010,9 +1052,13 @@ void Mlp::set_input_norm(const float* shift, const float* scale) {
 // the batch rows of X and Y) also the backward: dW1 / dW2 into their K-split slices, the other
 // gradients added into g, the loss into `loss`; with_adam then applies the Adam update.
 // Inference writes y for rows < n_valid.
+// One forward pass (and with targets the backward pass and, with `with_adam`, the update) of a
+// batch.  Each kernel after the first on `s` is a programmatic dependent launch; the first
+// one is too when `after_step` says the previous kernel on `s` was this network's update.
 static void run_batch(Mlp::Impl& m, const float* X, const uint32_t* rows, int64_t B, int64_t n_valid,
-                      const float* Y, float* y_out, bool with_adam, float lr) {
+                      const float* Y, float* y_out, bool with_adam, float lr, bool after_step = false) {
   cudaStream_t s = m.s;
+  const bool pdl = m.pdl;
   const bool train = Y != nullptr;
   float* g = m.g.p;
   GatherA ga{};
@@ -1035,32 +1081,34 @@ static void run_batch(Mlp::Impl& m, const float* X, const uint32_t* rows, int64_
   // gathered once instead of once per 64-column tile); training keeps 64-column tiles for
   // parallelism at its batch of a few thousand rows.
   const bool wide = !train && B >= 8192;
+  const bool pdl1 = pdl && after_step;
   if (wide)
-    launch_gemm<256, EPI_BIAS_GELU, true>(nullptr, 8, m.w1b.p, m.in_dim, B, HID, m.in_dim, 1, e1, m.err.p, s, &ga);
+    launch_gemm<256, EPI_BIAS_GELU, true>(nullptr, 8, m.w1b.p, m.in_dim, B, HID, m.in_dim, 1, e1, m.err.p, s, &ga,
+                                          pdl1);
   else
-    launch_gemm<64, EPI_BIAS_GELU, true>(nullptr, 8, m.w1b.p, m.in_dim, B, HID, m.in_dim, 1, e1, m.err.p, s, &ga);
+    launch_gemm<64, EPI_BIAS_GELU, true>(nullptr, 8, m.w1b.p, m.in_dim, B, HID, m.in_dim, 1, e1, m.err.p, s, &ga,
+                                         pdl1);
   EpiArgs e2{};
   e2.bias = m.w.p + m.o_b2;
   e2.out_f32 = train ? m.z2.p : nullptr;
   e2.out_bf16 = m.h2.p;
   e2.ldo = HID;
   if (wide)
-    launch_tma_gemm<256, EPI_BIAS_GELU>(m.h1.p, HID, m.w2b.p, HID, B, HID, HID, 1, e2, m.err.p, s);
+    launch_tma_gemm<256, EPI_BIAS_GELU>(m.h1.p, HID, m.w2b.p, HID, B, HID, HID, 1, e2, m.err.p, s, pdl);
   else
-    launch_tma_gemm<64, EPI_BIAS_GELU>(m.h1.p, HID, m.w2b.p, HID, B, HID, HID, 1, e2, m.err.p, s);
+    launch_tma_gemm<64, EPI_BIAS_GELU>(m.h1.p, HID, m.w2b.p, HID, B, HID, HID, 1, e2, m.err.p, s, pdl);
   const float inv = 1.0f / (float)(B * m.out_dim);
 #define UB_OUT_ARGS                                                                                                   \
   m.h2.p, m.z2.p, m.w3b.p, m.w.p + m.o_b3, train ? Y : nullptr, rows, n_valid, inv, y_out, m.dz2.p, m.dz2t.p, B, \
       g + m.o_w3, g + m.o_b3, g + m.o_b2, m.loss.p, with_adam ? m.step.p : nullptr
   const unsigned og = (unsigned)(B / 32);
   switch (m.out_dim) {
-    case 1: out_layer_kernel<1><<<og, 256, 0, s>>>(UB_OUT_ARGS); break;
-    case 2: out_layer_kernel<2><<<og, 256, 0, s>>>(UB_OUT_ARGS); break;
-    case 3: out_layer_kernel<3><<<og, 256, 0, s>>>(UB_OUT_ARGS); break;
-    default: out_layer_kernel<4><<<og, 256, 0, s>>>(UB_OUT_ARGS); break;
+    case 1: launch_k(out_layer_kernel<1>, dim3(og), dim3(256), 0, s, pdl, UB_OUT_ARGS); break;
+    case 2: launch_k(out_layer_kernel<2>, dim3(og), dim3(256), 0, s, pdl, UB_OUT_ARGS); break;
+    case 3: launch_k(out_layer_kernel<3>, dim3(og), dim3(256), 0, s, pdl, UB_OUT_ARGS); break;
+    default: launch_k(out_layer_kernel<4>, dim3(og), dim3(256), 0, s, pdl, UB_OUT_ARGS); break;
   }
 #undef UB_OUT_ARGS
-  UB_LAUNCH_CHECK();
   if (!train) return;
   // dW2 = dZ2^T H1 on the second stream, beside dH1 and dW1.
   UB_CUDA(cudaEventRecord(m.fork, s));
@@ -1079,13 +1127,13 @@ static void run_batch(Mlp::Impl& m, const float* X, const uint32_t* rows, int64_
   e3.colsum = g + m.o_b1;
   e3.ldo = HID;
   e3.ldt = (int)B;
-  launch_tma_gemm<64, EPI_GELU_GRAD>(m.dz2.p, HID, m.w2t.p, HID, B, HID, HID, 1, e3, m.err.p, s);
+  launch_tma_gemm<64, EPI_GELU_GRAD>(m.dz2.p, HID, m.w2t.p, HID, B, HID, HID, 1, e3, m.err.p, s, pdl);
   // dW1 = dZ1^T X
   EpiArgs e5{};
   e5.out_f32 = m.part1.p;
   e5.split_stride = (int64_t)HID * m.in_dim;
   e5.ldo = m.in_dim;
-  launch_tma_gemm<64, EPI_F32>(m.dz1t.p, B, m.xt.p, B, HID, m.in_dim, B, m.ks1, e5, m.err.p, s);
+  launch_tma_gemm<64, EPI_F32>(m.dz1t.p, B, m.xt.p, B, HID, m.in_dim, B, m.ks1, e5, m.err.p, s, pdl);
   UB_CUDA(cudaStreamWaitEvent(s, m.join, 0));
   if (!with_adam) return;
   AdamArgs a{};
@@ -1163,7 +1211,8 @@ void Mlp::train(const float* X, const float* Y, int64_t n, int epochs, int64_t b
   DevBuf<float> dloss(epochs, s);
   UB_CUDA(cudaMemsetAsync(m.g.p, 0, m.P * 4, s));
   auto one_epoch = [&]() {
-    for (int64_t t = 0; t < steps; ++t) run_batch(m, X, cur.p + t * batch, batch, batch, Y, nullptr, true, lr);
+    for (int64_t t = 0; t < steps; ++t)
+      run_batch(m, X, cur.p + t * batch, batch, batch, Y, nullptr, true, lr, t > 0);
   };
   cudaGraphExec_t exec = nullptr;
   if (graphs_enabled()) {

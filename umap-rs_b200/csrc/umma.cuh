@@ -73,6 +73,14 @@ __device__ __forceinline__ bool mbar_wait(uint32_t addr, uint32_t phase) {
   return false;
 }
 
+// Programmatic dependent launch.  `grid_wait` returns once every grid this launch depends on
+// has completed and its memory is visible (a no-op for a launch without the attribute); a
+// kernel reads and writes no global memory, and allocates no tensor memory, before it.
+// `grid_release` lets the dependent launch be scheduled once every CTA of this grid has
+// executed it (or exited); the dependent's own `grid_wait` still waits for this grid's end.
+__device__ __forceinline__ void grid_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void grid_release() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 }  // namespace umma
 
 // Tensor map of a row-major bf16 (or, with f16, fp16) matrix [rows, cols] (row stride ld

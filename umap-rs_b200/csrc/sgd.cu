@@ -31,13 +31,13 @@ namespace {
 
 constexpr uint32_t PAD_ROW = 0xFFFFFFFFu;
 
-// Tuning knobs (compile-time).
-#ifndef UB_SGD_NEG_BATCH
-#define UB_SGD_NEG_BATCH 4   // negative-sample rows fetched together
-#endif
-#ifndef UB_SGD_MIN_BLOCKS
-#define UB_SGD_MIN_BLOCKS 5  // resident 256-thread blocks per SM the register budget targets
-#endif
+// The epoch kernel comes in two register budgets.  Large graphs (many waves of warps) are
+// bound by instruction issue and L2 sector throughput: 4 negative rows fetched together and
+// 5 resident 256-thread blocks per SM (48 registers).  Graphs that fill about two waves or
+// fewer are bound by the chain of dependent loads of their busiest lanes: 8 negative rows
+// fetched together (one round trip for a firing's usual 4-6 negatives) and 4 blocks per SM.
+constexpr int NB_WIDE = 4, MINB_WIDE = 5;
+constexpr int NB_SHORT = 8, MINB_SHORT = 4;
 
 // ------------------------------------------------------------------------------ negatives' RNG
 // Counter-based: the firing of entry `idx` at `epoch` draws its negatives in pairs; pair t is
@@ -151,8 +151,6 @@ __device__ __forceinline__ uint64_t fma2(uint64_t a, uint64_t b, uint64_t c) {
 }
 
 // ------------------------------------------------------------------------------ K7
-constexpr int NEG_BATCH = UB_SGD_NEG_BATCH; // negative-sample rows fetched together
-static_assert(NEG_BATCH >= 1 && NEG_BATCH <= 16, "negative batch size");
 
 template <int DIM>
 __device__ __forceinline__ void load_row(float (&v)[DIM], const float* p) {
@@ -214,7 +212,7 @@ __device__ __forceinline__ float metric_coeff(float ds, float a, float two_b, fl
 // of optimize_layout_generic.rs:57-121): attractive step on (head, tail), then `nneg`
 // negative samples, all reading the snapshot buffer.  The tail row and a batch of negative
 // rows are fetched together before the (sequential) updates of `cur`.
-template <int DIM, bool GEN>
+template <int DIM, bool GEN, int NEG_BATCH>
 __device__ __forceinline__ void fired_edge(float (&cur)[DIM], uint32_t r, uint32_t k, uint32_t nneg,
                                            float* snap, const SgdParams& p, float alpha, uint64_t idx,
                                            uint32_t epoch, uint64_t seed, uint32_t seg_lo, uint32_t seg_n) {
@@ -326,8 +324,8 @@ __device__ __forceinline__ void fired_edge(float (&cur)[DIM], uint32_t r, uint32
 #ifndef UB_SGD2_W
 #define UB_SGD2_W 4
 #endif
-template <int DIM, bool GEN>
-__global__ void __launch_bounds__(256, UB_SGD_MIN_BLOCKS) sgd_epoch_kernel2(
+template <int DIM, bool GEN, int NEG_BATCH, int MINB>
+__global__ void __launch_bounds__(256, MINB) sgd_epoch_kernel2(
     const uint64_t* __restrict__ slice_base, const uint32_t* __restrict__ slice_width,
     const uint32_t* __restrict__ split_mask, const uint32_t* __restrict__ rowid,
     const uint2* __restrict__ entry, uint64_t n_slices, float* __restrict__ live, float* snap,
@@ -382,7 +380,7 @@ __global__ void __launch_bounds__(256, UB_SGD_MIN_BLOCKS) sgd_epoch_kernel2(
         if (t == j) en = win[t];
       const uint32_t nneg = negatives_at(n, en.y, p.neg_rate);
       const uint64_t idx = base + (uint64_t)(ebase + j) * 32 + lane;
-      fired_edge<DIM, GEN>(cur, r, en.x, nneg, snap, p, alpha, idx, epoch, seed, seg_lo, seg_n);
+      fired_edge<DIM, GEN, NEG_BATCH>(cur, r, en.x, nneg, snap, p, alpha, idx, epoch, seed, seg_lo, seg_n);
     }
   }
   if (active) {
@@ -759,6 +757,20 @@ uint32_t pick_chunk(uint64_t n_edges) {
   return (uint32_t)std::min<uint64_t>(512, std::max<uint64_t>(16, c));
 }
 
+// Whether the epoch kernel takes the short-graph budget (2-D and 1-D embeddings): the
+// layout's warps (one per slice) fill at most two waves of the wide budget's resident warps
+// (SMs x 5 blocks x 8 warps).  UMAP_B200_SGD_SHORT=0 / 1 forces it.
+bool pick_short_epoch(uint64_t n_slices) {
+  if (const char* e = getenv("UMAP_B200_SGD_SHORT")) {
+    if (e[0] == '0') return false;
+    if (e[0] == '1') return true;
+  }
+  int dev = 0, sms = 0;
+  UB_CUDA(cudaGetDevice(&dev));
+  UB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  return n_slices <= 2ull * (uint64_t)std::max(sms, 1) * MINB_WIDE * 8;
+}
+
 void build_sgd_layout(const uint64_t* kept_ptr, const uint32_t* ktail, const double* keps, uint64_t n,
                       uint32_t chunk, SgdLayout& L, cudaStream_t s, const Segments* seg) {
   L.n_vertices = n;
@@ -829,6 +841,7 @@ void build_sgd_layout(const uint64_t* kept_ptr, const uint32_t* ktail, const dou
   UB_CUDA(cudaStreamSynchronize(s));
   L.split_tasks = 0;
   for (uint32_t v : h) L.split_tasks += __builtin_popcount(v);
+  L.short_epoch = pick_short_epoch(L.n_slices);
 }
 
 void export_edges(const uint64_t* indptr, const uint32_t* indices, const float* data, uint64_t n,
@@ -859,12 +872,14 @@ void sgd_epoch(const SgdLayout& L, float* live, float* snap, const SgdParams& p,
   const unsigned grid = grid_for(L.n_slices * 32, bt);
 #define UB_SGD_ARGS L.slice_base.p, L.slice_width.p, L.split_mask.p, L.rowid.p, L.entry.p, L.n_slices, live, snap, \
                     p, epoch, alpha
+#define UB_SGD_WIDE(D, GEN) sgd_epoch_kernel2<D, GEN, NB_WIDE, MINB_WIDE><<<grid, bt, 0, s>>>(UB_SGD_ARGS)
+#define UB_SGD_SHORT(D, GEN) sgd_epoch_kernel2<D, GEN, NB_SHORT, MINB_SHORT><<<grid, bt, 0, s>>>(UB_SGD_ARGS)
 #define UB_SGD_DISPATCH(GEN)                                                          \
   switch (p.dim) {                                                                    \
-    case 1: sgd_epoch_kernel2<1, GEN><<<grid, bt, 0, s>>>(UB_SGD_ARGS); break;        \
-    case 2: sgd_epoch_kernel2<2, GEN><<<grid, bt, 0, s>>>(UB_SGD_ARGS); break;        \
-    case 3: sgd_epoch_kernel2<3, GEN><<<grid, bt, 0, s>>>(UB_SGD_ARGS); break;        \
-    case 4: sgd_epoch_kernel2<4, GEN><<<grid, bt, 0, s>>>(UB_SGD_ARGS); break;        \
+    case 1: if (L.short_epoch) UB_SGD_SHORT(1, GEN); else UB_SGD_WIDE(1, GEN); break; \
+    case 2: if (L.short_epoch) UB_SGD_SHORT(2, GEN); else UB_SGD_WIDE(2, GEN); break; \
+    case 3: UB_SGD_WIDE(3, GEN); break;                                               \
+    case 4: UB_SGD_WIDE(4, GEN); break;                                               \
     default: sgd_epoch_anydim<GEN><<<grid, bt, 0, s>>>(UB_SGD_ARGS); break;           \
   }
   if (p.generic_metric) {
@@ -873,6 +888,8 @@ void sgd_epoch(const SgdLayout& L, float* live, float* snap, const SgdParams& p,
     UB_SGD_DISPATCH(false)
   }
 #undef UB_SGD_DISPATCH
+#undef UB_SGD_SHORT
+#undef UB_SGD_WIDE
 #undef UB_SGD_ARGS
   UB_LAUNCH_CHECK();
 }

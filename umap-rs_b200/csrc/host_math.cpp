@@ -5,7 +5,11 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
+#include <utility>
 
 #include "host_math.hpp"
 
@@ -43,8 +47,37 @@ std::string rust_f32(float x) {
   return neg ? "-" + out : out;
 }
 
-// umap/find_ab_params.rs:9-82: custom f32 gradient descent (not scipy curve_fit).
+// umap/find_ab_params.rs:9-82: custom f32 gradient descent (not scipy curve_fit).  The
+// 300,000 steps take a few milliseconds of host time and the result depends only on the two
+// arguments' bits, so results are memoised per (spread, min_dist) for the process.
+static void find_ab_params_uncached(float spread, float min_dist, float* a_out, float* b_out);
+
 void find_ab_params(float spread, float min_dist, float* a_out, float* b_out) {
+  static std::mutex mu;
+  static std::map<uint64_t, std::pair<float, float>> memo;
+  uint32_t sb, mb;
+  std::memcpy(&sb, &spread, 4);
+  std::memcpy(&mb, &min_dist, 4);
+  const uint64_t key = (uint64_t)sb << 32 | mb;
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = memo.find(key);
+    if (it != memo.end()) {
+      *a_out = it->second.first;
+      *b_out = it->second.second;
+      return;
+    }
+  }
+  float a = 0.0f, b = 0.0f;
+  find_ab_params_uncached(spread, min_dist, &a, &b);
+  std::lock_guard<std::mutex> lock(mu);
+  if (memo.size() >= 256) memo.clear();
+  memo[key] = {a, b};
+  *a_out = a;
+  *b_out = b;
+}
+
+static void find_ab_params_uncached(float spread, float min_dist, float* a_out, float* b_out) {
   const int n_points = 300;
   float xv[300], yv[300];
   for (int i = 0; i < n_points; ++i) xv[i] = ((spread * 3.0f) * (float)i) / ((float)n_points - 1.0f);

@@ -718,9 +718,19 @@ struct AdamArgs {
   bf16* w3b;
 };
 
+// Sum of the K-split slices, added in slice order; the loads of eight slices are issued
+// before their additions (the slice count is a power of two, a multiple of 8 above 8).
 __device__ __forceinline__ float slice_sum(const float* part, int ks, int64_t stride, int64_t k) {
   float s = 0.0f;
-  for (int z = 0; z < ks; ++z) s += part[(int64_t)z * stride + k];
+  int z = 0;
+  for (; z + 8 <= ks; z += 8) {
+    float v[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) v[u] = part[(int64_t)(z + u) * stride + k];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) s += v[u];
+  }
+  for (; z < ks; ++z) s += part[(int64_t)z * stride + k];
   return s;
 }
 

@@ -250,8 +250,9 @@ __global__ void __launch_bounds__(GT) umma_gemm_kernel(const bf16* __restrict__ 
     uint8_t* sA = smem + st * STAGE;
     uint8_t* sB = sA + GM * KC * 2;
     if (GATHER) {
-      // consecutive threads take consecutive rows: the transposed copy is written coalesced
-#pragma unroll 2
+      // consecutive threads take consecutive rows: the transposed copy is written coalesced;
+      // a thread's four items are loaded together
+#pragma unroll 4
       for (int v = tid; v < GM * (KC / 8); v += GT) {
         const int r = v & (GM - 1), c8 = v / GM;
         const int64_t b = m0 + r;
@@ -261,8 +262,14 @@ __global__ void __launch_bounds__(GT) umma_gemm_kernel(const bf16* __restrict__ 
         const float4 x0 = __ldg(xp), x1 = __ldg(xp + 1);
         float f[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
         if (ga.scale) {
+          // shift / scale hold in_dim floats from a 256-byte aligned allocation; k0 % 8 == 0
+          const float4* sp = reinterpret_cast<const float4*>(ga.shift + k0);
+          const float4* cp = reinterpret_cast<const float4*>(ga.scale + k0);
+          const float4 s0 = __ldg(sp), s1 = __ldg(sp + 1), c0 = __ldg(cp), c1 = __ldg(cp + 1);
+          const float sh[8] = {s0.x, s0.y, s0.z, s0.w, s1.x, s1.y, s1.z, s1.w};
+          const float sc[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
 #pragma unroll
-          for (int e = 0; e < 8; ++e) f[e] = (f[e] - __ldg(ga.shift + k0 + e)) * __ldg(ga.scale + k0 + e);
+          for (int e = 0; e < 8; ++e) f[e] = (f[e] - sh[e]) * sc[e];
         }
         uint32_t pk[4];
 #pragma unroll

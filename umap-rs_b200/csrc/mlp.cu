@@ -826,15 +826,26 @@ __global__ void column_stats_kernel(const float* __restrict__ X, int64_t n, int 
 
 inline unsigned grid_for(int64_t n, unsigned bt) { return (unsigned)((n + bt - 1) / bt); }
 
-// Sort keys of one epoch's shuffle: splitmix64 finaliser of (seed, epoch, row), top 32 bits.
-__global__ void shuffle_keys_kernel(uint32_t* __restrict__ keys, int64_t n, uint64_t seed, uint32_t epoch) {
+// Sort keys of the shuffles of epochs e0 .. e0 + total / n - 1 (entry q * n + row): the
+// splitmix64 finaliser of (seed, epoch, row), top 32 bits; with eb > 0 the epoch's offset q
+// in the group takes the key's top eb bits and the hash's top 32 - eb bits follow.
+__global__ void shuffle_keys_kernel(uint32_t* __restrict__ keys, int64_t n, uint64_t seed, uint32_t e0,
+                                    int64_t total, int eb) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  uint64_t z = seed * 0x9E3779B97F4A7C15ull + ((uint64_t)epoch << 32) + (uint64_t)i + 0x632BE59BD9B4E019ull;
+  if (i >= total) return;
+  const int64_t q = i / n, r = i - q * n;
+  uint64_t z = seed * 0x9E3779B97F4A7C15ull + ((uint64_t)(e0 + (uint32_t)q) << 32) + (uint64_t)r + 0x632BE59BD9B4E019ull;
   z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
   z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
   z ^= z >> 31;
-  keys[i] = (uint32_t)(z >> 32);
+  const uint32_t h = (uint32_t)(z >> 32);
+  keys[i] = eb ? ((uint32_t)q << (32 - eb)) | (h >> eb) : h;
+}
+
+// Sorted positions q * n + row of a group of epochs back to rows.
+__global__ void perm_rows_kernel(uint32_t* __restrict__ p, int64_t total, uint32_t n) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < total) p[i] %= n;
 }
 
 bool graphs_enabled() {
@@ -1214,16 +1225,25 @@ void Mlp::train(const float* X, const float* Y, int64_t n, int epochs, int64_t b
   if (epochs == 0) return;
   m.ensure(batch, true);
   m.ensure_slices(batch);
-  // Shuffles on the device: epoch e orders the rows by a 32-bit hash of (seed, e, row)
-  // (stable radix sort, so equal hashes keep row order); the first steps * batch rows of
-  // each epoch's order are its batches.
+  // Shuffles on the device: epoch e orders the rows by a hash of (seed, e, row) (stable radix
+  // sort, so equal hashes keep row order); the first steps * batch rows of each epoch's
+  // order are its batches.  Groups of 2^eb epochs share one sort: the key of (epoch
+  // e0 + q, row) is q in the top eb bits over the hash's top 32 - eb bits.
   const int64_t per_epoch = steps * batch;
-  DevBuf<uint32_t> hkeys((uint64_t)n, s), hsorted((uint64_t)n, s), dperm((uint64_t)epochs * n, s);
+  int eb = 0;
+  while (eb < 5 && (1 << eb) < epochs && ((int64_t)2 << eb) * n <= (1ll << 26)) ++eb;
+  const int group = 1 << eb;
+  const int64_t gmax = (int64_t)std::min(group, epochs) * n;
+  DevBuf<uint32_t> hkeys((uint64_t)gmax, s), hsorted((uint64_t)gmax, s), dperm((uint64_t)epochs * n, s);
   DevBuf<uint32_t> cur(per_epoch, s);
-  for (int e = 0; e < epochs; ++e) {
-    shuffle_keys_kernel<<<grid_for(n, 256), 256, 0, s>>>(hkeys.p, n, seed, (uint32_t)e);
+  for (int e0 = 0; e0 < epochs; e0 += group) {
+    const int64_t total = (int64_t)std::min(group, epochs - e0) * n;
+    shuffle_keys_kernel<<<grid_for(total, 256), 256, 0, s>>>(hkeys.p, n, seed, (uint32_t)e0, total, eb);
     UB_LAUNCH_CHECK();
-    radix_sort_pairs(hkeys.p, nullptr, hsorted.p, dperm.p + (int64_t)e * n, (uint64_t)n, 32, s);
+    uint32_t* dst = dperm.p + (int64_t)e0 * n;
+    radix_sort_pairs(hkeys.p, nullptr, hsorted.p, dst, (uint64_t)total, 32, s);
+    perm_rows_kernel<<<grid_for(total, 256), 256, 0, s>>>(dst, total, (uint32_t)n);
+    UB_LAUNCH_CHECK();
   }
   DevBuf<float> dloss(epochs, s);
   UB_CUDA(cudaMemsetAsync(m.g.p, 0, m.P * 4, s));

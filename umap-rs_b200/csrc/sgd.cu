@@ -3,7 +3,10 @@
 //
 // Layout.  The kept edges of the symmetric graph are grouped by head row and cut into tasks
 // of at most `chunk` edges (see SgdLayout).  A warp owns a slice of 32 tasks and a lane owns
-// one task, keeping the head row's live embedding in registers.  The reference writes a
+// one task, keeping the head row's live embedding in registers.  A slice's entries are lane
+// major: task l's entries are contiguous at base + l * width (width = the slice's longest
+// task rounded up to 4 entries, padding never fires), so a lane's 4-entry window is one
+// aligned 32-byte sector whatever the other lanes' progress.  The reference writes a
 // head row only from edges whose head it is (optimize_layout_euclidean.rs:281-306, :338),
 // so a task that is a whole row reproduces the reference's sequential per-row order with
 // no lost head updates; the rare long rows (kNN hubs) are split so that one row cannot
@@ -355,15 +358,19 @@ __global__ void __launch_bounds__(256, MINB) sgd_epoch_kernel2(
   for (int d = 0; d < DIM; ++d) start[d] = cur[d];
   const uint32_t n = epoch;
   const uint64_t seed = p.seed;
+  static_assert(W % 4 == 0, "windows are whole 4-entry sectors");
+  const uint2* lent = entry + base + (uint64_t)lane * width;  // this lane's entries
   uint2 win[W];
   uint32_t mask = 0, ew = 0, ebase = 0;
   for (;;) {
     while (mask == 0 && ew < width) {
       ebase = ew;
+      // width is a multiple of 4: the window's sectors lie inside the lane's entries
 #pragma unroll
-      for (int j = 0; j < W; ++j) {
-        const uint32_t e = ew + j;
-        win[j] = e < width ? __ldg(entry + base + (uint64_t)e * 32 + lane) : make_uint2(0u, 0u);
+      for (int j = 0; j < W; j += 2) {
+        const uint4 v = __ldg(reinterpret_cast<const uint4*>(lent + ew + j));
+        win[j] = make_uint2(v.x, v.y);
+        win[j + 1] = make_uint2(v.z, v.w);
       }
 #pragma unroll
       for (int j = 0; j < W; ++j)
@@ -379,7 +386,7 @@ __global__ void __launch_bounds__(256, MINB) sgd_epoch_kernel2(
       for (int t = 1; t < W; ++t)
         if (t == j) en = win[t];
       const uint32_t nneg = negatives_at(n, en.y, p.neg_rate);
-      const uint64_t idx = base + (uint64_t)(ebase + j) * 32 + lane;
+      const uint64_t idx = base + (uint64_t)lane * width + ebase + j;
       fired_edge<DIM, GEN, NEG_BATCH>(cur, r, en.x, nneg, snap, p, alpha, idx, epoch, seed, seg_lo, seg_n);
     }
   }
@@ -426,7 +433,7 @@ __global__ void __launch_bounds__(256) sgd_epoch_anydim(
     else cur[d] += v;
   };
   for (uint32_t e = 0; e < width; ++e) {
-    const uint64_t idx = base + (uint64_t)e * 32 + lane;
+    const uint64_t idx = base + (uint64_t)lane * width + e;
     const uint2 en = __ldcs(entry + idx);
     if (!fires_at(n, en.y)) continue;
     float* oth = snap + (uint64_t)en.x * dim;
@@ -542,6 +549,7 @@ __global__ void slice_meta_kernel(const uint32_t* __restrict__ perm, const uint3
   // slice width = longest task of the slice (instance-major order: the max over lanes)
   uint32_t len = q < T ? chunk - (skey[q] & len_mask) : 0u;
   for (int o = 16; o > 0; o >>= 1) len = max(len, __shfl_xor_sync(0xFFFFFFFFu, len, o));
+  len = (len + 3u) & ~3u;  // whole 4-entry (32-byte) sectors per lane
   if ((q & 31) == 0) {
     width[q >> 5] = len;
     split_mask[q >> 5] = bits;
@@ -565,9 +573,9 @@ __global__ void slice_fill_kernel(const uint32_t* __restrict__ ktail, const doub
     const uint64_t st = tstart[perm[q]];
     const uint32_t len = chunk - (skey[q] & len_mask);
     for (; e < len; ++e)
-      entry[base + (uint64_t)e * 32 + lane] = make_uint2(ktail[st + e], q_minus_1(keps[st + e]));
+      entry[base + (uint64_t)lane * wd + e] = make_uint2(ktail[st + e], q_minus_1(keps[st + e]));
   }
-  for (; e < wd; ++e) entry[base + (uint64_t)e * 32 + lane] = make_uint2(0u, 0u);
+  for (; e < wd; ++e) entry[base + (uint64_t)lane * wd + e] = make_uint2(0u, 0u);
 }
 
 __global__ void head_from_ptr_kernel(const uint64_t* __restrict__ kptr, uint64_t n, uint32_t* __restrict__ head) {

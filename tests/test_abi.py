@@ -56,6 +56,33 @@ def test_find_ab_params_bit_identical_to_oracle(ub, oracle, spread, min_dist):
     assert ub.find_ab_params(spread, min_dist) == oracle.find_ab_params(spread, min_dist)
 
 
+def test_find_ab_params_memo_concurrent(ub, oracle):
+    """The library memoises (a, b) per (spread, min_dist) for the process: concurrent callers
+    (ctypes drops the GIL) with a mix of cached and new arguments all get the oracle's bits."""
+    import threading
+    args = [(1.0, 0.1), (1.5, 0.3), (0.7, 0.05), (2.0, 0.5), (1.25, 0.0)]
+    want = {a: oracle.find_ab_params(*a) for a in args}
+    got, errors = [], []
+
+    def worker(k):
+        try:
+            for i in range(12):
+                a = args[(k + i) % len(args)]
+                got.append((a, ub.find_ab_params(*a)))
+        except Exception as e:  # surfaced below
+            errors.append(e)
+
+    threads = [threading.Thread(target=worker, args=(k,)) for k in range(8)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    assert not errors, errors
+    assert len(got) == 8 * 12
+    for a, ab in got:
+        assert ab == want[a], (a, ab, want[a])
+
+
 def _learn(ub, cfg, n, rows, cols):
     idx = np.zeros((rows, cols), np.uint32)
     dist = np.zeros((rows, cols), np.float32)

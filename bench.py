@@ -82,16 +82,32 @@ def peak(key):
     return (float(v), "measured") if v else (FALLBACK_PEAKS[key], "fallback")
 
 
-def traffic_per_epoch():
-    """DRAM bytes per SGD launch from the committed ncu summary (None if absent)."""
+def _profile_value(key):
+    """A `key: value` line of the committed ncu summary of the SGD epoch (None if absent)."""
     p = os.path.join(ROOT, "profiles", "sgd_epoch_2m.md")
     try:
         for line in open(p):
-            if line.startswith("traffic_bytes_per_launch:"):
+            if line.startswith(key + ":"):
                 return float(line.split(":", 1)[1].split()[0])
     except OSError:
         pass
     return None
+
+
+def traffic_per_epoch():
+    """DRAM bytes per SGD launch from the committed ncu summary (None if absent)."""
+    return _profile_value("traffic_bytes_per_launch")
+
+
+def l2_counters():
+    """The SGD epoch's L2 and issue figures from the same ncu capture: the embedding of the
+    2M workload is L2-resident, so these, not DRAM, show how close the kernel runs to a limit."""
+    keys = ("l2_throughput_pct", "l2_hit_rate_pct", "issue_active_pct")
+    vals = {k: _profile_value(k) for k in keys}
+    if all(v is None for v in vals.values()):
+        return None
+    vals["source"] = "ncu --set full of one epoch (profiles/sgd_epoch_2m.md)"
+    return vals
 
 
 class _Sampler:
@@ -529,7 +545,7 @@ def run_swiss_roll(a):
                        "l2": "embedding 800 MB and edge slices exceed L2"},
             "sgd_ms_per_fit": sgd_ms, "sgd_edge_updates_per_s": F_tot / (sgd_ms / 1e3),
             "graph_and_setup_ms": ms_step - sgd_ms,
-            "roofline": {"bound": "hbm", "kernel": "sgd_epoch_kernel2<2>", "achieved": achieved, "peak": hbm,
+            "roofline": {"bound": "hbm", "kernel": "sgd_epoch_kernel2<2, false, 4, 5>", "achieved": achieved, "peak": hbm,
                          "unit": "GB/s", "frac": achieved / hbm, "peak_source": hbm_src, "traffic": swiss_traffic(E),
                          "traffic_note": "DRAM bytes of one epoch-20 launch captured at 20M points "
                                          "(profiles/sgd_epoch_swiss_roll_20m.md), scaled by kept edges",
@@ -820,10 +836,10 @@ def main():
         "sgd_edge_updates_per_s": F_tot / (float(np.median(sgd_ms)) / 1e3),
         "e2e": {"value": F_tot / (e2e_step / 1e3), "unit": "edge-updates/s", "ms_per_step": e2e_step,
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-        "roofline": {"bound": "hbm", "kernel": "sgd_epoch_kernel2<2>", "achieved": achieved,
+        "roofline": {"bound": "hbm", "kernel": "sgd_epoch_kernel2<2, false, 4, 5>", "achieved": achieved,
                      "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "peak_source": peak_src,
                      "traffic": tr, "algorithmic_bytes_per_launch": alg_bytes / a.epochs,
-                     "avg_launch_ms": sgd_kernel_ms},
+                     "avg_launch_ms": sgd_kernel_ms, "l2": l2_counters()},
         "gpu_launches": launches,
         "clocks": clocks,
     }

@@ -227,8 +227,9 @@ def test_nan_rows_for_disconnected_vertices(ub, oracle):
 def test_embedding_quality_matches_oracle(ub, oracle, gauss10k, monkeypatch):
     """C0 workload (10k points, 200 epochs): GPU recall within 0.01 and fuzzy CE within 1%
     of the oracle's (mean over 3 oracle seeds; the oracle's own spread is reported).  The
-    epoch kernel runs with both register budgets: the short-graph one this size selects and
-    the large-graph one, forced."""
+    epoch kernel runs with both register budgets and both entry orders: the short-graph
+    budget with lane-major entries this size selects, and the large-graph budget with the
+    lane-interleaved entries of DRAM-bound sizes, forced."""
     from umap_b200 import quality as Q
     idx, dist, init = gauss10k
     cfg = ub.UmapConfig()
@@ -253,9 +254,12 @@ def test_embedding_quality_matches_oracle(ub, oracle, gauss10k, monkeypatch):
         ce_o.append(Q.fuzzy_cross_entropy(emb, head, tail, w, a, b))
     res = []
     for short, seed in (("1", 1), ("1", 2), ("0", 1), ("0", 2)):
-        monkeypatch.setenv("UMAP_B200_SGD_SHORT", short)  # read when the optimizer is built
+        # read when the optimizer is built
+        monkeypatch.setenv("UMAP_B200_SGD_SHORT", short)
+        monkeypatch.setenv("UMAP_B200_SGD_LANE_MAJOR", short)
         opt = ub.Optimizer(ub.Umap(cfg).learn_manifold(10_000, idx, dist), init, 200, cfg)
         monkeypatch.delenv("UMAP_B200_SGD_SHORT")
+        monkeypatch.delenv("UMAP_B200_SGD_LANE_MAJOR")
         opt.set_seed(seed)
         opt.step_epochs(200)
         emb = opt.embedding()

@@ -4,9 +4,11 @@
 // Layout.  The kept edges of the symmetric graph are grouped by head row and cut into tasks
 // of at most `chunk` edges (see SgdLayout).  A warp owns a slice of 32 tasks and a lane owns
 // one task, keeping the head row's live embedding in registers.  A slice's entries are lane
-// major: task l's entries are contiguous at base + l * width (width = the slice's longest
-// task rounded up to 4 entries, padding never fires), so a lane's 4-entry window is one
-// aligned 32-byte sector whatever the other lanes' progress.  The reference writes a
+// major when the embedding the epoch touches stays in L2: task l's entries are contiguous at
+// base + l * width (width = the slice's longest task rounded up to 4 entries, padding never
+// fires), so a lane's 4-entry window is one aligned 32-byte sector whatever the other lanes'
+// progress.  Otherwise (DRAM-bound sizes) entry e of task l sits at base + 32 e + l, so a
+// warp's loads cover whole 256-byte rows (see pick_lane_major).  The reference writes a
 // head row only from edges whose head it is (optimize_layout_euclidean.rs:281-306, :338),
 // so a task that is a whole row reproduces the reference's sequential per-row order with
 // no lost head updates; the rare long rows (kNN hubs) are split so that one row cannot
@@ -327,7 +329,7 @@ __device__ __forceinline__ void fired_edge(float (&cur)[DIM], uint32_t r, uint32
 #ifndef UB_SGD2_W
 #define UB_SGD2_W 4
 #endif
-template <int DIM, bool GEN, int NEG_BATCH, int MINB>
+template <int DIM, bool GEN, int NEG_BATCH, int MINB, bool LM>
 __global__ void __launch_bounds__(256, MINB) sgd_epoch_kernel2(
     const uint64_t* __restrict__ slice_base, const uint32_t* __restrict__ slice_width,
     const uint32_t* __restrict__ split_mask, const uint32_t* __restrict__ rowid,
@@ -359,18 +361,27 @@ __global__ void __launch_bounds__(256, MINB) sgd_epoch_kernel2(
   const uint32_t n = epoch;
   const uint64_t seed = p.seed;
   static_assert(W % 4 == 0, "windows are whole 4-entry sectors");
-  const uint2* lent = entry + base + (uint64_t)lane * width;  // this lane's entries
+  // this lane's entries: contiguous (lane major) or every 32nd (interleaved)
+  const uint2* lent = LM ? entry + base + (uint64_t)lane * width : entry + base + lane;
   uint2 win[W];
   uint32_t mask = 0, ew = 0, ebase = 0;
   for (;;) {
     while (mask == 0 && ew < width) {
       ebase = ew;
-      // width is a multiple of 4: the window's sectors lie inside the lane's entries
+      if (LM) {
+        // width is a multiple of 4: the window's sectors lie inside the lane's entries
 #pragma unroll
-      for (int j = 0; j < W; j += 2) {
-        const uint4 v = __ldg(reinterpret_cast<const uint4*>(lent + ew + j));
-        win[j] = make_uint2(v.x, v.y);
-        win[j + 1] = make_uint2(v.z, v.w);
+        for (int j = 0; j < W; j += 2) {
+          const uint4 v = __ldg(reinterpret_cast<const uint4*>(lent + ew + j));
+          win[j] = make_uint2(v.x, v.y);
+          win[j + 1] = make_uint2(v.z, v.w);
+        }
+      } else {
+#pragma unroll
+        for (int j = 0; j < W; ++j) {
+          const uint32_t e = ew + j;
+          win[j] = e < width ? __ldg(lent + (uint64_t)e * 32) : make_uint2(0u, 0u);
+        }
       }
 #pragma unroll
       for (int j = 0; j < W; ++j)
@@ -386,7 +397,7 @@ __global__ void __launch_bounds__(256, MINB) sgd_epoch_kernel2(
       for (int t = 1; t < W; ++t)
         if (t == j) en = win[t];
       const uint32_t nneg = negatives_at(n, en.y, p.neg_rate);
-      const uint64_t idx = base + (uint64_t)lane * width + ebase + j;
+      const uint64_t idx = LM ? base + (uint64_t)lane * width + ebase + j : base + (uint64_t)(ebase + j) * 32 + lane;
       fired_edge<DIM, GEN, NEG_BATCH>(cur, r, en.x, nneg, snap, p, alpha, idx, epoch, seed, seg_lo, seg_n);
     }
   }
@@ -408,7 +419,7 @@ __global__ void __launch_bounds__(256) sgd_epoch_anydim(
     const uint64_t* __restrict__ slice_base, const uint32_t* __restrict__ slice_width,
     const uint32_t* __restrict__ split_mask, const uint32_t* __restrict__ rowid,
     const uint2* __restrict__ entry, uint64_t n_slices, float* __restrict__ live, float* snap,
-    SgdParams p, uint32_t epoch, float alpha) {
+    SgdParams p, uint32_t epoch, float alpha, bool lane_major) {
   const uint64_t slice = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t lane = threadIdx.x & 31;
   if (slice >= n_slices) return;
@@ -433,7 +444,7 @@ __global__ void __launch_bounds__(256) sgd_epoch_anydim(
     else cur[d] += v;
   };
   for (uint32_t e = 0; e < width; ++e) {
-    const uint64_t idx = base + (uint64_t)lane * width + e;
+    const uint64_t idx = lane_major ? base + (uint64_t)lane * width + e : base + (uint64_t)e * 32 + lane;
     const uint2 en = __ldcs(entry + idx);
     if (!fires_at(n, en.y)) continue;
     float* oth = snap + (uint64_t)en.x * dim;
@@ -539,7 +550,7 @@ __global__ void task_fill_kernel(const uint64_t* __restrict__ kptr, const uint32
 
 __global__ void slice_meta_kernel(const uint32_t* __restrict__ perm, const uint32_t* __restrict__ trow,
                                   const uint32_t* __restrict__ skey, uint64_t T, uint64_t n_slices,
-                                  uint32_t chunk, uint32_t len_mask, uint32_t* __restrict__ width,
+                                  uint32_t chunk, uint32_t len_mask, bool lane_major, uint32_t* __restrict__ width,
                                   uint32_t* __restrict__ rowid, uint32_t* __restrict__ split_mask) {
   const uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= n_slices * 32) return;
@@ -549,7 +560,7 @@ __global__ void slice_meta_kernel(const uint32_t* __restrict__ perm, const uint3
   // slice width = longest task of the slice (instance-major order: the max over lanes)
   uint32_t len = q < T ? chunk - (skey[q] & len_mask) : 0u;
   for (int o = 16; o > 0; o >>= 1) len = max(len, __shfl_xor_sync(0xFFFFFFFFu, len, o));
-  len = (len + 3u) & ~3u;  // whole 4-entry (32-byte) sectors per lane
+  if (lane_major) len = (len + 3u) & ~3u;  // whole 4-entry (32-byte) sectors per lane
   if ((q & 31) == 0) {
     width[q >> 5] = len;
     split_mask[q >> 5] = bits;
@@ -560,7 +571,7 @@ __global__ void slice_fill_kernel(const uint32_t* __restrict__ ktail, const doub
                                   const uint32_t* __restrict__ perm, const uint64_t* __restrict__ tstart,
                                   const uint32_t* __restrict__ skey, uint64_t T, uint32_t chunk,
                                   uint32_t len_mask, const uint64_t* __restrict__ wscan,
-                                  const uint32_t* __restrict__ width, uint64_t n_slices,
+                                  const uint32_t* __restrict__ width, uint64_t n_slices, bool lane_major,
                                   uint2* __restrict__ entry) {
   const uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= n_slices * 32) return;
@@ -573,9 +584,11 @@ __global__ void slice_fill_kernel(const uint32_t* __restrict__ ktail, const doub
     const uint64_t st = tstart[perm[q]];
     const uint32_t len = chunk - (skey[q] & len_mask);
     for (; e < len; ++e)
-      entry[base + (uint64_t)lane * wd + e] = make_uint2(ktail[st + e], q_minus_1(keps[st + e]));
+      entry[lane_major ? base + (uint64_t)lane * wd + e : base + (uint64_t)e * 32 + lane] =
+          make_uint2(ktail[st + e], q_minus_1(keps[st + e]));
   }
-  for (; e < wd; ++e) entry[base + (uint64_t)lane * wd + e] = make_uint2(0u, 0u);
+  for (; e < wd; ++e)
+    entry[lane_major ? base + (uint64_t)lane * wd + e : base + (uint64_t)e * 32 + lane] = make_uint2(0u, 0u);
 }
 
 __global__ void head_from_ptr_kernel(const uint64_t* __restrict__ kptr, uint64_t n, uint32_t* __restrict__ head) {
@@ -779,9 +792,24 @@ bool pick_short_epoch(uint64_t n_slices) {
   return n_slices <= 2ull * (uint64_t)std::max(sms, 1) * MINB_WIDE * 8;
 }
 
+// Entry order of the layout.  Lane major (a lane's window is one 32-byte sector) wins while
+// the rows the negatives and tails reach stay in L2: a plain fit whose 2-D embedding (live +
+// snapshot, 16 B per vertex) is at most 64 MB, and batched instances, whose instance-major
+// task order keeps the instances in flight in L2.  Beyond that every access goes to DRAM,
+// where the interleaved order's whole 256-byte rows per warp use DRAM bursts better than
+// 32-byte windows.  UMAP_B200_SGD_LANE_MAJOR=0 / 1 forces either.
+bool pick_lane_major(uint64_t n, bool segmented) {
+  if (const char* e = getenv("UMAP_B200_SGD_LANE_MAJOR")) {
+    if (e[0] == '0') return false;
+    if (e[0] == '1') return true;
+  }
+  return segmented || n <= 4000000ull;
+}
+
 void build_sgd_layout(const uint64_t* kept_ptr, const uint32_t* ktail, const double* keps, uint64_t n,
                       uint32_t chunk, SgdLayout& L, cudaStream_t s, const Segments* seg) {
   L.n_vertices = n;
+  L.lane_major = pick_lane_major(n, seg != nullptr);
   uint64_t n_edges = 0;
   UB_CUDA(cudaMemcpyAsync(&n_edges, kept_ptr + n, 8, cudaMemcpyDeviceToHost, s));
   UB_CUDA(cudaStreamSynchronize(s));
@@ -822,8 +850,9 @@ void build_sgd_layout(const uint64_t* kept_ptr, const uint32_t* ktail, const dou
   L.slice_base.alloc(L.n_slices + 1, s);
   if (L.n_slices) {
     slice_meta_kernel<<<grid_for(L.n_slices * 32, 256), 256, 0, s>>>(perm.p, trow.p, skey.p, T, L.n_slices,
-                                                                        L.chunk, len_mask, L.slice_width.p,
-                                                                        L.rowid.p, L.split_mask.p);
+                                                                        L.chunk, len_mask, L.lane_major,
+                                                                        L.slice_width.p, L.rowid.p,
+                                                                        L.split_mask.p);
     UB_LAUNCH_CHECK();
   }
   DevBuf<uint64_t> wscan(L.n_slices + 1, s);
@@ -836,7 +865,8 @@ void build_sgd_layout(const uint64_t* kept_ptr, const uint32_t* ktail, const dou
   if (L.n_slices) {
     slice_fill_kernel<<<grid_for(L.n_slices * 32, 256), 256, 0, s>>>(ktail, keps, perm.p, tstart.p, skey.p, T,
                                                                         L.chunk, len_mask, wscan.p,
-                                                                        L.slice_width.p, L.n_slices, L.entry.p);
+                                                                        L.slice_width.p, L.n_slices,
+                                                                        L.lane_major, L.entry.p);
     UB_LAUNCH_CHECK();
   }
   // slice_base = 32 * wscan (entries, not widths)
@@ -880,22 +910,25 @@ void sgd_epoch(const SgdLayout& L, float* live, float* snap, const SgdParams& p,
   const unsigned grid = grid_for(L.n_slices * 32, bt);
 #define UB_SGD_ARGS L.slice_base.p, L.slice_width.p, L.split_mask.p, L.rowid.p, L.entry.p, L.n_slices, live, snap, \
                     p, epoch, alpha
-#define UB_SGD_WIDE(D, GEN) sgd_epoch_kernel2<D, GEN, NB_WIDE, MINB_WIDE><<<grid, bt, 0, s>>>(UB_SGD_ARGS)
-#define UB_SGD_SHORT(D, GEN) sgd_epoch_kernel2<D, GEN, NB_SHORT, MINB_SHORT><<<grid, bt, 0, s>>>(UB_SGD_ARGS)
+#define UB_SGD_WIDE(D, GEN)                                                                   \
+  if (L.lane_major) sgd_epoch_kernel2<D, GEN, NB_WIDE, MINB_WIDE, true><<<grid, bt, 0, s>>>(UB_SGD_ARGS); \
+  else sgd_epoch_kernel2<D, GEN, NB_WIDE, MINB_WIDE, false><<<grid, bt, 0, s>>>(UB_SGD_ARGS)
+// short graphs always have lane-major entries (pick_lane_major)
+#define UB_SGD_SHORT(D, GEN) sgd_epoch_kernel2<D, GEN, NB_SHORT, MINB_SHORT, true><<<grid, bt, 0, s>>>(UB_SGD_ARGS)
 #define UB_SGD_DISPATCH(GEN, SHORT)                                                   \
   switch (p.dim) {                                                                    \
     case 1: if (SHORT) UB_SGD_SHORT(1, GEN); else UB_SGD_WIDE(1, GEN); break;         \
     case 2: if (SHORT) UB_SGD_SHORT(2, GEN); else UB_SGD_WIDE(2, GEN); break;         \
     case 3: UB_SGD_WIDE(3, GEN); break;                                               \
     case 4: UB_SGD_WIDE(4, GEN); break;                                               \
-    default: sgd_epoch_anydim<GEN><<<grid, bt, 0, s>>>(UB_SGD_ARGS); break;           \
+    default: sgd_epoch_anydim<GEN><<<grid, bt, 0, s>>>(UB_SGD_ARGS, L.lane_major); break; \
   }
   // The generic-metric rule keeps the large-graph budget at every size (its statistical
   // parity with the reference's sequential loop was established with it).
   if (p.generic_metric) {
     UB_SGD_DISPATCH(true, false)
   } else {
-    UB_SGD_DISPATCH(false, L.short_epoch)
+    UB_SGD_DISPATCH(false, L.short_epoch && L.lane_major)
   }
 #undef UB_SGD_DISPATCH
 #undef UB_SGD_SHORT

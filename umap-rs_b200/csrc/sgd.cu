@@ -13,8 +13,8 @@
 // so a task that is a whole row reproduces the reference's sequential per-row order with
 // no lost head updates; the rare long rows (kNN hubs) are split so that one row cannot
 // serialise an epoch, and each partial task merges its head delta with an atomic add.
-// Tail moves and negative samples touch the per-call snapshot buffer with racy loads and
-// stores, as the reference does.
+// Tail moves (fire-and-forget atomic adds, see sub_row) and negative samples (racy loads)
+// touch the per-call snapshot buffer, where the reference reads and writes it racily.
 //
 // Schedule.  The reference keeps four f64 arrays per edge (optimizer.rs:33-43).  Here one
 // u32 per edge holds Q = ceil(2^32 / epochs_per_sample) and the state is recomputed in

@@ -294,7 +294,8 @@ int umap_smooth_knn_dist_device(const float* dev_dists, uint64_t n, uint64_t k,
                                 float* dev_sigmas, float* dev_rhos);
 /* Stable LSD radix sort of (u32 key, u32 value) pairs by key bits [0, end_bit): the
  * transpose step that replaces build_csc_structure (fuzzy_simplicial_set.rs:310-370).
- * dev_values_in may be NULL (values = 0..n-1). */
+ * dev_values_in may be NULL (values = 0..n-1).  Neither output may overlap an input or the
+ * other output (UMAP_ERR_INVALID_ARGUMENT). */
 int umap_radix_sort_pairs_device(const uint32_t* dev_keys_in, const uint32_t* dev_values_in,
                                  uint32_t* dev_keys_out, uint32_t* dev_values_out,
                                  uint64_t n, int end_bit);
@@ -304,13 +305,19 @@ int umap_radix_sort_pairs_device(const uint32_t* dev_keys_in, const uint32_t* de
  * memory when they sort: a host application whose allocator owns the whole GPU heap, or a
  * latency-critical loop that must not enter the CUDA allocator.  It performs no cudaMalloc
  * / cudaFree and no allocating library call: its scratch is a static device array of about
- * 9 MiB that every GPU loading this library holds until exit.  At most
- * umap_radix_sort_noalloc_max_pairs() pairs (1,048,576); larger n returns
- * UMAP_ERR_INVALID_ARGUMENT.  The first call on a device looks up the array's device
- * address (cudaGetSymbolAddress) with that device current; make that first call before
- * any stream capture.  Work is queued on `stream` (NULL = the default stream) and the call
- * returns when it is done.  All calls share the array: calls whose GPU work overlaps (on
- * different streams or threads) race on it and must be serialised by the caller. */
+ * 9 MiB.  The CUDA runtime places that array on a GPU when it loads the library's sort
+ * module there (lazily, by default: at the module's first kernel launch or symbol lookup on
+ * that device), and the GPU then holds it until the process exits.  That load is itself a
+ * device allocation, so a caller that later reserves the whole heap should first call this
+ * entry point once per device with n = 0 (buffers may then be NULL): that call loads the
+ * module, looks up the array's device address (cudaGetSymbolAddress) with that device
+ * current, and queues no GPU work.  Make that first call before any stream capture.
+ * At most umap_radix_sort_noalloc_max_pairs() pairs (1,048,576); larger n returns
+ * UMAP_ERR_INVALID_ARGUMENT, as do outputs that overlap an input or each other.  Work is
+ * queued on `stream` (NULL = the default stream), and every call synchronises that stream
+ * (cudaStreamSynchronize) before it returns.  All calls share the array: calls whose GPU
+ * work overlaps (on different streams or threads) race on it and must be serialised by the
+ * caller. */
 int umap_radix_sort_pairs_device_noalloc(const uint32_t* dev_keys_in, const uint32_t* dev_values_in,
                                          uint32_t* dev_keys_out, uint32_t* dev_values_out,
                                          uint64_t n, int end_bit, void* stream);

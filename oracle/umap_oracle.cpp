@@ -315,6 +315,17 @@ Csr build_membership_csr(uint64_t n, uint64_t k, const uint32_t* idx, const floa
   return out;
 }
 
+// fuzzy_simplicial_set.rs:291 passes the sorted rows to sprs 0.11's CsMatI::new, which
+// unwraps its structure check; that check (a dependency, not in the reference tree) wants
+// the column indices of every row strictly increasing, so a row that keeps one neighbour
+// twice panics.  Returns the first such row, or n when there is none.
+uint64_t first_repeated_column_row(const Csr& a) {
+  for (uint64_t r = 0; r < a.n; ++r)
+    for (uint64_t q = a.indptr[r] + 1; q < a.indptr[r + 1]; ++q)
+      if (a.indices[q - 1] == a.indices[q]) return r;
+  return a.n;
+}
+
 // umap/fuzzy_simplicial_set.rs:373-383 (binary search within the sorted row).
 inline float csr_get(const Csr& a, uint64_t row, uint32_t col) {
   const uint32_t* b = a.indices.data() + a.indptr[row];
@@ -562,6 +573,13 @@ OrcManifold* orc_learn_manifold(uint64_t n_samples, uint64_t knn_rows, uint64_t 
                   m->sigmas.data(), m->rhos.data());
   m->directed = build_membership_csr(n_samples, n_neighbors, knn_idx, knn_dist, disc_thr,
                                      m->sigmas.data(), m->rhos.data());
+  if (uint64_t r = first_repeated_column_row(m->directed); r < n_samples) {
+    delete m;
+    snprintf(buf, sizeof buf,
+             "knn_indices row %llu keeps the same neighbour more than once: called `Result::unwrap()` on an "
+             "`Err` value: Unsorted(\"Indices are not sorted\")", (unsigned long long)r);
+    return fail(buf);
+  }
   if (symmetrize) m->graph = apply_set_operations(m->directed, set_op_mix_ratio);
   else m->graph = m->directed;
   uint64_t disconnected = 0;                                          // embedding.rs:216-223

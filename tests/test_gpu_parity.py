@@ -71,7 +71,17 @@ def graph_cases():
     sent[::13, -1] = 0xFFFFFFFF                 # sentinel indices (skipped)
     dist_inf = dist.copy()
     dist_inf[::17, 5] = np.inf                  # disconnected entries
+    # repeated neighbours that never reach the CSR: a disconnected repeat, repeated
+    # sentinels, self listed twice
+    rep_i, rep_d = idx.copy(), dist.copy()
+    rep_i[::19, 9] = rep_i[::19, 3]
+    rep_d[::19, 9] = np.inf
+    rep_i[5::23, 11] = rep_i[5::23, 12] = 0xFFFFFFFF
+    rows = np.arange(7, 4000, 29)
+    rep_i[rows, 13] = rows
+    rep_i[rows, 14] = rows
     return [
+        ("repeats_dropped", rep_i, rep_d, {}),
         ("default", idx, dist, {}),
         ("directed", idx, dist, {"symmetrize": False}),
         ("mix_half", idx, dist, {"set_op_mix_ratio": 0.5}),
@@ -121,6 +131,24 @@ def test_graph_parity(ub, oracle, case):
     assert mg.disconnection_counts() == (info["edges_removed"], info["vertices_disconnected"])
     exact = np.mean(G.data.view(np.uint32) == dt_o.view(np.uint32))
     assert exact > 0.999, f"only {exact:.5f} of weights bit-identical"
+
+
+@pytest.mark.parametrize("symmetrize", [True, False])
+def test_repeated_neighbour_refused_like_the_oracle(ub, oracle, symmetrize):
+    """A kNN row that keeps one neighbour twice makes the reference panic in sprs's
+    CsMatI::new (fuzzy_simplicial_set.rs:291: a row's column indices must increase strictly);
+    the GPU build refuses it with the oracle's message, naming the smallest such row."""
+    idx, dist, _ = small_gauss(2000, 15, seed=3)
+    idx = idx.copy()
+    idx[1500, 7] = idx[1500, 2]
+    idx[311, 14] = idx[311, 1]
+    cfg, ocfg = _configs(ub, oracle, 15, {"symmetrize": symmetrize})
+    with pytest.raises(oracle.OracleError) as eo:
+        oracle.learn_manifold(idx, dist, ocfg)
+    with pytest.raises(ub.UmapError) as eg:
+        ub.Umap(cfg).learn_manifold(2000, idx, dist)
+    assert eg.value.code == ub.ERR_INVALID_ARGUMENT
+    assert str(eo.value) == str(eg.value) and "row 311 " in str(eg.value)
 
 
 @pytest.mark.parametrize("total_epochs", [200, 5, 500])

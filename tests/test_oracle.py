@@ -162,6 +162,41 @@ def test_disconnection_distance(oracle):
         assert all(d_of[int(c)] < 1.0 for c in ix[ip[r]:ip[r + 1]])
 
 
+def _repeat_neighbour(idx, dist, row, dup_col, src_col):
+    """Row `row` lists neighbour idx[row, src_col] a second time, in column dup_col."""
+    idx, dist = idx.copy(), dist.copy()
+    idx[row, dup_col] = idx[row, src_col]
+    return idx, dist
+
+
+def test_repeated_neighbour_is_refused(oracle):
+    """A kNN row that keeps one neighbour twice reaches sprs's CsMatI::new with a repeated
+    column (fuzzy_simplicial_set.rs:291), whose structure check refuses it: the reference
+    panics, the oracle returns that text with the smallest offending row."""
+    idx, dist, _ = ring_fixture()
+    bad_i, bad_d = _repeat_neighbour(idx, dist, 7, 4, 2)
+    bad_i[30, 9] = bad_i[30, 0]
+    with pytest.raises(oracle.OracleError, match=r"^knn_indices row 7 keeps the same neighbour more than once"):
+        oracle.learn_manifold(bad_i, bad_d, oracle.OracleConfig(n_neighbors=10))
+    with pytest.raises(oracle.OracleError, match=r"Unsorted\("):
+        oracle.learn_manifold(bad_i, bad_d, oracle.OracleConfig(n_neighbors=10, symmetrize=False))
+
+
+def test_repeated_neighbour_dropped_before_the_csr_is_accepted(oracle):
+    """A repeat that never reaches the CSR is harmless: a disconnected copy (distance at or
+    beyond disconnection_distance) or a repeated sentinel / self entry is skipped first."""
+    idx, dist, _ = ring_fixture()
+    i2, d2 = _repeat_neighbour(idx, dist, 7, 4, 2)
+    d2[7, 4] = np.inf                                      # the repeat is disconnected
+    m = oracle.learn_manifold(i2, d2, oracle.OracleConfig(n_neighbors=10))
+    ip, ix, _ = m.directed()
+    assert ip[8] - ip[7] == 9 and len(set(ix[ip[7]:ip[8]].tolist())) == 9
+    i3 = idx.copy()
+    i3[11, 3] = i3[11, 5] = 0xFFFFFFFF                     # two sentinels
+    i3[12, 3] = i3[12, 6] = 12                             # self twice
+    oracle.learn_manifold(i3, dist, oracle.OracleConfig(n_neighbors=10))
+
+
 # ---- the reference's smoke tests (umap-rs/src/tests.rs), against the oracle
 def test_ref_learn_manifold(oracle, ring):
     idx, dist, _ = ring

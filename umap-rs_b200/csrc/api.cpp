@@ -246,14 +246,20 @@ std::unique_ptr<umap_manifold> learn_manifold_impl(const umap_config& c, uint64_
 
   DevBuf<uint32_t> pcol(n * k, s), cnt(n, s);
   DevBuf<float> pw(n * k, s);
-  DevBuf<unsigned long long> dcount(2, s);
-  UB_CUDA(cudaMemsetAsync(dcount.p, 0, 16, s));
-  membership(idx, dist, n, k, gp, m->sigmas.p, m->rhos.p, pcol.p, pw.p, cnt.p, dcount.p, s);
+  DevBuf<unsigned long long> dcount(3, s);
+  UB_CUDA(cudaMemsetAsync(dcount.p, 0, 24, s));
+  membership(idx, dist, n, k, gp, m->sigmas.p, m->rhos.p, pcol.p, pw.p, cnt.p, dcount.p, dcount.p + 2, s);
   DevBuf<uint64_t> dptr(n + 1, s);
   scan_u32_to_u64(cnt.p, dptr.p, n, s);
   uint64_t nnz_dir = 0;
+  unsigned long long dup = 0;
   d2h(&nnz_dir, dptr.p + n, 1, s);
+  d2h(&dup, dcount.p + 2, 1, s);
   UB_CUDA(cudaStreamSynchronize(s));
+  if (dup)  // fuzzy_simplicial_set.rs:291: sprs's CsMatI::new refuses a row with a repeated column
+    throw Error(INVALID_ARGUMENT, "knn_indices row " + std::to_string(~dup) +
+                                      " keeps the same neighbour more than once: called `Result::unwrap()` on an "
+                                      "`Err` value: Unsorted(\"Indices are not sorted\")");
   DevBuf<uint32_t> keys(nnz_dir, s), vals(nnz_dir, s);
   compact_directed(pcol.p, cnt.p, dptr.p, n, k, keys.p, vals.p, s);
   log.mark("build_membership_csr complete");
@@ -2016,10 +2022,25 @@ int umap_knn_bruteforce_device(const float* data, uint64_t n, uint64_t dim, uint
   API_END
 }
 
+// The sort's passes read one buffer while they scatter into another, so no output may share
+// memory with an input or with the other output.
+void sort_buffers_disjoint(const uint32_t* keys_in, const uint32_t* vals_in, const uint32_t* keys_out,
+                           const uint32_t* vals_out, uint64_t n) {
+  const auto overlap = [n](const uint32_t* a, const uint32_t* b) {
+    if (!a || !b || n == 0) return false;
+    const uintptr_t x = reinterpret_cast<uintptr_t>(a), y = reinterpret_cast<uintptr_t>(b), len = n * 4;
+    return x < y + len && y < x + len;
+  };
+  if (overlap(keys_out, keys_in) || overlap(keys_out, vals_in) || overlap(vals_out, keys_in) ||
+      overlap(vals_out, vals_in) || overlap(keys_out, vals_out))
+    throw Error(INVALID_ARGUMENT, "radix sort: output buffers must not overlap the inputs or each other");
+}
+
 int umap_radix_sort_pairs_device(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
                                  uint32_t* vals_out, uint64_t n, int end_bit) {
   API_BEGIN
   need(keys_in, "keys_in"); need(keys_out, "keys_out"); need(vals_out, "values_out");
+  sort_buffers_disjoint(keys_in, vals_in, keys_out, vals_out, n);
   cudaStream_t s;
   UB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
   struct SGuard { cudaStream_t s; ~SGuard() { (void)cudaStreamSynchronize(s); (void)cudaStreamDestroy(s); } } g{s};
@@ -2032,7 +2053,12 @@ int umap_radix_sort_pairs_device(const uint32_t* keys_in, const uint32_t* vals_i
 int umap_radix_sort_pairs_device_noalloc(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
                                          uint32_t* vals_out, uint64_t n, int end_bit, void* stream) {
   API_BEGIN
-  need(keys_in, "keys_in"); need(keys_out, "keys_out"); need(vals_out, "values_out");
+  // n = 0 is the per-device warm-up call: it only loads the scratch array and looks up its
+  // address, so its buffers may be NULL.
+  if (n > 0) {
+    need(keys_in, "keys_in"); need(keys_out, "keys_out"); need(vals_out, "values_out");
+  }
+  sort_buffers_disjoint(keys_in, vals_in, keys_out, vals_out, n);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   radix_sort_pairs_noalloc(keys_in, vals_in, keys_out, vals_out, n, end_bit, s);
   UB_CUDA(cudaStreamSynchronize(s));

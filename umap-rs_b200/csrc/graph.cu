@@ -220,11 +220,15 @@ __global__ void row_segment_kernel(const uint64_t* __restrict__ seg_off, uint32_
 // disconnected, not self, not a sentinel >= n, weight != 0) in j order, then a stable
 // insertion sort by column (:264-282).  Rows are staged in shared memory; output rows are
 // written back cooperatively (coalesced) into the padded [n][k] arrays.
+// The reference hands each sorted row to sprs's CsMatI::new (:291), whose structure check
+// wants strictly increasing column indices in a row, so a row that keeps the same neighbour
+// twice makes it panic.  Such rows are reported through dup_row (the largest ~row, i.e. the
+// smallest offending row, by atomicMax over ~row; 0 = none) for the host to refuse.
 __global__ void __launch_bounds__(BT) membership_kernel(
     const uint32_t* __restrict__ idx, const float* __restrict__ dist, uint64_t n, uint32_t k,
     GraphParams gp, const float* __restrict__ sigmas, const float* __restrict__ rhos,
     uint32_t* __restrict__ pcol, float* __restrict__ pw, uint32_t* __restrict__ cnt,
-    unsigned long long* __restrict__ edges_removed) {
+    unsigned long long* __restrict__ edges_removed, unsigned long long* __restrict__ dup_row) {
   extern __shared__ unsigned char smem[];
   const uint32_t stride = k | 1u;
   uint32_t* s_col = (uint32_t*)smem;
@@ -265,6 +269,11 @@ __global__ void __launch_bounds__(BT) membership_kernel(
         --m;
       }
     }
+    for (uint32_t q = 1; q < o; ++q)
+      if (c[q - 1] == c[q]) {
+        atomicMax(dup_row, (unsigned long long)~i);
+        break;
+      }
     for (uint32_t q = o; q < k; ++q) { c[q] = 0xFFFFFFFFu; w[q] = 0.0f; }
     cnt[i] = o;
   }
@@ -411,7 +420,8 @@ void smooth_knn(const float* dist, uint64_t n, uint64_t k, const GraphParams& gp
 
 void membership(const uint32_t* idx, const float* dist, uint64_t n, uint64_t k,
                 const GraphParams& gp, const float* sigmas, const float* rhos, uint32_t* pcol,
-                float* pw, uint32_t* cnt, unsigned long long* edges_removed, cudaStream_t s) {
+                float* pw, uint32_t* cnt, unsigned long long* edges_removed, unsigned long long* dup_row,
+                cudaStream_t s) {
   if (n == 0) return;
   const uint32_t stride = (uint32_t)k | 1u;
   const size_t smem = (size_t)BT * stride * 8;
@@ -419,7 +429,7 @@ void membership(const uint32_t* idx, const float* dist, uint64_t n, uint64_t k,
   if (smem > 48 * 1024)
     UB_CUDA(cudaFuncSetAttribute(membership_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   membership_kernel<<<grid_for(n, BT), BT, smem, s>>>(idx, dist, n, (uint32_t)k, gp, sigmas, rhos,
-                                                      pcol, pw, cnt, edges_removed);
+                                                      pcol, pw, cnt, edges_removed, dup_row);
   UB_LAUNCH_CHECK();
 }
 

@@ -347,8 +347,10 @@ void reduce_sum_u64(const uint64_t* x, uint64_t n, uint64_t* out, cudaStream_t s
 // application whose allocator owns the whole GPU heap (it reserves the device memory up
 // front and a foreign cudaMalloc would fail or fragment it), or a latency-critical loop
 // that must not enter the CUDA allocator at all.  For them the scratch space lives in the
-// file-scope array below, sized for at most NOALLOC_MAX_PAIRS pairs; every GPU that loads
-// the library holds it (about 9 MiB) until the process exits.  In host code the array's
+// file-scope array below, sized for at most NOALLOC_MAX_PAIRS pairs (about 9 MiB).  The CUDA
+// runtime places it on a GPU when it loads this file's module there (lazily: at the first
+// kernel launch or symbol lookup on that device), and the GPU holds it until the process
+// exits; a call with n = 0 performs that load and the address lookup.  In host code the array's
 // name is only a host-side stand-in, so its device address is looked up with
 // cudaGetSymbolAddress, once per device, with that device current.  Every call shares the
 // array and it keeps the previous call's contents: all of it is fully rewritten before it

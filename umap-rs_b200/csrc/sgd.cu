@@ -369,7 +369,7 @@ __global__ void __launch_bounds__(256, MINB) sgd_epoch_kernel2(
     while (mask == 0 && ew < width) {
       ebase = ew;
       if (LM) {
-        // width is a multiple of 4: the window's sectors lie inside the lane's entries
+        // width is a multiple of W (slice_meta_kernel): the window lies inside the lane's entries
 #pragma unroll
         for (int j = 0; j < W; j += 2) {
           const uint4 v = __ldg(reinterpret_cast<const uint4*>(lent + ew + j));
@@ -560,7 +560,9 @@ __global__ void slice_meta_kernel(const uint32_t* __restrict__ perm, const uint3
   // slice width = longest task of the slice (instance-major order: the max over lanes)
   uint32_t len = q < T ? chunk - (skey[q] & len_mask) : 0u;
   for (int o = 16; o > 0; o >>= 1) len = max(len, __shfl_xor_sync(0xFFFFFFFFu, len, o));
-  if (lane_major) len = (len + 3u) & ~3u;  // whole 4-entry (32-byte) sectors per lane
+  // whole register windows per lane (UB_SGD2_W entries, a multiple of one 4-entry sector): the
+  // lane-major epoch loads a full window without a bounds check
+  if (lane_major) len = (len + (UB_SGD2_W - 1u)) / UB_SGD2_W * UB_SGD2_W;
   if ((q & 31) == 0) {
     width[q >> 5] = len;
     split_mask[q >> 5] = bits;

@@ -140,10 +140,12 @@ void localize_knn(const uint32_t* idx, uint64_t n, uint64_t k, const Segments& s
 void fill_row_segments(const uint64_t* seg_off, uint32_t n_seg, uint32_t* row_seg, cudaStream_t s);
 // K2: directed membership entries per row, kept ones sorted by column (stable) into the
 // padded [n][k] arrays pcol/pw; cnt[r] = kept count.  edges_removed (device u64) counts
-// dist >= disc_thr entries.
+// dist >= disc_thr entries; dup_row (device u64, zeroed by the caller) receives ~r of the
+// smallest row r that keeps one neighbour twice (0 = none).
 void membership(const uint32_t* idx, const float* dist, uint64_t n, uint64_t k,
                 const GraphParams& gp, const float* sigmas, const float* rhos, uint32_t* pcol,
-                float* pw, uint32_t* cnt, unsigned long long* edges_removed, cudaStream_t s);
+                float* pw, uint32_t* cnt, unsigned long long* edges_removed, unsigned long long* dup_row,
+                cudaStream_t s);
 // Compacts padded rows into CSR order: keys[q] = column, vals[q] = padded position r*k+e.
 void compact_directed(const uint32_t* pcol, const uint32_t* cnt, const uint64_t* dptr,
                       uint64_t n, uint64_t k, uint32_t* keys, uint32_t* vals, cudaStream_t s);

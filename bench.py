@@ -82,20 +82,22 @@ def peak(key):
     return (float(v), "measured") if v else (FALLBACK_PEAKS[key], "fallback")
 
 
-def _profile_value(key):
-    """A `key: value` line of the committed ncu summary of the SGD epoch (None if absent)."""
-    p = os.path.join(ROOT, "profiles", "sgd_epoch_2m.md")
+def ncu_figure(capture, key):
+    """One figure of a committed ncu capture (profiles/ncu_figures.json; None if absent)."""
     try:
-        for line in open(p):
-            if line.startswith(key + ":"):
-                return float(line.split(":", 1)[1].split()[0])
-    except OSError:
-        pass
-    return None
+        with open(os.path.join(ROOT, "profiles", "ncu_figures.json")) as f:
+            v = json.load(f).get(capture, {}).get(key)
+    except (OSError, ValueError):
+        return None
+    return float(v) if isinstance(v, (int, float)) else None
+
+
+def _profile_value(key):
+    return ncu_figure("sgd_epoch_2m", key)
 
 
 def traffic_per_epoch():
-    """DRAM bytes per SGD launch from the committed ncu summary (None if absent)."""
+    """DRAM bytes per SGD launch of the 2M workload from the committed ncu capture."""
     return _profile_value("traffic_bytes_per_launch")
 
 
@@ -106,7 +108,7 @@ def l2_counters():
     vals = {k: _profile_value(k) for k in keys}
     if all(v is None for v in vals.values()):
         return None
-    vals["source"] = "ncu --set full of one epoch (profiles/sgd_epoch_2m.md)"
+    vals["source"] = "ncu --set full of one epoch of the 2M workload"
     return vals
 
 
@@ -432,14 +434,9 @@ def run_warm_start(a):
 
 def swiss_traffic(edges):
     """DRAM bytes per SGD launch at `edges` kept edges, scaled from the 20M-point capture."""
-    p = os.path.join(ROOT, "profiles", "sgd_epoch_swiss_roll_20m.md")
-    try:
-        for line in open(p):
-            if line.startswith("traffic_bytes_per_launch:"):
-                return float(line.split(":", 1)[1].split()[0]) * edges / 332297330.0
-    except OSError:
-        pass
-    return None
+    t = ncu_figure("sgd_epoch_swiss_roll_20m", "traffic_bytes_per_launch")
+    e0 = ncu_figure("sgd_epoch_swiss_roll_20m", "kept_edges")
+    return t * edges / e0 if t and e0 else None
 
 
 def run_swiss_roll(a):
@@ -547,8 +544,8 @@ def run_swiss_roll(a):
             "graph_and_setup_ms": ms_step - sgd_ms,
             "roofline": {"bound": "hbm", "kernel": "sgd_epoch_kernel2<2, false, 4, 5>", "achieved": achieved, "peak": hbm,
                          "unit": "GB/s", "frac": achieved / hbm, "peak_source": hbm_src, "traffic": swiss_traffic(E),
-                         "traffic_note": "DRAM bytes of one epoch-20 launch captured at 20M points "
-                                         "(profiles/sgd_epoch_swiss_roll_20m.md), scaled by kept edges",
+                         "traffic_note": "DRAM bytes of one epoch-20 launch captured at 20M points, "
+                                         "scaled by kept edges",
                          "algorithmic_bytes_per_launch": alg / a.swiss_epochs,
                          "avg_launch_ms": sgd_ms / a.swiss_epochs},
             "device_memory_gb": {"total": total_mem / 1e9, "inputs_resident": (total_mem - free0) / 1e9,
@@ -670,13 +667,7 @@ def run_knn(a):
     cms = float(np.mean(cand_ms))
     achieved = flops / (cms / 1e3) / 1e12
     pk, pk_src = peak("bf16_tflops")
-    traffic = None
-    try:
-        for line in open(os.path.join(ROOT, "profiles", "knn_candidates_digits70k.md")):
-            if line.startswith("traffic_bytes_per_launch:"):
-                traffic = float(line.split(":", 1)[1].split()[0])
-    except OSError:
-        pass
+    traffic = ncu_figure("knn_candidates_digits70k", "traffic_bytes_per_launch")
     cpu = None
     if not a.no_cpu:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))

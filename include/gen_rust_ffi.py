@@ -1,6 +1,6 @@
 """Generates umap_b200_ffi.rs, the Rust `extern "C"` declarations of every entry point, enum
 constant and type in umap_b200.h, for a Rust crate that binds the library (the crate's
-`src/ffi.rs`; see INTEGRATION.md for build.rs and the safe wrappers).
+`src/ffi.rs`, which its build.rs links against libumap_b200.so and its safe wrappers call).
 
     python include/gen_rust_ffi.py            # rewrites include/umap_b200_ffi.rs
     python include/gen_rust_ffi.py --check    # exit 1 if the committed file is stale

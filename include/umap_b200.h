@@ -3,7 +3,7 @@
  *
  * Each entry point stands in for one item of the Rust API of wilsonzlin/umap-rs 0.4.5
  * (paths below are relative to that project).  A Rust crate keeps its public API and
- * implements the bodies by calling these functions (binding sketch in INTEGRATION.md).
+ * implements the bodies by calling these functions.
  *
  * Conventions
  *  - Every function returns an int status: UMAP_OK (0) or a UMAP_ERR_* code.  Where the

@@ -519,3 +519,34 @@ def test_generic_optimizer_checkpoint_resumes(ub, ring):
         assert e.value.code == ub.ERR_UNSUPPORTED
         o2.step_epochs(20)
         assert o2.remaining_epochs() == 0 and np.isfinite(o2.embedding()).all()
+
+
+def test_persisting_l2_set_aside_released_with_the_last_optimizer(ub):
+    """An optimizer puts its embedding in a persisting-L2 window, which reserves a device-wide
+    L2 set-aside.  The set-aside stays while any optimizer on the device holds a window and
+    returns to 0 when the last one is consumed (into_fitted) or freed, so the host
+    application's own kernels get the whole L2 back."""
+    import torch
+    from cuda.bindings import runtime as rt
+
+    def limit():
+        torch.cuda.synchronize()
+        err, v = rt.cudaDeviceGetLimit(rt.cudaLimit.cudaLimitPersistingL2CacheSize)
+        assert err == rt.cudaError_t.cudaSuccess
+        return v
+
+    idx, dist, init = small_gauss(3000, 15, seed=5)
+    cfg = ub.UmapConfig()
+    cfg.optimization.n_epochs = 20
+    u = ub.Umap(cfg)
+    o1 = ub.Optimizer(u.learn_manifold(3000, idx, dist), init, 20, cfg)
+    o2 = ub.Optimizer(u.learn_manifold(3000, idx, dist), init, 20, cfg)
+    o1.step_epochs(5)
+    o2.step_epochs(5)
+    assert limit() > 0
+    o1.into_fitted(cfg)
+    assert limit() > 0           # o2 still holds its window
+    del o2                       # freed without into_fitted
+    import gc
+    gc.collect()
+    assert limit() == 0

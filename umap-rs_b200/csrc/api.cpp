@@ -136,6 +136,12 @@ struct umap_manifold {
   cudaStream_t s() const { return stream->s; }
 };
 
+namespace ub {
+namespace {
+void release_l2_window(umap_optimizer& o) noexcept;
+}  // namespace
+}  // namespace ub
+
 struct umap_optimizer {
   std::unique_ptr<umap_manifold> manifold;  // declared first: owns the stream
   uint64_t n = 0, dim = 0;
@@ -153,7 +159,12 @@ struct umap_optimizer {
   ub::DevBuf<uint64_t> seg_off;
   ub::DevBuf<uint32_t> row_seg;
   ub::DevBuf<float> seg_thr, seg_maxw;
+  bool l2_window = false;  // holds a persisting-L2 access-policy window (see set_l2_window)
   cudaStream_t s() const { return manifold->s(); }
+  umap_optimizer() = default;
+  umap_optimizer(const umap_optimizer&) = delete;
+  umap_optimizer& operator=(const umap_optimizer&) = delete;
+  ~umap_optimizer() { ub::release_l2_window(*this); }
 };
 
 struct umap_fitted {
@@ -332,20 +343,58 @@ std::unique_ptr<umap_manifold> clone_manifold(const umap_manifold& src) {
 }
 
 // ------------------------------------------------------------------ Optimizer
+// Optimizers on each device that currently hold a persisting-L2 window.  The set-aside
+// (cudaLimitPersistingL2CacheSize) is device-wide and outlives the stream, so it is handed
+// back, and lines still marked persisting are reset to normal, when the last holder on the
+// device is consumed (into_fitted) or freed: the host application's own kernels then get
+// the whole L2 again.
+std::mutex g_l2_mu;
+std::map<int, int> g_l2_holders;
+
+void release_l2_window(umap_optimizer& o) noexcept {
+  if (!o.l2_window) return;
+  o.l2_window = false;
+  int prev = -1;
+  (void)cudaGetDevice(&prev);
+  const int dev = o.manifold->stream->device;
+  (void)cudaSetDevice(dev);
+  cudaStreamAttrValue attr;
+  memset(&attr, 0, sizeof attr);
+  (void)cudaStreamSetAttribute(o.s(), cudaStreamAttributeAccessPolicyWindow, &attr);
+  std::lock_guard<std::mutex> lock(g_l2_mu);
+  if (--g_l2_holders[dev] <= 0) {
+    g_l2_holders.erase(dev);
+    (void)cudaStreamSynchronize(o.s());
+    (void)cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, 0);
+    (void)cudaCtxResetPersistingL2Cache();
+  }
+  (void)cudaGetLastError();
+  if (prev >= 0 && prev != dev) (void)cudaSetDevice(prev);
+}
+
 void set_l2_window(umap_optimizer& o, bool enable) {
   static const bool disabled = [] {
     const char* e = getenv("UMAP_B200_L2_PERSIST");
     return e && e[0] == '0';
   }();
+  if (!enable) {
+    release_l2_window(o);
+    return;
+  }
   cudaStreamAttrValue attr;
   memset(&attr, 0, sizeof attr);
-  if (enable && !disabled && o.emb2.p) {
+  if (!disabled && o.emb2.p) {
     int dev = o.manifold->stream->device, max_persist = 0, max_window = 0;
     UB_CUDA(cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, dev));
     UB_CUDA(cudaDeviceGetAttribute(&max_window, cudaDevAttrMaxAccessPolicyWindowSize, dev));
     if (max_persist <= 0 || max_window <= 0) return;
     const size_t bytes = o.emb2.bytes();
     const size_t lim = std::min(bytes, (size_t)max_persist);
+    {
+      std::lock_guard<std::mutex> lock(g_l2_mu);
+      if (!o.l2_window) ++g_l2_holders[dev];
+      o.l2_window = true;
+    }
     UB_CUDA(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, lim));
     attr.accessPolicyWindow.base_ptr = o.emb2.p;
     attr.accessPolicyWindow.num_bytes = std::min(bytes, (size_t)max_window);

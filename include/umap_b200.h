@@ -300,6 +300,17 @@ int umap_radix_sort_pairs_device(const uint32_t* dev_keys_in, const uint32_t* de
                                  uint32_t* dev_keys_out, uint32_t* dev_values_out,
                                  uint64_t n, int end_bit);
 
+/* The negative samples of the SGD epoch kernel (optimize_layout_euclidean.rs:313-314, which
+ * draws rng.random_range(0..n_vertices) from an unseeded thread-local generator; here a
+ * counter-based generator keyed by (seed, edge entry, epoch)).  For entries first_entry ..
+ * first_entry + n_entries - 1 firing at `epoch`, draw q (q < per_entry <= 64) of entry e is
+ * written to dev_out[(e - first_entry) * per_entry + q], in [lo, lo + range): exactly the
+ * values the epoch kernel uses for an optimizer whose seed is `seed`.  For statistical
+ * tests of the generator. */
+int umap_sgd_negative_draws_device(uint64_t seed, uint64_t first_entry, uint64_t n_entries,
+                                   uint32_t epoch, uint32_t per_entry, uint32_t lo, uint32_t range,
+                                   uint32_t* dev_out);
+
 /* Allocation-free variant of umap_radix_sort_pairs_device (no counterpart in the
  * reference; the reference has no device code).  For callers that cannot allocate device
  * memory when they sort: a host application whose allocator owns the whole GPU heap, or a

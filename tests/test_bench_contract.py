@@ -25,3 +25,15 @@ def test_roofline_inputs_from_committed_profile():
     assert l2 is not None
     for k in ("l2_throughput_pct", "l2_hit_rate_pct", "issue_active_pct"):
         assert 0.0 < l2[k] <= 100.0, (k, l2[k])
+
+
+def test_both_arms_share_one_config():
+    """The default workload's `config` is built by one function for both arms from the
+    workload and the cached inputs' digest, and carries no per-arm timing or work counts."""
+    sys.path.insert(0, ROOT)
+    import bench
+    info = {"knn": "exact", "knn_rows_recomputed": 0, "inputs_sha1_16": "0123456789abcdef"}
+    c1 = bench.fit_config(2_000_000, 500, 1, info)
+    c2 = bench.fit_config(2_000_000, 500, 1, dict(info))
+    assert c1 == c2 and c1["workload"] == "gaussians_2000000_d64_k15_500ep"
+    assert not {"knn_seconds", "kept_edges", "edge_updates_per_fit"} & set(c1)

@@ -2099,11 +2099,30 @@ int umap_radix_sort_pairs_device(const uint32_t* keys_in, const uint32_t* vals_i
   API_END
 }
 
+int umap_sgd_negative_draws_device(uint64_t seed, uint64_t first_entry, uint64_t n_entries, uint32_t epoch,
+                                   uint32_t per_entry, uint32_t lo, uint32_t range, uint32_t* dev_out) {
+  API_BEGIN
+  need(dev_out, "out");
+  if (range == 0) throw Error(INVALID_ARGUMENT, "range must be at least 1");
+  if (per_entry > 64) throw Error(INVALID_ARGUMENT, "per_entry must be at most 64");
+  cudaStream_t s;
+  UB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  struct SGuard { cudaStream_t s; ~SGuard() { (void)cudaStreamSynchronize(s); (void)cudaStreamDestroy(s); } } g{s};
+  wait_for_inputs();
+  negative_draws(seed, first_entry, n_entries, epoch, per_entry, lo, range, dev_out, s);
+  UB_CUDA(cudaStreamSynchronize(s));
+  API_END
+}
+
 int umap_radix_sort_pairs_device_noalloc(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
                                          uint32_t* vals_out, uint64_t n, int end_bit, void* stream) {
   API_BEGIN
   // n = 0 is the per-device warm-up call: it only loads the scratch array and looks up its
   // address, so its buffers may be NULL.
+  if (n > radix_sort_noalloc_max_pairs())
+    throw Error(INVALID_ARGUMENT, "allocation-free radix sort takes at most " +
+                                      std::to_string(radix_sort_noalloc_max_pairs()) + " pairs, got " +
+                                      std::to_string(n));
   if (n > 0) {
     need(keys_in, "keys_in"); need(keys_out, "keys_out"); need(vals_out, "values_out");
   }

@@ -715,6 +715,23 @@ __global__ void schedule_totals_kernel(const uint2* __restrict__ entry, uint64_t
   }
 }
 
+// The negative samples the epoch kernel would draw for the firings of entries
+// [first, first + count) at `epoch`: draw q of entry e is out[(e - first) * per + q], made by
+// the same generator and mapping as fired_edge (half q & 1 of pair q >> 1, multiply-high into
+// [lo, lo + range)).  Statistical tests of the generator read these.
+__global__ void negative_draws_kernel(uint64_t seed, uint64_t first, uint64_t count, uint32_t epoch,
+                                      uint32_t per, uint32_t lo, uint32_t range, uint32_t* __restrict__ out) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const NegRng rng(seed, first + i, epoch);
+  uint64_t rnd = 0;
+  for (uint32_t q = 0; q < per; ++q) {
+    if ((q & 1) == 0) rnd = rng.pair(q >> 1);
+    const uint32_t rv = (q & 1) ? (uint32_t)(rnd >> 32) : (uint32_t)rnd;
+    out[i * per + q] = lo + __umulhi(rv, range);
+  }
+}
+
 __global__ void nan_rows_kernel(const uint64_t* __restrict__ indptr, uint64_t n, uint32_t dim,
                                 float* __restrict__ emb) {
   const uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -946,6 +963,13 @@ void schedule_totals(const SgdLayout& L, uint32_t neg_rate, uint32_t start, uint
   if (L.n_entries == 0 || end <= start) return;
   schedule_totals_kernel<<<grid_for(L.n_entries, 256), 256, 0, s>>>(L.entry.p, L.n_entries, neg_rate, start, end,
                                                                    d_fired, d_negs);
+  UB_LAUNCH_CHECK();
+}
+
+void negative_draws(uint64_t seed, uint64_t first, uint64_t count, uint32_t epoch, uint32_t per, uint32_t lo,
+                    uint32_t range, uint32_t* out, cudaStream_t s) {
+  if (count == 0 || per == 0) return;
+  negative_draws_kernel<<<grid_for(count, 256), 256, 0, s>>>(seed, first, count, epoch, per, lo, range, out);
   UB_LAUNCH_CHECK();
 }
 

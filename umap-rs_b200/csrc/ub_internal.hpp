@@ -245,6 +245,9 @@ void normalize_init(float* emb, uint64_t n, uint32_t dim, cudaStream_t s,
 void sgd_epoch(const SgdLayout& L, float* live, float* snap, const SgdParams& p,
                uint32_t epoch, float alpha, cudaStream_t s);
 // Exact totals of fired edges / negatives over epochs [start, end).
+// Negative samples of the SGD epoch's generator (see negative_draws_kernel in sgd.cu).
+void negative_draws(uint64_t seed, uint64_t first, uint64_t count, uint32_t epoch, uint32_t per, uint32_t lo,
+                    uint32_t range, uint32_t* out, cudaStream_t s);
 void schedule_totals(const SgdLayout& L, uint32_t neg_rate, uint32_t start, uint32_t end,
                      unsigned long long* d_fired, unsigned long long* d_negs, cudaStream_t s);
 // Rows with an empty graph row -> NaN (embedding.rs:327-334).

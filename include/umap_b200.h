@@ -311,6 +311,13 @@ int umap_sgd_negative_draws_device(uint64_t seed, uint64_t first_entry, uint64_t
                                    uint32_t epoch, uint32_t per_entry, uint32_t lo, uint32_t range,
                                    uint32_t* dev_out);
 
+/* The SGD schedule's negative count per firing (optimize_layout_euclidean.rs:308-311, :343:
+ * n_neg = floor((n - epoch_of_next_negative_sample) / epochs_per_negative_sample)), as the
+ * epoch kernel evaluates it from an edge's stored schedule word dev_q[i] (ceil(2^32 /
+ * epochs_per_sample) - 1) at epoch dev_epoch[i]; 0 where the edge does not fire then. */
+int umap_sgd_negatives_per_firing_device(const uint32_t* dev_q, const uint32_t* dev_epoch, uint64_t count,
+                                         uint32_t negative_sample_rate, uint32_t* dev_out);
+
 /* Allocation-free variant of umap_radix_sort_pairs_device (no counterpart in the
  * reference; the reference has no device code).  For callers that cannot allocate device
  * memory when they sort: a host application whose allocator owns the whole GPU heap, or a

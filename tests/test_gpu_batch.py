@@ -84,3 +84,71 @@ def test_batch_fit_quality_matches_plain(ub):
         spread = max(ces) - min(ces)
         print(i, n, ce_b, ces)
         assert abs(ce_b - np.mean(ces)) <= max(0.02 * np.mean(ces), 3 * spread)
+
+
+def _oracle_weights(mo, head, tail):
+    ip, ix, dt = mo.graph()
+    ip = ip.astype(np.int64)
+    h = np.asarray(head, np.int64)
+    return dt[ip[h] + np.array([np.searchsorted(ix[ip[r]:ip[r + 1]], t) for r, t in zip(h, tail)], np.int64)]
+
+
+def test_batch_instances_match_the_oracle(ub, oracle):
+    """Every instance of a batch against the oracle's per-instance Umap::fit path
+    (embedding.rs:274-337 run once per dataset): rho bit-exact and sigma within 1e-5; graph
+    row pointers and columns bit-exact, weights within 1e-5; pruned head/tail bit-exact,
+    epochs_per_sample within 1e-5; normalised init bit-exact; and, for the embedding, fuzzy
+    cross-entropy of the batched fit within 1% of the oracle's (2 GPU seeds against 3 oracle
+    seeds, means compared)."""
+    from umap_b200 import quality as Q
+    sizes = [700, 1800, 64, 2600]
+    off, idxs, dists, inits = make_batch(sizes, seed0=500)
+    idxs[1] = idxs[1].copy()
+    idxs[1][::9, -2] = 0xFFFFFFFF
+    dists[3] = dists[3].copy()
+    dists[3][::13, 6] = np.inf
+    total = 200
+    cfg = ub.UmapConfig()
+    cfg.optimization.n_epochs = total
+    ocfg = oracle.OracleConfig(n_epochs=total)
+    I, D, X0 = np.vstack(idxs), np.vstack(dists), np.vstack(inits)
+    bopt = ub.Optimizer.batch(cfg, off, I, D, X0, total)
+    G = bopt.manifold().graph()
+    bs, br = bopt.manifold().sigmas_rhos()
+    bh, bt, be, _, _, _ = bopt.export_edges()
+    bemb0 = bopt.embedding()
+    fits = []
+    for seed in (11, 12):
+        o = ub.Optimizer.batch(cfg, off, I, D, X0, total)
+        o.set_seed(seed)
+        o.step_epochs(total)
+        fits.append(o.embedding())
+    ce_checked = 0
+    for i, n in enumerate(sizes):
+        lo, hi = int(off[i]), int(off[i + 1])
+        mo = oracle.learn_manifold(idxs[i], dists[i], ocfg)
+        so, ro = mo.sigmas_rhos()
+        assert np.array_equal(br[lo:hi].view(np.uint32), ro.view(np.uint32)), i
+        assert np.allclose(bs[lo:hi], so, rtol=1e-5, atol=0), i
+        ip, ix, dt = mo.graph()
+        rows = G.indptr[lo:hi + 1]
+        assert np.array_equal(rows - rows[0], ip), i
+        assert np.array_equal(G.indices[rows[0]:rows[-1]], ix.astype(np.int64) + lo), i
+        assert np.allclose(G.data[rows[0]:rows[-1]], dt, rtol=1e-5, atol=0), i
+        oo = oracle.Optimizer(mo, inits[i], total, ocfg, seed=1)
+        h, t, e = oo.edges()
+        sel = (bh >= lo) & (bh < hi)
+        assert np.array_equal(bh[sel], h.astype(np.int64) + lo) and np.array_equal(bt[sel], t.astype(np.int64) + lo)
+        assert np.allclose(be[sel], e, rtol=1e-5, atol=0), i
+        assert np.array_equal(bemb0[lo:hi].view(np.uint32), oo.embedding().view(np.uint32)), i
+        if n < 500:
+            continue
+        a, b = mo.info()["a"], mo.info()["b"]
+        w = _oracle_weights(mo, h, t)
+        ce_o = [Q.fuzzy_cross_entropy(oracle.fit(idxs[i], dists[i], inits[i], ocfg, seed=s)[0], h, t, w, a, b)
+                for s in (1, 2, 3)]
+        ce_g = [Q.fuzzy_cross_entropy(f[lo:hi], h, t, w, a, b) for f in fits]
+        print(i, n, "oracle", ce_o, "batch", ce_g)
+        assert abs(np.mean(ce_g) - np.mean(ce_o)) <= 0.01 * np.mean(ce_o), (i, ce_g, ce_o)
+        ce_checked += 1
+    assert ce_checked == 3

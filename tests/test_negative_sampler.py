@@ -149,3 +149,53 @@ def test_kernel_draws_pass_uniformity_and_independence_at_1e8(ub):
     assert abs(c(u[:, 4], nxt[:, 4])) < lim
     cells = (torch.floor(u[:-1, 0] * 64) * 64 + torch.floor(u[1:, 0] * 64)).to(torch.int64)
     assert abs(chi2_z(torch.bincount(cells, minlength=4096).cpu().numpy(), np.full(4096, (m - 1) / 4096))) < 5
+
+
+# ------------------------------------------------------------------ negatives per firing
+def negatives_per_firing_exact(q, n, neg):
+    """The schedule's closed form in exact integers: with Q = q + 1, firing m happens at epoch
+    e_m = ceil(m 2^32 / Q), and the firing at epoch n (m = floor(n Q / 2^32)) draws
+    y(n) - y(e_{m-1}) negatives, y(x) = floor(x neg Q / 2^32), or y(n) - 1 for m = 1."""
+    Q = q.astype(np.uint64) + np.uint64(1)
+    n64 = n.astype(np.uint64)
+    m = (n64 * Q) >> np.uint64(32)
+    fires = m > ((n64 - np.uint64(1)) * Q >> np.uint64(32))
+    prev_e = (((m - np.uint64(1)) << np.uint64(32)) + Q - np.uint64(1)) // Q
+    y = (n64 * np.uint64(neg) * Q) >> np.uint64(32)
+    yp = np.where(m > 1, (prev_e * np.uint64(neg) * Q) >> np.uint64(32), np.uint64(1))
+    out = np.where(y > yp, y - yp, np.uint64(0))
+    return np.where(fires & (n64 > 0), out, np.uint64(0)).astype(np.uint32)
+
+
+@pytest.mark.gpu
+def test_kernel_negative_counts_per_firing_are_exact(ub):
+    """The epoch kernel's per-firing negative count against the exact closed form, on firing
+    epochs of edges with epochs_per_sample in [1, 500] (the prune keeps eps <= total_epochs),
+    on non-firing epochs (0), at Q = 2^32 (an edge that fires every epoch), and for huge
+    epochs_per_sample (X up to 2^26 epochs, where the kernel's float estimate needs its exact
+    fallback)."""
+    import torch
+    g = np.random.Generator(np.random.PCG64(5))
+    neg = 5
+    eps = np.concatenate([g.uniform(1.0, 500.0, 400_000), np.round(g.uniform(1, 60, 20_000)),
+                          2.0 ** g.uniform(20, 26, 2_000)])
+    with np.errstate(over="ignore"):
+        Q = np.minimum(np.ceil(2.0 ** 32 / eps), 2.0 ** 32).astype(np.uint64)
+    Q[:1000] = 1 << 32
+    q = (Q - np.uint64(1)).astype(np.uint32)
+    m = g.integers(1, 40, q.size).astype(np.uint64)
+    m[-2000:] = g.integers(1, 4, 2000)
+    n = ((m << np.uint64(32)) + Q - np.uint64(1)) // Q        # firing epochs
+    n[: 50_000] += np.uint64(1)                               # mostly not firing
+    n = n.astype(np.uint32)
+    assert int(n.max()) * neg < 2 ** 32
+    want = negatives_per_firing_exact(q, n, neg)
+    tq = torch.from_numpy(q.view(np.int32)).cuda()
+    tn = torch.from_numpy(n.view(np.int32)).cuda()
+    out = torch.empty(q.size, dtype=torch.int32, device="cuda")
+    rc = ub.lib().umap_sgd_negatives_per_firing_device(C.c_void_p(tq.data_ptr()), C.c_void_p(tn.data_ptr()), q.size,
+                                                       neg, C.c_void_p(out.data_ptr()))
+    assert rc == 0, ub.lib().umap_last_error()
+    got = out.cpu().numpy().view(np.uint32)
+    assert np.array_equal(got, want), np.flatnonzero(got != want)[:10]
+    assert (want[50_000:] > 0).mean() > 0.99

@@ -2114,6 +2114,19 @@ int umap_sgd_negative_draws_device(uint64_t seed, uint64_t first_entry, uint64_t
   API_END
 }
 
+int umap_sgd_negatives_per_firing_device(const uint32_t* dev_q, const uint32_t* dev_epoch, uint64_t count,
+                                         uint32_t negative_sample_rate, uint32_t* dev_out) {
+  API_BEGIN
+  need(dev_q, "q"); need(dev_epoch, "epoch"); need(dev_out, "out");
+  cudaStream_t s;
+  UB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  struct SGuard { cudaStream_t s; ~SGuard() { (void)cudaStreamSynchronize(s); (void)cudaStreamDestroy(s); } } g{s};
+  wait_for_inputs();
+  negatives_per_firing(dev_q, dev_epoch, count, negative_sample_rate, dev_out, s);
+  UB_CUDA(cudaStreamSynchronize(s));
+  API_END
+}
+
 int umap_radix_sort_pairs_device_noalloc(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
                                          uint32_t* vals_out, uint64_t n, int end_bit, void* stream) {
   API_BEGIN

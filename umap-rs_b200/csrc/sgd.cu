@@ -98,25 +98,33 @@ __device__ __forceinline__ bool fires_at(uint32_t n, uint32_t q) {
 }
 // Negatives drawn by the firing at epoch n (n * neg < 2^32 is checked on the host):
 // y(n) - y(p) with y(x) = fires_by(x * neg) and p the epoch of the previous firing, or
-// y(n) - 1 for the first.  Firings are floor(2^32 / Q) or one more epochs apart, so p is found
-// among a few candidates below n - floor(2^32 / Q) + 1 with the cheap test above.
+// y(n) - 1 for the first.  Firing m is at epoch ceil(m X), X = 2^32 / Q, so consecutive
+// firings are G = floor(X) or G + 1 epochs apart and p is n - G if the edge fires there, else
+// n - G - 1 (no firing fits in between).  G comes from a float estimate (relative error below
+// 2^-21), made exact by integer checks (G Q <= 2^32 < (G + 1) Q); a second firing needs
+// n >= 2X, so G < 2^31 here.  Estimates still off after two steps each way (X beyond about
+// 2^21 epochs) take the exact search instead.
 __device__ __forceinline__ uint32_t negatives_at(uint32_t n, uint32_t q, uint32_t neg) {
-  const int64_t y = (int64_t)fires_by(n * neg, q);
-  const uint64_t m = fires_by(n, q);
-  int64_t prev = 1;
+  const uint32_t y = (uint32_t)fires_by(n * neg, q);
+  const uint32_t m = (uint32_t)fires_by(n, q);
+  uint32_t prev = 1;
   if (m > 1) {
-    const int64_t g0 = (int64_t)__fdividef(4294967296.0f, (float)q + 1.0f);
-    uint32_t pe = 0;
+    const uint64_t Q = (uint64_t)q + 1;
+    uint32_t g = (uint32_t)__fdividef(4294967296.0f, (float)Q);
 #pragma unroll
-    for (int t = 1; t >= -2; --t) {
-      const int64_t x = (int64_t)n - g0 + t;
-      if (pe == 0 && x >= 1 && x < (int64_t)n && fires_at((uint32_t)x, q)) pe = (uint32_t)x;
-    }
-    if (pe == 0) pe = fire_epoch(m - 1, q);
-    prev = (int64_t)fires_by(pe * neg, q);
+    for (int t = 0; t < 2; ++t)
+      if ((uint64_t)g * Q > 4294967296ull) --g;
+#pragma unroll
+    for (int t = 0; t < 2; ++t)
+      if ((uint64_t)(g + 1) * Q <= 4294967296ull) ++g;
+    uint32_t p;
+    if ((uint64_t)g * Q <= 4294967296ull && (uint64_t)(g + 1) * Q > 4294967296ull)
+      p = fires_at(n - g, q) ? n - g : n - g - 1;
+    else
+      p = fire_epoch(m - 1, q);
+    prev = (uint32_t)fires_by(p * neg, q);
   }
-  const int64_t d = y - prev;
-  return d > 0 ? (uint32_t)d : 0u;
+  return y > prev ? y - prev : 0u;
 }
 
 // Rust f32::clamp(-4, 4) (utils/clip.rs:13-15): NaN passes through.
@@ -732,6 +740,16 @@ __global__ void negative_draws_kernel(uint64_t seed, uint64_t first, uint64_t co
   }
 }
 
+// Negatives the epoch kernel draws for a firing of an entry with schedule word q at epoch n
+// (0 where the entry does not fire at n): the schedule's per-firing count, for exact tests.
+__global__ void negatives_per_firing_kernel(const uint32_t* __restrict__ qs, const uint32_t* __restrict__ ns,
+                                            uint64_t count, uint32_t neg, uint32_t* __restrict__ out) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const uint32_t q = qs[i], n = ns[i];
+  out[i] = fires_at(n, q) ? negatives_at(n, q, neg) : 0u;
+}
+
 __global__ void nan_rows_kernel(const uint64_t* __restrict__ indptr, uint64_t n, uint32_t dim,
                                 float* __restrict__ emb) {
   const uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -970,6 +988,13 @@ void negative_draws(uint64_t seed, uint64_t first, uint64_t count, uint32_t epoc
                     uint32_t range, uint32_t* out, cudaStream_t s) {
   if (count == 0 || per == 0) return;
   negative_draws_kernel<<<grid_for(count, 256), 256, 0, s>>>(seed, first, count, epoch, per, lo, range, out);
+  UB_LAUNCH_CHECK();
+}
+
+void negatives_per_firing(const uint32_t* qs, const uint32_t* ns, uint64_t count, uint32_t neg, uint32_t* out,
+                          cudaStream_t s) {
+  if (count == 0) return;
+  negatives_per_firing_kernel<<<grid_for(count, 256), 256, 0, s>>>(qs, ns, count, neg, out);
   UB_LAUNCH_CHECK();
 }
 

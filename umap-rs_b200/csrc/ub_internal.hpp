@@ -248,6 +248,9 @@ void sgd_epoch(const SgdLayout& L, float* live, float* snap, const SgdParams& p,
 // Negative samples of the SGD epoch's generator (see negative_draws_kernel in sgd.cu).
 void negative_draws(uint64_t seed, uint64_t first, uint64_t count, uint32_t epoch, uint32_t per, uint32_t lo,
                     uint32_t range, uint32_t* out, cudaStream_t s);
+// Per-firing negative counts of the epoch kernel's schedule (negatives_per_firing_kernel).
+void negatives_per_firing(const uint32_t* qs, const uint32_t* ns, uint64_t count, uint32_t neg, uint32_t* out,
+                          cudaStream_t s);
 void schedule_totals(const SgdLayout& L, uint32_t neg_rate, uint32_t start, uint32_t end,
                      unsigned long long* d_fired, unsigned long long* d_negs, cudaStream_t s);
 // Rows with an empty graph row -> NaN (embedding.rs:327-334).

@@ -95,6 +95,7 @@ SIGNATURES = {
     "umap_radix_sort_pairs_device": [P, P, P, P, u64, i32],
     "umap_radix_sort_pairs_device_noalloc": [P, P, P, P, u64, i32, P],
     "umap_sgd_negative_draws_device": [u64, u64, u64, u32, u32, u32, u32, P],
+    "umap_sgd_negatives_per_firing_device": [P, P, u64, u32, P],
     "umap_radix_sort_noalloc_max_pairs": [C.POINTER(u64)],
     "umap_fit_manifold": [P, C.POINTER(UmapConfigC), P, u64, u64, PP],
     "umap_fit_manifold_device": [P, C.POINTER(UmapConfigC), P, u64, u64, PP],

@@ -379,6 +379,42 @@ int umap_mlp_free(umap_mlp* m);
 int umap_gemm_bf16_device(const void* dev_a, const void* dev_b, float* dev_c, uint64_t m, uint64_t n,
                           uint64_t k, uint64_t k_splits);
 
+/* The whole warm start in one call, standing in for the `init` a caller hands to Umap::fit
+ * (embedding.rs:274-280): a plain fit of a subsample for sub_epochs, the network trained for
+ * mlp_epochs of Adam on (subsample rows, that embedding), its prediction for every row as
+ * init, then Umap::fit of all rows for `epochs` epochs (the prune threshold and the
+ * learning-rate decay follow that epoch count, optimizer.rs:96-102, :317).  The full data's
+ * graph is built on another stream and host thread while the subsample is fitted and the
+ * network trained. */
+typedef struct umap_warm_start_params {
+  uint64_t sub_epochs;            /* 500: the subsample's plain fit */
+  uint64_t epochs;                /* 100: the fit of all rows from the learned init */
+  uint64_t mlp_epochs;            /* 20 */
+  uint64_t batch;                 /* 4096; rounded down to a multiple of 128 and at most the subsample */
+  float mlp_learning_rate;        /* 1e-3 (Adam) */
+  int32_t has_learning_rate;      /* 0: the final fit uses cfg's learning_rate */
+  float learning_rate;
+  uint64_t seed;                  /* network initialisation, batch shuffles, default subsample init */
+} umap_warm_start_params;
+int umap_warm_start_params_default(umap_warm_start_params* out);
+/* Phases reported in phase_ms (milliseconds of host wall time, in this order). */
+#define UMAP_WARM_START_PHASES 8  /* prepare, subsample_fit, mlp_train, mlp_predict,
+                                     wait_full_graph, fit, full_graph_overlapped, total */
+/* dev_data f32 [n_samples][data_dim] (any data_dim up to 4096: rows are zero-padded to a
+ * multiple of 64 for the network); dev_knn_* the full data's kNN [n_samples][knn_cols] as for
+ * umap_fit_device; dev_sub_rows u32[n_sub] the subsample's row numbers; dev_sub_knn_* its own
+ * kNN [n_sub][knn_cols] with ids local to the subsample; dev_sub_init f32 [n_sub][n_components]
+ * or NULL for uniform [-10, 10] from `seed`.  phase_ms (UMAP_WARM_START_PHASES floats) and
+ * mlp_losses (mlp_epochs floats, each epoch's mean batch loss) are host arrays and may be
+ * NULL.  n_sub must leave at least 128 rows with a non-empty graph row. */
+int umap_warm_start_fit_device(const umap_config* cfg, const umap_warm_start_params* params,
+                               const float* dev_data, uint64_t n_samples, uint64_t data_dim,
+                               const uint32_t* dev_knn_indices, const float* dev_knn_dists,
+                               uint64_t knn_cols, const uint32_t* dev_sub_rows, uint64_t n_sub,
+                               const uint32_t* dev_sub_knn_indices, const float* dev_sub_knn_dists,
+                               const float* dev_sub_init, umap_fitted** out, float* phase_ms,
+                               float* mlp_losses);
+
 #ifdef __cplusplus
 }
 #endif

@@ -142,4 +142,6 @@ extern "C" {
     pub fn umap_mlp_predict_device(m: *mut umap_mlp, dev_x: *const f32, rows: u64, dev_y: *mut f32) -> c_int;
     pub fn umap_mlp_free(m: *mut umap_mlp) -> c_int;
     pub fn umap_gemm_bf16_device(dev_a: *const c_void, dev_b: *const c_void, dev_c: *mut f32, m: u64, n: u64, k: u64, k_splits: u64) -> c_int;
+    pub fn umap_warm_start_params_default(out: *mut umap_warm_start_params) -> c_int;
+    pub fn umap_warm_start_fit_device(cfg: *const umap_config, params: *const umap_warm_start_params, dev_data: *const f32, n_samples: u64, data_dim: u64, dev_knn_indices: *const u32, dev_knn_dists: *const f32, knn_cols: u64, dev_sub_rows: *const u32, n_sub: u64, dev_sub_knn_indices: *const u32, dev_sub_knn_dists: *const f32, dev_sub_init: *const f32, out: *mut *mut umap_fitted, phase_ms: *mut f32, mlp_losses: *mut f32) -> c_int;
 }

@@ -550,3 +550,55 @@ def test_persisting_l2_set_aside_released_with_the_last_optimizer(ub):
     import gc
     gc.collect()
     assert limit() == 0
+
+
+def test_relabelled_layout_is_the_same_fit(ub, oracle, monkeypatch):
+    """DRAM-bound fits rename their vertices into a locality order inside the SGD layout;
+    forced here on a 20,000-point swiss roll.  Only the order in which edges are processed may
+    change: the normalised init and the exported edges are bit-identical to the plain
+    layout's, schedule totals equal, the embedding comes back in the caller's vertex order
+    (recall and fuzzy cross-entropy within the bars against the oracle), and a checkpoint
+    round trip keeps the renamed layout working."""
+    from umap_b200 import quality as Q
+    from umap_b200 import workloads as W
+    X, _ = W.swiss_roll(20000, seed=8)
+    idx, dist = W.knn_exact_numpy(X, 15)
+    init = W.uniform_init(20000, seed=3)
+    cfg = ub.UmapConfig()
+    cfg.optimization.n_epochs = 200
+    monkeypatch.setenv("UMAP_B200_RELABEL", "1")
+    opt_r = ub.Optimizer(ub.Umap(cfg).learn_manifold(20000, idx, dist), init, 200, cfg)
+    monkeypatch.setenv("UMAP_B200_RELABEL", "0")
+    opt_p = ub.Optimizer(ub.Umap(cfg).learn_manifold(20000, idx, dist), init, 200, cfg)
+    monkeypatch.delenv("UMAP_B200_RELABEL")
+    assert np.array_equal(opt_r.embedding().view(np.uint32), opt_p.embedding().view(np.uint32))
+    er, ep = opt_r.export_edges(), opt_p.export_edges()
+    for a_, b_ in zip(er, ep):
+        assert np.array_equal(a_, b_)
+    assert opt_r.schedule_totals(0, 200) == opt_p.schedule_totals(0, 200)
+    opt_r.set_seed(3)
+    opt_r.step_epochs(100)
+    monkeypatch.setenv("UMAP_B200_RELABEL", "1")
+    opt_r = ub.Optimizer.from_bytes(opt_r.to_bytes())   # layout rebuilt (renamed) from the checkpoint
+    monkeypatch.delenv("UMAP_B200_RELABEL")
+    opt_r.step_epochs(100)
+    emb = opt_r.embedding()
+    ocfg = oracle.OracleConfig(n_epochs=200)
+    mo = oracle.learn_manifold(idx, dist, ocfg)
+    a, b = mo.info()["a"], mo.info()["b"]
+    h, t, _ = oracle.Optimizer(mo, init, 200, ocfg).edges()
+    ip, ix, dt = mo.graph()
+    ip = ip.astype(np.int64)
+    w = dt[ip[h.astype(np.int64)] + np.array([np.searchsorted(ix[ip[r]:ip[r + 1]], c) for r, c in zip(h, t)])]
+    rec_o, ce_o = [], []
+    for seed in (1, 2, 3):
+        oo = oracle.Optimizer(oracle.learn_manifold(idx, dist, ocfg), init, 200, ocfg, seed=seed)
+        oo.step_epochs(100)
+        oo.step_epochs(100)
+        e_o = oo.embedding()
+        rec_o.append(Q.knn_recall(e_o, idx))
+        ce_o.append(Q.fuzzy_cross_entropy(e_o, h, t, w, a, b))
+    r, c = Q.knn_recall(emb, idx), Q.fuzzy_cross_entropy(emb, h, t, w, a, b)
+    print(f"relabelled: recall {r:.4f} CE {c:.6g}; oracle recall {rec_o} CE {ce_o}")
+    assert abs(r - np.mean(rec_o)) <= 0.01
+    assert abs(c - np.mean(ce_o)) <= 0.01 * np.mean(ce_o)

@@ -10,9 +10,12 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <chrono>
+#include <exception>
 #include <mutex>
 #include <new>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/umap_b200.h"
@@ -537,6 +540,15 @@ void step_epochs_impl(umap_optimizer& o, uint64_t n_ep, int output_metric = UMAP
   const uint64_t nd = o.n * o.dim;
   float* live = o.emb2.p;
   float* snap = o.emb2.p + nd;
+  // A layout with renamed vertices runs the epochs on a working pair in its own vertex order
+  // (gathered here, scattered back below); the optimizer's embedding keeps the caller's order.
+  DevBuf<float> work;
+  if (o.layout.order.p) {
+    work.alloc(2 * nd, s);
+    permute_rows(o.emb2.p, o.layout.order.p, o.n, (uint32_t)o.dim, true, work.p, s);
+    live = work.p;
+    snap = work.p + nd;
+  }
   d2d(snap, live, nd, s);  // :314 embedding_copy
   const SgdParams p = sgd_params(o);
   cudaEvent_t ev[2];
@@ -584,6 +596,7 @@ void step_epochs_impl(umap_optimizer& o, uint64_t n_ep, int output_metric = UMAP
     }
   }
   UB_CUDA(cudaEventRecord(ev[1], s));
+  if (work.p) permute_rows(live, o.layout.order.p, o.n, (uint32_t)o.dim, false, o.emb2.p, s);
   cudaError_t se = cudaStreamSynchronize(s);
   if (exec) (void)cudaGraphExecDestroy(exec);
   UB_CUDA(se);
@@ -1185,6 +1198,170 @@ int copy_out(const Writer& w, uint8_t* buf, uint64_t cap, uint64_t* needed) {
   if (needed) *needed = w.b.size();
   if (buf && cap) memcpy(buf, w.b.data(), std::min<uint64_t>(cap, w.b.size()));
   return (buf && cap < w.b.size()) ? UMAP_ERR_INVALID_ARGUMENT : UMAP_OK;
+}
+
+// ------------------------------------------------------------------ learned warm start
+// Uniform floats in [0, 1) from a SplitMix64 stream (Steele, Lea, Flood, OOPSLA 2014): the
+// network's initial parameters and the default subsample init.
+struct HostUniform {
+  uint64_t x;
+  explicit HostUniform(uint64_t seed) : x(seed) {}
+  float next() {
+    uint64_t z = (x += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    return (float)(z >> 40) * (1.0f / 16777216.0f);
+  }
+};
+
+// Flat parameters W1, b1, W2, b2, W3, b3 drawn like a default linear layer:
+// U(-1/sqrt(fan_in), 1/sqrt(fan_in)) for weights and biases.
+std::vector<float> mlp_initial_params(int in_dim, int out_dim, uint64_t seed) {
+  std::vector<float> p;
+  p.reserve((size_t)Mlp::param_count(in_dim, out_dim));
+  HostUniform u(seed ^ 0x6D6C705F696E6974ull);
+  const int fan[3][2] = {{in_dim, 256}, {256, 256}, {256, out_dim}};
+  for (const auto& f : fan) {
+    const float bound = 1.0f / sqrtf((float)f[0]);
+    for (int i = 0; i < f[1] * f[0] + f[1]; ++i) p.push_back(bound * (2.0f * u.next() - 1.0f));
+  }
+  return p;
+}
+
+std::unique_ptr<umap_fitted> warm_start_impl(const umap_config& c, const umap_warm_start_params& wp,
+                                             const float* data, uint64_t n, uint64_t d, const uint32_t* idx,
+                                             const float* dist, uint64_t k, const uint32_t* sub_rows,
+                                             uint64_t n_sub, const uint32_t* sub_idx, const float* sub_dist,
+                                             const float* sub_init, float* phase_ms, float* losses) {
+  using clk = std::chrono::steady_clock;
+  const auto ms_since = [](clk::time_point t) {
+    return std::chrono::duration<float, std::milli>(clk::now() - t).count();
+  };
+  const uint64_t dim = c.n_components;
+  if (d < 1 || d > 4096) throw Error(INVALID_ARGUMENT, "data_dim must be 1..4096, got " + std::to_string(d));
+  if (dim < 1 || dim > 4) throw Error(INVALID_ARGUMENT, "the warm start's network predicts 1..4 components");
+  if (n_sub < 128 || n_sub > n) throw Error(INVALID_ARGUMENT, "the subsample must have 128..n_samples rows");
+  if (wp.sub_epochs < 1 || wp.epochs < 1 || wp.mlp_epochs < 1)
+    throw Error(INVALID_ARGUMENT, "sub_epochs, epochs and mlp_epochs must be positive");
+  std::string err = validate_parameters(c, n, n, k);
+  if (!err.empty()) throw Error(INVALID_ARGUMENT, err);
+  int dev = 0;
+  UB_CUDA(cudaGetDevice(&dev));
+  float ph[UMAP_WARM_START_PHASES] = {};
+  const auto t_start = clk::now();
+  auto t0 = t_start;
+  umap_config cfg_full = c;
+  cfg_full.has_n_epochs = 1;
+  cfg_full.n_epochs = wp.epochs;
+  if (wp.has_learning_rate) cfg_full.learning_rate = wp.learning_rate;
+  umap_config cfg_sub = c;
+  cfg_sub.has_n_epochs = 1;
+  cfg_sub.n_epochs = wp.sub_epochs;
+
+  // The full graph does not depend on the initial embedding: built on its own stream and
+  // host thread while the subsample is fitted and the network trained.
+  std::unique_ptr<umap_manifold> full;
+  std::exception_ptr full_err;
+  float full_ms = 0.0f;
+  std::thread worker([&] {
+    try {
+      UB_CUDA(cudaSetDevice(dev));
+      const auto tg = clk::now();
+      full = learn_manifold_impl(cfg_full, n, idx, dist, n, k);
+      UB_CUDA(cudaStreamSynchronize(full->s()));
+      full_ms = ms_since(tg);
+    } catch (...) {
+      full_err = std::current_exception();
+    }
+  });
+  struct Join {
+    std::thread& t;
+    ~Join() { if (t.joinable()) t.join(); }
+  } join{worker};
+
+  Stream st;
+  cudaStream_t s = st.s;
+  const uint64_t dp = (d + 63) / 64 * 64;
+  DevBuf<float> sub(n_sub * dp, s);
+  pad_gather_rows(data, d, dp, sub_rows, n_sub, sub.p, s);
+  DevBuf<float> sinit;
+  if (!sub_init) {
+    std::vector<float> h(n_sub * dim);
+    HostUniform u(wp.seed);
+    for (float& v : h) v = -10.0f + 20.0f * u.next();
+    sinit.alloc(n_sub * dim, s);
+    h2d(sinit.p, h.data(), h.size(), s);
+    sub_init = sinit.p;
+  }
+  UB_CUDA(cudaStreamSynchronize(s));
+  ph[0] = ms_since(t0);
+  t0 = clk::now();
+
+  auto fsub = fit_impl(cfg_sub, n_sub, sub_idx, sub_dist, n_sub, k, sub_init, n_sub, dim, false);
+  const float* y = fsub->embedding.p;
+  // rows whose graph row is empty come back NaN: train on the others
+  DevBuf<uint32_t> keep(n_sub, s);
+  DevBuf<uint64_t> pos(n_sub + 1, s);
+  finite_rows(y, n_sub, (uint32_t)dim, keep.p, s);
+  scan_u32_to_u64(keep.p, pos.p, n_sub, s);
+  uint64_t n_keep = 0;
+  d2h(&n_keep, pos.p + n_sub, 1, s);
+  UB_CUDA(cudaStreamSynchronize(s));
+  DevBuf<float> xk, yk;
+  const float* xt = sub.p;
+  if (n_keep < n_sub) {
+    xk.alloc(n_keep * dp, s);
+    yk.alloc(n_keep * dim, s);
+    compact_rows(sub.p, n_sub, dp, keep.p, pos.p, xk.p, s);
+    compact_rows(y, n_sub, dim, keep.p, pos.p, yk.p, s);
+    xt = xk.p;
+    y = yk.p;
+  }
+  if (n_keep < 128) throw Error(INVALID_ARGUMENT, "fewer than 128 subsample rows have a non-empty graph row");
+  UB_CUDA(cudaStreamSynchronize(s));
+  ph[1] = ms_since(t0);
+  t0 = clk::now();
+
+  const std::vector<float> params = mlp_initial_params((int)dp, (int)dim, wp.seed);
+  Mlp net((int)dp, (int)dim, params.data(), s);
+  net.fit_input_norm(xt, (int64_t)n_keep);
+  const uint64_t batch = std::min<uint64_t>(wp.batch, n_keep) / 128 * 128;
+  std::vector<float> loss(wp.mlp_epochs);
+  net.train(xt, y, (int64_t)n_keep, (int)wp.mlp_epochs, (int64_t)batch, wp.mlp_learning_rate, wp.seed, loss.data());
+  if (losses) memcpy(losses, loss.data(), loss.size() * sizeof(float));
+  UB_CUDA(cudaStreamSynchronize(s));
+  ph[2] = ms_since(t0);
+  t0 = clk::now();
+  fsub.reset();
+  xk.reset();
+  yk.reset();
+  sub.reset();
+
+  DevBuf<float> xpad;
+  const float* x = data;
+  if (dp != d) {
+    xpad.alloc(n * dp, s);
+    pad_gather_rows(data, d, dp, nullptr, n, xpad.p, s);
+    x = xpad.p;
+  }
+  DevBuf<float> init(n * dim, s);
+  net.predict(x, (int64_t)n, init.p);
+  UB_CUDA(cudaStreamSynchronize(s));
+  xpad.reset();
+  ph[3] = ms_since(t0);
+  t0 = clk::now();
+
+  worker.join();
+  if (full_err) std::rethrow_exception(full_err);
+  ph[4] = ms_since(t0);
+  t0 = clk::now();
+  auto fitted = fit_manifold_impl(cfg_full, std::move(full), init.p, n, dim, false);
+  ph[5] = ms_since(t0);
+  ph[6] = full_ms;
+  ph[7] = ms_since(t_start);
+  if (phase_ms) memcpy(phase_ms, ph, sizeof ph);
+  return fitted;
 }
 
 }  // namespace
@@ -2262,6 +2439,38 @@ int umap_mlp_free(umap_mlp* m) {
     m->stream->activate();
     delete m;
   }
+  API_END
+}
+
+int umap_warm_start_params_default(umap_warm_start_params* out) {
+  API_BEGIN
+  need(out, "out");
+  *out = umap_warm_start_params{};
+  out->sub_epochs = 500;
+  out->epochs = 100;
+  out->mlp_epochs = 20;
+  out->batch = 4096;
+  out->mlp_learning_rate = 1e-3f;
+  out->has_learning_rate = 0;
+  out->learning_rate = 1.0f;
+  out->seed = 0;
+  API_END
+}
+
+int umap_warm_start_fit_device(const umap_config* cfg, const umap_warm_start_params* params, const float* data,
+                               uint64_t n_samples, uint64_t data_dim, const uint32_t* knn_indices,
+                               const float* knn_dists, uint64_t knn_cols, const uint32_t* sub_rows, uint64_t n_sub,
+                               const uint32_t* sub_knn_indices, const float* sub_knn_dists, const float* sub_init,
+                               umap_fitted** out, float* phase_ms, float* mlp_losses) {
+  API_BEGIN
+  need(cfg, "config"); need(params, "params"); need(data, "data"); need(knn_indices, "knn_indices");
+  need(knn_dists, "knn_dists"); need(sub_rows, "sub_rows"); need(sub_knn_indices, "sub_knn_indices");
+  need(sub_knn_dists, "sub_knn_dists"); need(out, "out");
+  *out = nullptr;
+  wait_for_inputs();
+  *out = warm_start_impl(*cfg, *params, data, n_samples, data_dim, knn_indices, knn_dists, knn_cols, sub_rows, n_sub,
+                         sub_knn_indices, sub_knn_dists, sub_init, phase_ms, mlp_losses)
+             .release();
   API_END
 }
 

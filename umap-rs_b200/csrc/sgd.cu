@@ -528,29 +528,33 @@ __global__ void segment_max_kernel(const uint64_t* __restrict__ indptr, const fl
   }
 }
 
+// Row u of the layout is row order[u] of the kept-edge CSR (order null: the same row).
 __global__ void ptr_degree_kernel(const uint64_t* __restrict__ kptr, uint64_t n, uint32_t chunk,
-                                  uint32_t* __restrict__ deg, uint32_t* __restrict__ ntask) {
-  const uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= n) return;
+                                  const uint32_t* __restrict__ order, uint32_t* __restrict__ deg,
+                                  uint32_t* __restrict__ ntask) {
+  const uint64_t u = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= n) return;
+  const uint64_t r = order ? order[u] : u;
   const uint32_t d = (uint32_t)(kptr[r + 1] - kptr[r]);
-  deg[r] = d;
-  ntask[r] = (d + chunk - 1) / chunk;
+  deg[u] = d;
+  ntask[u] = (d + chunk - 1) / chunk;
 }
 
 // One task per chunk of a row: row id, first kept-edge index, length, split flag.
 __global__ void task_fill_kernel(const uint64_t* __restrict__ kptr, const uint32_t* __restrict__ deg,
                                  const uint64_t* __restrict__ tptr, uint64_t n, uint32_t chunk,
                                  const uint32_t* __restrict__ row_seg, int len_bits,
-                                 uint32_t* __restrict__ trow, uint64_t* __restrict__ tstart,
-                                 uint32_t* __restrict__ tkey) {
+                                 const uint32_t* __restrict__ order, uint32_t* __restrict__ trow,
+                                 uint64_t* __restrict__ tstart, uint32_t* __restrict__ tkey) {
   const uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= n) return;
+  const uint64_t src = order ? order[r] : r;  // the kept-edge CSR row of layout row r
   const uint32_t d = deg[r];
   const uint64_t t0 = tptr[r], nt = tptr[r + 1] - t0;
   for (uint64_t c = 0; c < nt; ++c) {
     const uint32_t len = (uint32_t)min((uint64_t)chunk, (uint64_t)d - c * chunk);
     trow[t0 + c] = (uint32_t)r | (nt > 1 ? 0x80000000u : 0u);   // high bit: partial row
-    tstart[t0 + c] = kptr[r] + c * chunk;
+    tstart[t0 + c] = kptr[src] + c * chunk;
     // ascending key = descending length; batched instances sort instance-major first
     tkey[t0 + c] = (row_seg ? (row_seg[r] << len_bits) : 0u) | (chunk - len);
   }
@@ -582,7 +586,7 @@ __global__ void slice_fill_kernel(const uint32_t* __restrict__ ktail, const doub
                                   const uint32_t* __restrict__ skey, uint64_t T, uint32_t chunk,
                                   uint32_t len_mask, const uint64_t* __restrict__ wscan,
                                   const uint32_t* __restrict__ width, uint64_t n_slices, bool lane_major,
-                                  uint2* __restrict__ entry) {
+                                  const uint32_t* __restrict__ rank, uint2* __restrict__ entry) {
   const uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= n_slices * 32) return;
   const uint64_t s = q >> 5;
@@ -595,7 +599,7 @@ __global__ void slice_fill_kernel(const uint32_t* __restrict__ ktail, const doub
     const uint32_t len = chunk - (skey[q] & len_mask);
     for (; e < len; ++e)
       entry[lane_major ? base + (uint64_t)lane * wd + e : base + (uint64_t)e * 32 + lane] =
-          make_uint2(ktail[st + e], q_minus_1(keps[st + e]));
+          make_uint2(rank ? rank[ktail[st + e]] : ktail[st + e], q_minus_1(keps[st + e]));
   }
   for (; e < wd; ++e)
     entry[lane_major ? base + (uint64_t)lane * wd + e : base + (uint64_t)e * 32 + lane] = make_uint2(0u, 0u);
@@ -843,10 +847,29 @@ bool pick_lane_major(uint64_t n, bool segmented) {
   return segmented || n <= 4000000ull;
 }
 
+// Whether a plain fit's layout renames its vertices into a locality order (order.cu): where
+// every random access is a DRAM access, i.e. the sizes that take interleaved entries.
+// UMAP_B200_RELABEL=0 / 1 forces either.
+bool pick_relabel(uint64_t n, bool segmented) {
+  if (segmented) return false;
+  if (const char* e = getenv("UMAP_B200_RELABEL")) {
+    if (e[0] == '0') return false;
+    if (e[0] == '1') return true;
+  }
+  return n > 4000000ull;
+}
+
 void build_sgd_layout(const uint64_t* kept_ptr, const uint32_t* ktail, const double* keps, uint64_t n,
                       uint32_t chunk, SgdLayout& L, cudaStream_t s, const Segments* seg) {
   L.n_vertices = n;
   L.lane_major = pick_lane_major(n, seg != nullptr);
+  DevBuf<uint32_t> rank;
+  L.order.reset();
+  if (n && pick_relabel(n, seg != nullptr)) {
+    L.order.alloc(n, s);
+    rank.alloc(n, s);
+    locality_order(kept_ptr, ktail, n, L.order.p, rank.p, s);
+  }
   uint64_t n_edges = 0;
   UB_CUDA(cudaMemcpyAsync(&n_edges, kept_ptr + n, 8, cudaMemcpyDeviceToHost, s));
   UB_CUDA(cudaStreamSynchronize(s));
@@ -854,7 +877,7 @@ void build_sgd_layout(const uint64_t* kept_ptr, const uint32_t* ktail, const dou
   L.chunk = chunk ? chunk : pick_chunk(n_edges);
   DevBuf<uint32_t> deg(n, s), ntask(n, s);
   if (n) {
-    ptr_degree_kernel<<<grid_for(n, 256), 256, 0, s>>>(kept_ptr, n, L.chunk, deg.p, ntask.p);
+    ptr_degree_kernel<<<grid_for(n, 256), 256, 0, s>>>(kept_ptr, n, L.chunk, L.order.p, deg.p, ntask.p);
     UB_LAUNCH_CHECK();
   }
   DevBuf<uint32_t> dmax(1, s);
@@ -875,8 +898,8 @@ void build_sgd_layout(const uint64_t* kept_ptr, const uint32_t* ktail, const dou
   if ((uint64_t)n_seg << len_bits >= (1ull << 32)) throw Error(UNSUPPORTED, "too many instances for the task sort key");
   if (n) {
     task_fill_kernel<<<grid_for(n, 256), 256, 0, s>>>(kept_ptr, deg.p, tptr.p, n, L.chunk,
-                                                      seg ? seg->row_seg : nullptr, len_bits, trow.p,
-                                                      tstart.p, tkey.p);
+                                                      seg ? seg->row_seg : nullptr, len_bits, L.order.p,
+                                                      trow.p, tstart.p, tkey.p);
     UB_LAUNCH_CHECK();
   }
   if (T) radix_sort_pairs(tkey.p, nullptr, skey.p, perm.p, T, len_bits + (n_seg ? bits_for(n_seg) : 0), s);
@@ -903,7 +926,7 @@ void build_sgd_layout(const uint64_t* kept_ptr, const uint32_t* ktail, const dou
     slice_fill_kernel<<<grid_for(L.n_slices * 32, 256), 256, 0, s>>>(ktail, keps, perm.p, tstart.p, skey.p, T,
                                                                         L.chunk, len_mask, wscan.p,
                                                                         L.slice_width.p, L.n_slices,
-                                                                        L.lane_major, L.entry.p);
+                                                                        L.lane_major, rank.p, L.entry.p);
     UB_LAUNCH_CHECK();
   }
   // slice_base = 32 * wscan (entries, not widths)
@@ -950,8 +973,10 @@ void sgd_epoch(const SgdLayout& L, float* live, float* snap, const SgdParams& p,
 #define UB_SGD_WIDE(D, GEN)                                                                   \
   if (L.lane_major) sgd_epoch_kernel2<D, GEN, NB_WIDE, MINB_WIDE, true><<<grid, bt, 0, s>>>(UB_SGD_ARGS); \
   else sgd_epoch_kernel2<D, GEN, NB_WIDE, MINB_WIDE, false><<<grid, bt, 0, s>>>(UB_SGD_ARGS)
-// short graphs always have lane-major entries (pick_lane_major)
-#define UB_SGD_SHORT(D, GEN) sgd_epoch_kernel2<D, GEN, NB_SHORT, MINB_SHORT, true><<<grid, bt, 0, s>>>(UB_SGD_ARGS)
+// short graphs are small, so lane major by default (pick_lane_major); both orders are built
+#define UB_SGD_SHORT(D, GEN)                                                                    \
+  if (L.lane_major) sgd_epoch_kernel2<D, GEN, NB_SHORT, MINB_SHORT, true><<<grid, bt, 0, s>>>(UB_SGD_ARGS); \
+  else sgd_epoch_kernel2<D, GEN, NB_SHORT, MINB_SHORT, false><<<grid, bt, 0, s>>>(UB_SGD_ARGS)
 #define UB_SGD_DISPATCH(GEN, SHORT)                                                   \
   switch (p.dim) {                                                                    \
     case 1: if (SHORT) UB_SGD_SHORT(1, GEN); else UB_SGD_WIDE(1, GEN); break;         \
@@ -965,7 +990,7 @@ void sgd_epoch(const SgdLayout& L, float* live, float* snap, const SgdParams& p,
   if (p.generic_metric) {
     UB_SGD_DISPATCH(true, false)
   } else {
-    UB_SGD_DISPATCH(false, L.short_epoch && L.lane_major)
+    UB_SGD_DISPATCH(false, L.short_epoch)
   }
 #undef UB_SGD_DISPATCH
 #undef UB_SGD_SHORT

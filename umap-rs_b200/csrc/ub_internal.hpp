@@ -186,6 +186,10 @@ struct SgdLayout {
   DevBuf<uint32_t> split_mask;   // [n_slices]
   DevBuf<uint32_t> rowid;        // [n_slices * 32]; 0xFFFFFFFF = padding lane
   DevBuf<uint2> entry;           // [n_entries] {tail, Q - 1}
+  // Renamed vertices (DRAM-bound plain fits, see order.cu; empty otherwise): rowid and entry
+  // tails are new ids, vertex order[u] of the caller is vertex u of the layout, and the epoch
+  // loop runs on a working copy of the embedding permuted into that order.
+  DevBuf<uint32_t> order;        // [n_vertices] or empty
 };
 
 struct SgdParams {
@@ -245,6 +249,20 @@ void normalize_init(float* emb, uint64_t n, uint32_t dim, cudaStream_t s,
 void sgd_epoch(const SgdLayout& L, float* live, float* snap, const SgdParams& p,
                uint32_t epoch, float alpha, cudaStream_t s);
 // Exact totals of fired edges / negatives over epochs [start, end).
+// Warm-start row helpers (warm.cu): rows (or rows[i]) of x [*, d] zero-padded to dp columns;
+// keep[r] = 1 for rows of y [n, dim] without NaN/inf; rows with keep set moved to pos[r].
+void pad_gather_rows(const float* x, uint64_t d, uint64_t dp, const uint32_t* rows, uint64_t count, float* out,
+                     cudaStream_t s);
+void finite_rows(const float* y, uint64_t n, uint32_t dim, uint32_t* keep, cudaStream_t s);
+void compact_rows(const float* src, uint64_t n, uint64_t width, const uint32_t* keep, const uint64_t* pos,
+                  float* dst, cudaStream_t s);
+// Locality order of a graph's vertices (order.cu): order[u] = old id of new vertex u,
+// rank = its inverse.
+void locality_order(const uint64_t* kptr, const uint32_t* ktail, uint64_t n, uint32_t* order, uint32_t* rank,
+                    cudaStream_t s);
+// Rows of an n x dim array into the new order (to_new: dst[u] = src[order[u]]) or back.
+void permute_rows(const float* src, const uint32_t* order, uint64_t n, uint32_t dim, bool to_new, float* dst,
+                  cudaStream_t s);
 // Negative samples of the SGD epoch's generator (see negative_draws_kernel in sgd.cu).
 void negative_draws(uint64_t seed, uint64_t first, uint64_t count, uint32_t epoch, uint32_t per, uint32_t lo,
                     uint32_t range, uint32_t* out, cudaStream_t s);

@@ -30,6 +30,18 @@ class UmapConfigC(C.Structure):
     ]
 
 
+class WarmStartParamsC(C.Structure):
+    """Mirror of `umap_warm_start_params` (include/umap_b200.h)."""
+    _fields_ = [
+        ("sub_epochs", u64), ("epochs", u64), ("mlp_epochs", u64), ("batch", u64),
+        ("mlp_learning_rate", f32), ("has_learning_rate", C.c_int32), ("learning_rate", f32),
+        ("seed", u64),
+    ]
+
+
+WARM_START_PHASES = ("prepare", "subsample_fit", "mlp_train", "mlp_predict", "wait_full_graph", "fit",
+                     "full_graph_overlapped", "total")
+
 # name -> (argtypes) ; every function returns int status
 SIGNATURES = {
     "umap_config_default": [C.POINTER(UmapConfigC)],
@@ -96,6 +108,9 @@ SIGNATURES = {
     "umap_radix_sort_pairs_device_noalloc": [P, P, P, P, u64, i32, P],
     "umap_sgd_negative_draws_device": [u64, u64, u64, u32, u32, u32, u32, P],
     "umap_sgd_negatives_per_firing_device": [P, P, u64, u32, P],
+    "umap_warm_start_params_default": [C.POINTER(WarmStartParamsC)],
+    "umap_warm_start_fit_device": [C.POINTER(UmapConfigC), C.POINTER(WarmStartParamsC), P, u64, u64, P, P, u64,
+                                   P, u64, P, P, P, PP, P, P],
     "umap_radix_sort_noalloc_max_pairs": [C.POINTER(u64)],
     "umap_fit_manifold": [P, C.POINTER(UmapConfigC), P, u64, u64, PP],
     "umap_fit_manifold_device": [P, C.POINTER(UmapConfigC), P, u64, u64, PP],

@@ -9,20 +9,18 @@ semantics for that epoch count: `Optimizer::new` prunes at max_w / total_epochs
 (optimizer.rs:96-102) and the learning rate decays from `learning_rate` over the shorter run.
 
 Everything here runs through the library's C ABI: `umap_mlp_*` for the network (forward,
-backward and Adam are the library's own kernels) and `umap_fit_device` / `umap_learn_manifold_device` + `umap_fit_manifold_device` for the
-fits.  The
-caller supplies the subsample's kNN, as it supplies the kNN of the full data set.
+backward and Adam are the library's own kernels) and `umap_warm_start_fit_device` for the
+whole pipeline.  The caller supplies the subsample's kNN, as it supplies the kNN of the full
+data set.
 """
 from __future__ import annotations
 
-import copy
 import ctypes as C
-import time
 
 import numpy as np
 
 from . import _lib
-from . import (ERR_INVALID_ARGUMENT, FittedUmap, Umap, UmapConfig, UmapError, _check, _Handle)
+from . import (ERR_INVALID_ARGUMENT, FittedUmap, UmapConfig, UmapError, _check, _Handle)
 
 HIDDEN = 256
 
@@ -158,100 +156,67 @@ def gemm_bf16(a, b, k_splits: int = 1):
     return c
 
 
-def _pad64(x):
-    """Zero-pads feature columns to a multiple of 64 (the network's input tile)."""
-    import torch
-    d = x.shape[1]
-    if d % 64 == 0:
-        return x
-    return torch.nn.functional.pad(x, (0, 64 - d % 64))
-
-
-def _with_epochs(config: UmapConfig, n_epochs: int, learning_rate: float | None) -> UmapConfig:
-    c = copy.deepcopy(config)
-    c.optimization.n_epochs = n_epochs
-    if learning_rate is not None:
-        c.optimization.learning_rate = learning_rate
-    return c
-
-
 def warm_start_fit(config: UmapConfig, data, knn_indices, knn_dists, sub_index, sub_knn_indices, sub_knn_dists,
                    *, sub_init=None, sub_epochs: int = 500, epochs: int = 100, mlp_epochs: int = 20,
                    batch: int = 4096, mlp_lr: float = 1e-3, learning_rate: float | None = None, seed: int = 0,
                    info: dict | None = None) -> FittedUmap:
-    """Fit with a learned initial embedding.
+    """Fit with a learned initial embedding (umap_warm_start_fit_device: one call into the
+    library, which builds the full graph on another stream while it fits the subsample and
+    trains the network).
 
     data: CUDA f32 [n, d]; knn_*: the full data set's kNN (as for `Umap.fit`); sub_index:
-    CUDA int64 rows of the subsample; sub_knn_*: the subsample's own kNN (local ids).
-    The subsample is fitted plainly for `sub_epochs` from `sub_init` (uniform [-10, 10]^2,
-    seeded, when None); the network is trained on (data[sub_index], that embedding) for
+    CUDA integer rows of the subsample; sub_knn_*: the subsample's own kNN (local ids).
+    The subsample is fitted plainly for `sub_epochs` from `sub_init` (uniform [-10, 10]^2
+    from `seed` when None); the network is trained on (data[sub_index], that embedding) for
     `mlp_epochs` epochs of Adam; its predictions initialise a fit of all points for `epochs`
     epochs.  `info`, when given, receives per-phase wall times (ms) and the loss curve.
     """
-    import threading
-
     import torch
     data = _cuda_f32(data, "data")
-    t = {}
+    n, d = data.shape
     dev = data.device
-
-    def mark(name, t0):
-        torch.cuda.synchronize(dev)
-        t[name] = (time.perf_counter() - t0) * 1e3
-        return time.perf_counter()
-
+    ki, pki = _dev_u32(knn_indices, dev)
+    kd = _cuda_f32(knn_dists, "knn_dists")
+    rows, prows = _dev_u32(sub_index, dev)
+    si, psi = _dev_u32(sub_knn_indices, dev)
+    sd = _cuda_f32(sub_knn_dists, "sub_knn_dists")
+    n_sub = int(rows.shape[0])
+    sinit = None
+    if sub_init is not None:
+        sinit = _cuda_f32(sub_init if hasattr(sub_init, "is_cuda") else torch.from_numpy(np.asarray(sub_init)).to(dev),
+                          "sub_init")
+    wp = _lib.WarmStartParamsC()
+    L = _lib.load()
+    _check(L.umap_warm_start_params_default(C.byref(wp)))
+    wp.sub_epochs, wp.epochs, wp.mlp_epochs, wp.batch = sub_epochs, epochs, mlp_epochs, batch
+    wp.mlp_learning_rate = mlp_lr
+    wp.has_learning_rate = int(learning_rate is not None)
+    wp.learning_rate = 1.0 if learning_rate is None else learning_rate
+    wp.seed = seed
+    ph = np.zeros(len(_lib.WARM_START_PHASES), np.float32)
+    losses = np.zeros(max(mlp_epochs, 1), np.float32)
+    cfg = config.to_c()
+    out = C.c_void_p()
     torch.cuda.synchronize(dev)
-    t_start = t0 = time.perf_counter()
-    cfg_full = _with_epochs(config, epochs, learning_rate)
-    # The full graph does not depend on the initial embedding: build it on its own stream
-    # (another handle, another host thread) while the subsample is fitted and the network
-    # trained.
-    full = {}
-
-    def build_full_graph():
-        try:
-            tg = time.perf_counter()
-            full["manifold"] = Umap(cfg_full).learn_manifold(data, knn_indices, knn_dists)
-            full["ms"] = (time.perf_counter() - tg) * 1e3
-        except BaseException as e:  # re-raised on the calling thread
-            full["error"] = e
-
-    worker = threading.Thread(target=build_full_graph, name="umap-b200-full-graph")
-    worker.start()
-    try:
-        x = _pad64(data)
-        sub = x[sub_index]
-        n_sub = sub.shape[0]
-        dim = config.n_components
-        if sub_init is None:
-            g = np.random.default_rng(seed)
-            sub_init = torch.from_numpy(g.uniform(-10.0, 10.0, size=(n_sub, dim)).astype(np.float32)).to(dev)
-        t0 = mark("prepare", t0)
-        fitted_sub = Umap(_with_epochs(config, sub_epochs, None)).fit(sub, sub_knn_indices, sub_knn_dists, sub_init)
-        y = torch.from_numpy(fitted_sub.embedding()).to(dev)
-        del fitted_sub
-        keep = torch.isfinite(y).all(dim=1)  # rows with an empty graph row come back NaN
-        if not bool(keep.all()):
-            sub, y = sub[keep].contiguous(), y[keep].contiguous()
-        t0 = mark("subsample_fit", t0)
-        net = Mlp.create(x.shape[1], dim, seed=seed)
-        net.fit_input_norm(sub)
-        losses = net.train(sub, y, epochs=mlp_epochs, batch=min(batch, sub.shape[0] // 128 * 128), lr=mlp_lr,
-                           seed=seed)
-        t0 = mark("mlp_train", t0)
-        init = net.predict(x)
-        t0 = mark("mlp_predict", t0)
-    finally:
-        worker.join()
-    if "error" in full:
-        raise full["error"]
-    t0 = mark("wait_full_graph", t0)
-    fitted = Umap(cfg_full).fit_manifold(full.pop("manifold"), init)
-    mark("fit", t0)
-    t["full_graph_overlapped"] = full.get("ms", 0.0)
-    t["total"] = (time.perf_counter() - t_start) * 1e3
+    _check(L.umap_warm_start_fit_device(
+        C.byref(cfg), C.byref(wp), C.c_void_p(data.data_ptr()), n, d, pki, C.c_void_p(kd.data_ptr()),
+        int(kd.shape[1]), prows, n_sub, psi, C.c_void_p(sd.data_ptr()),
+        C.c_void_p(sinit.data_ptr()) if sinit is not None else None, C.byref(out),
+        ph.ctypes.data_as(C.c_void_p), losses.ctypes.data_as(C.c_void_p)))
+    fitted = FittedUmap(out.value)
     if info is not None:
-        info["ms"] = t
-        info["mlp_losses"] = losses.tolist()
-        info["n_sub"] = int(n_sub)
+        info["ms"] = {k: float(v) for k, v in zip(_lib.WARM_START_PHASES, ph)}
+        info["mlp_losses"] = losses[:mlp_epochs].tolist()
+        info["n_sub"] = n_sub
     return fitted
+
+
+def _dev_u32(x, dev):
+    """A CUDA int32 view of integer ids (u32 values; int64 input narrowed) and its pointer."""
+    import torch
+    t = x if hasattr(x, "is_cuda") else torch.from_numpy(np.ascontiguousarray(np.asarray(x).astype(np.int64)))
+    t = t.to(dev)
+    if t.dtype != torch.int32:
+        t = t.to(torch.int64).to(torch.int32)
+    t = t.contiguous()
+    return t, C.c_void_p(t.data_ptr())

@@ -314,7 +314,8 @@ int umap_sgd_negative_draws_device(uint64_t seed, uint64_t first_entry, uint64_t
 /* The SGD schedule's negative count per firing (optimize_layout_euclidean.rs:308-311, :343:
  * n_neg = floor((n - epoch_of_next_negative_sample) / epochs_per_negative_sample)), as the
  * epoch kernel evaluates it from an edge's stored schedule word dev_q[i] (ceil(2^32 /
- * epochs_per_sample) - 1) at epoch dev_epoch[i]; 0 where the edge does not fire then. */
+ * epochs_per_sample) - 1) at epoch dev_epoch[i] (below 2^21, the largest total_epochs an
+ * optimizer accepts); 0 where the edge does not fire then. */
 int umap_sgd_negatives_per_firing_device(const uint32_t* dev_q, const uint32_t* dev_epoch, uint64_t count,
                                          uint32_t negative_sample_rate, uint32_t* dev_out);
 
@@ -384,8 +385,9 @@ int umap_gemm_bf16_device(const void* dev_a, const void* dev_b, float* dev_c, ui
  * mlp_epochs of Adam on (subsample rows, that embedding), its prediction for every row as
  * init, then Umap::fit of all rows for `epochs` epochs (the prune threshold and the
  * learning-rate decay follow that epoch count, optimizer.rs:96-102, :317).  The full data's
- * graph is built on another stream and host thread while the subsample is fitted and the
- * network trained. */
+ * graph and that fit's optimizer set-up (prune, schedule, task layout) are built on another
+ * stream and host thread while the subsample is fitted and the network trained
+ * (full_graph_overlapped below times them). */
 typedef struct umap_warm_start_params {
   uint64_t sub_epochs;            /* 500: the subsample's plain fit */
   uint64_t epochs;                /* 100: the fit of all rows from the learned init */

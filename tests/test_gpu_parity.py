@@ -252,34 +252,59 @@ def test_nan_rows_for_disconnected_vertices(ub, oracle):
 
 
 # ---------------------------------------------------------------- embedding quality
+# Hogwild SGD is nondeterministic in the reference and here, so embeddings are compared by
+# their statistics against the oracle's own run-to-run spread (5 seeds, all host cores, as
+# Rayon's default pool uses).  Bars: every GPU run's 15-NN recall within 0.01 of the oracle's
+# mean and its fuzzy cross-entropy within 1%; the mean of the GPU runs' recall inside the
+# oracle's seed range widened by that range on each side.
+def _oracle_scores(oracle, idx, dist, init, epochs, metric_type=0, chunks=(None,)):
+    """(recalls, CEs, (head, tail, w), (a, b)) of 5 oracle fits; `chunks` = step_epochs calls."""
+    from umap_b200 import quality as Q
+    import os
+    ocfg = oracle.OracleConfig(n_epochs=epochs)
+    oracle.set_threads(os.cpu_count() or 8)
+    mo = oracle.learn_manifold(idx, dist, ocfg)
+    a, b = mo.info()["a"], mo.info()["b"]
+    head, tail, _ = oracle.Optimizer(mo, init, epochs, ocfg, seed=0).edges()
+    ip, ix, dt = mo.graph()
+    ip = ip.astype(np.int64)
+    h64 = head.astype(np.int64)
+    w = dt[ip[h64] + np.array([np.searchsorted(ix[ip[r]:ip[r + 1]], t) for r, t in zip(h64, tail)], np.int64)]
+    rec, ce = [], []
+    for seed in (1, 2, 3, 4, 5):
+        oo = oracle.Optimizer(oracle.learn_manifold(idx, dist, ocfg), init, epochs, ocfg, seed=seed,
+                              metric_type=metric_type)
+        for c in chunks:
+            oo.step_epochs(epochs if c is None else c)
+        emb = oo.embedding()
+        rec.append(Q.knn_recall(emb, idx))
+        ce.append(Q.fuzzy_cross_entropy(emb, head, tail, w, a, b))
+    return rec, ce, (head, tail, w), (a, b)
+
+
+def _assert_quality(res, rec_o, ce_o, what):
+    ro, co = float(np.mean(rec_o)), float(np.mean(ce_o))
+    spread = max(rec_o) - min(rec_o)
+    lo, hi = min(rec_o) - spread, max(rec_o) + spread
+    rg = float(np.mean([r for r, _ in res]))
+    print(f"{what}: oracle recall {np.round(rec_o, 5)} CE {np.round(ce_o, 0)}; "
+          f"gpu recall {[round(r, 5) for r, _ in res]} CE {[round(c, 0) for _, c in res]}")
+    for r, c in res:
+        assert abs(r - ro) <= 0.01, (what, r, ro)
+        assert abs(c - co) <= 0.01 * co, (what, c, co)
+    assert lo <= rg <= hi, (what, rg, lo, hi)
+
+
 def test_embedding_quality_matches_oracle(ub, oracle, gauss10k, monkeypatch):
-    """C0 workload (10k points, 200 epochs): GPU recall within 0.01 and fuzzy CE within 1%
-    of the oracle's (mean over 3 oracle seeds; the oracle's own spread is reported).  The
-    epoch kernel runs with both register budgets and both entry orders: the short-graph
-    budget with lane-major entries this size selects, and the large-graph budget with the
-    lane-interleaved entries of DRAM-bound sizes, forced."""
+    """10k-point Gaussian-mixture workload, 200 epochs.  The epoch kernel runs with both
+    register budgets and both entry orders: the short-graph budget with lane-major entries
+    this size selects, and the large-graph budget with the lane-interleaved entries of
+    DRAM-bound sizes, forced."""
     from umap_b200 import quality as Q
     idx, dist, init = gauss10k
     cfg = ub.UmapConfig()
     cfg.optimization.n_epochs = 200
-    ocfg = oracle.OracleConfig(n_epochs=200)
-    oracle.set_threads(8)
-    rec_o, ce_o = [], []
-    mo = oracle.learn_manifold(idx, dist, ocfg)
-    a, b = mo.info()["a"], mo.info()["b"]
-    opt0 = oracle.Optimizer(mo, init, 200, ocfg, seed=0)
-    head, tail, _ = opt0.edges()
-    ip, ix, dt = mo.graph()
-    ip = ip.astype(np.int64)
-    w = np.empty(len(head), np.float32)
-    for e in range(len(head)):
-        r = int(head[e])
-        seg = ix[ip[r]:ip[r + 1]]
-        w[e] = dt[ip[r] + int(np.searchsorted(seg, tail[e]))]
-    for seed in (1, 2, 3):
-        emb, _, _ = oracle.fit(idx, dist, init, ocfg, seed=seed)
-        rec_o.append(Q.knn_recall(emb, idx))
-        ce_o.append(Q.fuzzy_cross_entropy(emb, head, tail, w, a, b))
+    rec_o, ce_o, (head, tail, w), (a, b) = _oracle_scores(oracle, idx, dist, init, 200)
     res = []
     for short, seed in (("1", 1), ("1", 2), ("0", 1), ("0", 2)):
         # read when the optimizer is built
@@ -292,11 +317,31 @@ def test_embedding_quality_matches_oracle(ub, oracle, gauss10k, monkeypatch):
         opt.step_epochs(200)
         emb = opt.embedding()
         res.append((Q.knn_recall(emb, idx), Q.fuzzy_cross_entropy(emb, head, tail, w, a, b)))
-    ro, co = float(np.mean(rec_o)), float(np.mean(ce_o))
-    print(f"oracle recall {rec_o} CE {ce_o}; gpu {res}")
-    for r, c in res:
-        assert abs(r - ro) <= 0.01, (r, ro)
-        assert abs(c - co) <= 0.01 * co, (c, co)
+    _assert_quality(res, rec_o, ce_o, "gaussians 10k")
+
+
+def test_embedding_quality_on_a_structured_manifold(ub, oracle):
+    """A workload on which 15-NN recall can fail: a 20,000-point noisy swiss roll (3-D) whose
+    initial embedding is its own (angle, height) sheet coordinates, 200 epochs.  Recall stays
+    near 0.17 here (chance: 14 / 20,000 = 0.0007); an SGD that scrambles or fails to keep
+    the sheet's neighbourhoods falls far outside the oracle's band."""
+    from umap_b200 import quality as Q
+    from umap_b200 import workloads as W
+    X, t = W.swiss_roll(20000, seed=3)
+    idx, dist = W.knn_exact_numpy(X, 15)
+    init = np.stack([t, X[:, 1]], 1).astype(np.float32)
+    cfg = ub.UmapConfig()
+    cfg.optimization.n_epochs = 200
+    rec_o, ce_o, (head, tail, w), (a, b) = _oracle_scores(oracle, idx, dist, init, 200)
+    assert min(rec_o) > 0.1
+    res = []
+    for seed in (1, 2, 3):
+        opt = ub.Optimizer(ub.Umap(cfg).learn_manifold(20000, idx, dist), init, 200, cfg)
+        opt.set_seed(seed)
+        opt.step_epochs(200)
+        emb = opt.embedding()
+        res.append((Q.knn_recall(emb, idx), Q.fuzzy_cross_entropy(emb, head, tail, w, a, b)))
+    _assert_quality(res, rec_o, ce_o, "swiss roll 20k, sheet init")
 
 
 # ---------------------------------------------------------------- reference smoke tests

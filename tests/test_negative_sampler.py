@@ -171,14 +171,14 @@ def negatives_per_firing_exact(q, n, neg):
 def test_kernel_negative_counts_per_firing_are_exact(ub):
     """The epoch kernel's per-firing negative count against the exact closed form, on firing
     epochs of edges with epochs_per_sample in [1, 500] (the prune keeps eps <= total_epochs),
-    on non-firing epochs (0), at Q = 2^32 (an edge that fires every epoch), and for huge
-    epochs_per_sample (X up to 2^26 epochs, where the kernel's float estimate needs its exact
-    fallback)."""
+    on non-firing epochs (0), at Q = 2^32 (an edge that fires every epoch), and for
+    epochs_per_sample up to 2^20 with firing epochs below 2^21 (the largest total_epochs an
+    optimizer accepts), where the kernel's float estimate of the firing gap is least exact."""
     import torch
     g = np.random.Generator(np.random.PCG64(5))
     neg = 5
     eps = np.concatenate([g.uniform(1.0, 500.0, 400_000), np.round(g.uniform(1, 60, 20_000)),
-                          2.0 ** g.uniform(20, 26, 2_000)])
+                          2.0 ** g.uniform(14, 19.9, 2_000)])
     with np.errstate(over="ignore"):
         Q = np.minimum(np.ceil(2.0 ** 32 / eps), 2.0 ** 32).astype(np.uint64)
     Q[:1000] = 1 << 32

@@ -453,10 +453,26 @@ void compute_thresholds(umap_optimizer& o) {
 }
 
 // optimizer.rs:74-290.  `init` is a device array of n*dim floats on stream `s` (or host).
+// Optimizer::new up to, not including, the initial embedding (optimizer.rs:74-180): nothing
+// here depends on `init`, so a caller that computes init meanwhile can run this first.
+std::unique_ptr<umap_optimizer> optimizer_prepare_impl(std::unique_ptr<umap_manifold> man, uint64_t rows,
+                                                       uint64_t dims, uint64_t total_epochs, const umap_config& c,
+                                                       int metric_type);
+// optimizer.rs:181-230 on a prepared optimizer: the initial embedding, normalised.
+void optimizer_set_init_impl(umap_optimizer& o, const float* init, bool init_on_host);
+
 std::unique_ptr<umap_optimizer> optimizer_new_impl(std::unique_ptr<umap_manifold> man, const float* init,
                                                    bool init_on_host, uint64_t rows, uint64_t dims,
                                                    uint64_t total_epochs, const umap_config& c,
                                                    int metric_type) {
+  auto o = optimizer_prepare_impl(std::move(man), rows, dims, total_epochs, c, metric_type);
+  optimizer_set_init_impl(*o, init, init_on_host);
+  return o;
+}
+
+std::unique_ptr<umap_optimizer> optimizer_prepare_impl(std::unique_ptr<umap_manifold> man, uint64_t rows,
+                                                       uint64_t dims, uint64_t total_epochs, const umap_config& c,
+                                                       int metric_type) {
   if (metric_type != UMAP_METRIC_EUCLIDEAN && metric_type != UMAP_METRIC_GENERIC)
     throw Error(INVALID_ARGUMENT, "unknown metric_type");
   if (rows != man->n_vertices)
@@ -466,6 +482,8 @@ std::unique_ptr<umap_optimizer> optimizer_new_impl(std::unique_ptr<umap_manifold
   if (man->n_vertices >= 0xFFFFFFFFull) throw Error(UNSUPPORTED, "n_vertices must be < 2^32");
   if ((total_epochs + 1) * (c.negative_sample_rate + 1) >= 0xFFFFFFFFull)
     throw Error(UNSUPPORTED, "total_epochs * negative_sample_rate must be < 2^32");
+  if (total_epochs > MAX_EPOCHS)
+    throw Error(UNSUPPORTED, "total_epochs must be at most " + std::to_string(MAX_EPOCHS) + " on this build");
   auto o = std::make_unique<umap_optimizer>();
   o->manifold = std::move(man);
   cudaStream_t s = o->s();
@@ -491,20 +509,26 @@ std::unique_ptr<umap_optimizer> optimizer_new_impl(std::unique_ptr<umap_manifold
     build_sgd_layout(K.ptr.p, K.tail.p, K.eps.p, n, 0, o->layout, s);
     log.mark("optimizer task layout complete");
   }
-  // :181-230 normalise init
-  o->emb2.alloc(2 * n * dims, s);
-  if (init_on_host) h2d(o->emb2.p, init, n * dims, s);
-  else d2d(o->emb2.p, init, n * dims, s);
-  normalize_init(o->emb2.p, n, (uint32_t)dims, s);
-  log.mark("optimizer embedding normalization complete");
   if (log.on)
     fprintf(stderr, "[umap_b200] edges=%llu tasks=%llu split_tasks=%llu chunk=%u max_degree=%u entries=%llu\n",
             (unsigned long long)o->layout.n_edges, (unsigned long long)o->layout.n_tasks,
             (unsigned long long)o->layout.split_tasks, o->layout.chunk, o->layout.max_degree,
             (unsigned long long)o->layout.n_entries);
-  set_l2_window(*o, true);
   UB_CUDA(cudaStreamSynchronize(s));
   return o;
+}
+
+void optimizer_set_init_impl(umap_optimizer& o, const float* init, bool init_on_host) {
+  cudaStream_t s = o.s();
+  const uint64_t n = o.n, dims = o.dim;
+  PhaseLog log(s);
+  o.emb2.alloc(2 * n * dims, s);
+  if (init_on_host) h2d(o.emb2.p, init, n * dims, s);
+  else d2d(o.emb2.p, init, n * dims, s);
+  normalize_init(o.emb2.p, n, (uint32_t)dims, s);
+  log.mark("optimizer embedding normalization complete");
+  set_l2_window(o, true);
+  UB_CUDA(cudaStreamSynchronize(s));
 }
 
 SgdParams sgd_params(const umap_optimizer& o) {
@@ -777,6 +801,8 @@ std::unique_ptr<umap_optimizer> batch_new_impl(const umap_config& c, uint64_t n_
     throw Error(UNSUPPORTED, "total points * n_neighbors must be < 2^32 on this build");
   if ((total_epochs + 1) * (c.negative_sample_rate + 1) >= 0xFFFFFFFFull)
     throw Error(UNSUPPORTED, "total_epochs * negative_sample_rate must be < 2^32");
+  if (total_epochs > MAX_EPOCHS)
+    throw Error(UNSUPPORTED, "total_epochs must be at most " + std::to_string(MAX_EPOCHS) + " on this build");
 
   cudaStream_t s0;
   UB_CUDA(cudaStreamCreateWithFlags(&s0, cudaStreamNonBlocking));
@@ -1031,6 +1057,8 @@ void finish_loaded_optimizer(umap_optimizer& o, const DevBuf<uint32_t>& head, co
   cudaStream_t s = o.s();
   const uint64_t n = o.manifold->n_vertices, E = head.n;
   if (o.current_epoch > o.total_epochs) throw Error(FORMAT, "current_epoch exceeds total_epochs");
+  if (o.total_epochs > MAX_EPOCHS)
+    throw Error(UNSUPPORTED, "total_epochs must be at most " + std::to_string(MAX_EPOCHS) + " on this build");
   if (o.metric_type != UMAP_METRIC_EUCLIDEAN && o.metric_type != UMAP_METRIC_GENERIC)
     throw Error(FORMAT, "invalid MetricType");
   std::vector<uint32_t> hh(E), tt(E);
@@ -1259,16 +1287,18 @@ std::unique_ptr<umap_fitted> warm_start_impl(const umap_config& c, const umap_wa
   cfg_sub.has_n_epochs = 1;
   cfg_sub.n_epochs = wp.sub_epochs;
 
-  // The full graph does not depend on the initial embedding: built on its own stream and
-  // host thread while the subsample is fitted and the network trained.
-  std::unique_ptr<umap_manifold> full;
+  // The full graph and the final fit's optimizer set-up (prune, schedule, task layout) do not
+  // depend on the initial embedding: built on their own stream and host thread while the
+  // subsample is fitted and the network trained.
+  std::unique_ptr<umap_optimizer> full;
   std::exception_ptr full_err;
   float full_ms = 0.0f;
   std::thread worker([&] {
     try {
       UB_CUDA(cudaSetDevice(dev));
       const auto tg = clk::now();
-      full = learn_manifold_impl(cfg_full, n, idx, dist, n, k);
+      full = optimizer_prepare_impl(learn_manifold_impl(cfg_full, n, idx, dist, n, k), n, dim, wp.epochs, cfg_full,
+                                    UMAP_METRIC_EUCLIDEAN);
       UB_CUDA(cudaStreamSynchronize(full->s()));
       full_ms = ms_since(tg);
     } catch (...) {
@@ -1356,7 +1386,12 @@ std::unique_ptr<umap_fitted> warm_start_impl(const umap_config& c, const umap_wa
   if (full_err) std::rethrow_exception(full_err);
   ph[4] = ms_since(t0);
   t0 = clk::now();
-  auto fitted = fit_manifold_impl(cfg_full, std::move(full), init.p, n, dim, false);
+  // the rest of Umap::fit (embedding.rs:311-337) on the prepared optimizer
+  optimizer_set_init_impl(*full, init.p, false);
+  step_epochs_impl(*full, wp.epochs);
+  auto fitted = into_fitted_impl(std::move(full), cfg_full);
+  nan_empty_rows(fitted->manifold->indptr.p, fitted->n, (uint32_t)fitted->dim, fitted->embedding.p, fitted->s());
+  UB_CUDA(cudaStreamSynchronize(fitted->s()));
   ph[5] = ms_since(t0);
   ph[6] = full_ms;
   ph[7] = ms_since(t_start);

@@ -100,10 +100,10 @@ __device__ __forceinline__ bool fires_at(uint32_t n, uint32_t q) {
 // y(n) - y(p) with y(x) = fires_by(x * neg) and p the epoch of the previous firing, or
 // y(n) - 1 for the first.  Firing m is at epoch ceil(m X), X = 2^32 / Q, so consecutive
 // firings are G = floor(X) or G + 1 epochs apart and p is n - G if the edge fires there, else
-// n - G - 1 (no firing fits in between).  G comes from a float estimate (relative error below
-// 2^-21), made exact by integer checks (G Q <= 2^32 < (G + 1) Q); a second firing needs
-// n >= 2X, so G < 2^31 here.  Estimates still off after two steps each way (X beyond about
-// 2^21 epochs) take the exact search instead.
+// n - G - 1 (no firing fits in between).  A second firing needs n >= 2X, and epochs are
+// below MAX_EPOCHS = 2^21 (checked on the host), so X < 2^20 here: the float estimate of X
+// (relative error below 2^-21, absolute below 0.5) is off by at most one after truncation,
+// and one integer check (G Q <= 2^32 < (G + 1) Q) makes G exact.
 __device__ __forceinline__ uint32_t negatives_at(uint32_t n, uint32_t q, uint32_t neg) {
   const uint32_t y = (uint32_t)fires_by(n * neg, q);
   const uint32_t m = (uint32_t)fires_by(n, q);
@@ -111,17 +111,9 @@ __device__ __forceinline__ uint32_t negatives_at(uint32_t n, uint32_t q, uint32_
   if (m > 1) {
     const uint64_t Q = (uint64_t)q + 1;
     uint32_t g = (uint32_t)__fdividef(4294967296.0f, (float)Q);
-#pragma unroll
-    for (int t = 0; t < 2; ++t)
-      if ((uint64_t)g * Q > 4294967296ull) --g;
-#pragma unroll
-    for (int t = 0; t < 2; ++t)
-      if ((uint64_t)(g + 1) * Q <= 4294967296ull) ++g;
-    uint32_t p;
-    if ((uint64_t)g * Q <= 4294967296ull && (uint64_t)(g + 1) * Q > 4294967296ull)
-      p = fires_at(n - g, q) ? n - g : n - g - 1;
-    else
-      p = fire_epoch(m - 1, q);
+    if ((uint64_t)g * Q > 4294967296ull) --g;
+    else if ((uint64_t)(g + 1) * Q <= 4294967296ull) ++g;
+    const uint32_t p = fires_at(n - g, q) ? n - g : n - g - 1;
     prev = (uint32_t)fires_by(p * neg, q);
   }
   return y > prev ? y - prev : 0u;
@@ -819,14 +811,17 @@ uint32_t pick_chunk(uint64_t n_edges) {
   return (uint32_t)std::min<uint64_t>(512, std::max<uint64_t>(16, c));
 }
 
-// Whether the epoch kernel takes the short-graph budget (the Euclidean rule in 2-D and 1-D): the
-// layout's warps (one per slice) fill at most two waves of the wide budget's resident warps
-// (SMs x 5 blocks x 8 warps).  UMAP_B200_SGD_SHORT=0 / 1 forces it.
-bool pick_short_epoch(uint64_t n_slices) {
+// Whether the epoch kernel takes the 8-negatives budget (the Euclidean rule in 2-D and 1-D):
+// where the layout's warps (one per slice) fill at most two waves of the wide budget's
+// resident warps (SMs x 5 blocks x 8 warps), and for renamed DRAM-bound layouts, where more
+// row loads in flight per lane hide DRAM latency (20M-point swiss roll, 30 epochs: 337.7 ->
+// 308.4 ms).  UMAP_B200_SGD_SHORT=0 / 1 forces it.
+bool pick_short_epoch(uint64_t n_slices, bool renamed) {
   if (const char* e = getenv("UMAP_B200_SGD_SHORT")) {
     if (e[0] == '0') return false;
     if (e[0] == '1') return true;
   }
+  if (renamed) return true;
   int dev = 0, sms = 0;
   UB_CUDA(cudaGetDevice(&dev));
   UB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
@@ -939,7 +934,7 @@ void build_sgd_layout(const uint64_t* kept_ptr, const uint32_t* ktail, const dou
   UB_CUDA(cudaStreamSynchronize(s));
   L.split_tasks = 0;
   for (uint32_t v : h) L.split_tasks += __builtin_popcount(v);
-  L.short_epoch = pick_short_epoch(L.n_slices);
+  L.short_epoch = pick_short_epoch(L.n_slices, L.order.p != nullptr);
 }
 
 void export_edges(const uint64_t* indptr, const uint32_t* indices, const float* data, uint64_t n,

@@ -174,6 +174,10 @@ void count_empty_rows(const uint64_t* indptr, const float* data, uint64_t n,
 // warp owns a slice, a lane owns a task.  Entry (e, lane) of slice s lives at
 // slice_base[s] + e*32 + lane as uint2 {tail, Q - 1}.  Bit `lane` of split_mask[s] is set
 // when the lane's task is a partial row (its head update is merged with an atomic add).
+// Largest total epoch count of an optimizer: keeps the epoch kernel's per-firing schedule
+// arithmetic exact in 32 bits (see negatives_at in sgd.cu).
+constexpr uint64_t MAX_EPOCHS = 1ull << 21;
+
 struct SgdLayout {
   uint64_t n_vertices = 0, n_edges = 0, n_entries = 0, n_slices = 0, n_tasks = 0;
   uint32_t max_degree = 0, chunk = 0;

@@ -540,6 +540,7 @@ def run_swiss_roll(a):
         opt = ub.Optimizer(m, init, a.swiss_epochs, cfg)
         if stats is not None:
             stats["E"] = opt.n_edges()
+            stats["layout"] = opt.layout()
             stats["FN"] = opt.schedule_totals(0, a.swiss_epochs)
             stats["free_after_setup"] = torch.cuda.mem_get_info()[0]
         opt.step_epochs(a.swiss_epochs)
@@ -600,7 +601,7 @@ def run_swiss_roll(a):
                        "l2": "embedding 800 MB and edge slices exceed L2"},
             "sgd_ms_per_fit": sgd_ms, "sgd_edge_updates_per_s": F_tot / (sgd_ms / 1e3),
             "graph_and_setup_ms": ms_step - sgd_ms,
-            "roofline": {"bound": "hbm", "kernel": "sgd_epoch_kernel2<2, false, 4, 5>", "achieved": achieved, "peak": hbm,
+            "roofline": {"bound": "hbm", "kernel": stats["layout"]["kernel"], "achieved": achieved, "peak": hbm,
                          "unit": "GB/s", "frac": achieved / hbm, "peak_source": hbm_src, "traffic": swiss_traffic(E),
                          "traffic_note": "DRAM bytes of one epoch-20 launch captured at 20M points, "
                                          "scaled by kept edges",
@@ -811,6 +812,7 @@ def main():
     o0 = ub.Optimizer(m0, d_init, a.epochs, cfg)
     E = o0.n_edges()
     F_tot, N_tot = o0.schedule_totals(0, a.epochs)
+    layout = o0.layout()
     del o0
     dim = 2
     alg_bytes = 4.0 * E * a.epochs + F_tot * (8 + 16 * dim) + 4.0 * dim * N_tot
@@ -883,7 +885,7 @@ def main():
         "sgd_edge_updates_per_s": F_tot / (float(np.median(sgd_ms)) / 1e3),
         "e2e": {"value": F_tot / (e2e_step / 1e3), "unit": "edge-updates/s", "ms_per_step": e2e_step,
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-        "roofline": {"bound": "hbm", "kernel": "sgd_epoch_kernel2<2, false, 4, 5>", "achieved": achieved,
+        "roofline": {"bound": "hbm", "kernel": layout["kernel"], "achieved": achieved,
                      "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "peak_source": peak_src,
                      "traffic": tr, "algorithmic_bytes_per_launch": alg_bytes / a.epochs,
                      "avg_launch_ms": sgd_kernel_ms, "l2": l2_counters()},

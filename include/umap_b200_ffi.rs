@@ -111,6 +111,7 @@ extern "C" {
     pub fn umap_batch_fit(cfg: *const umap_config, n_instances: u64, host_offsets: *const u64, host_knn_indices: *const u32, host_knn_dists: *const f32, knn_cols: u64, host_init: *const f32, init_cols: u64, host_embedding_out: *mut f32) -> c_int;
     pub fn umap_batch_fit_device(cfg: *const umap_config, n_instances: u64, host_offsets: *const u64, dev_knn_indices: *const u32, dev_knn_dists: *const f32, knn_cols: u64, dev_init: *const f32, init_cols: u64, dev_embedding_out: *mut f32) -> c_int;
     pub fn umap_optimizer_tuning(opt: *const umap_optimizer, chunk: *mut u32, block_threads: *mut u32) -> c_int;
+    pub fn umap_optimizer_layout_flags(opt: *const umap_optimizer, flags: *mut u32) -> c_int;
     pub fn umap_manifold_serialize(m: *const umap_manifold, buf: *mut u8, cap: u64, needed: *mut u64) -> c_int;
     pub fn umap_manifold_deserialize(buf: *const u8, len: u64, out: *mut *mut umap_manifold) -> c_int;
     pub fn umap_optimizer_serialize(o: *const umap_optimizer, buf: *mut u8, cap: u64, needed: *mut u64) -> c_int;

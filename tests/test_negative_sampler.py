@@ -184,11 +184,11 @@ def test_kernel_negative_counts_per_firing_are_exact(ub):
     Q[:1000] = 1 << 32
     q = (Q - np.uint64(1)).astype(np.uint32)
     m = g.integers(1, 40, q.size).astype(np.uint64)
-    m[-2000:] = g.integers(1, 4, 2000)
+    m[-2000:] = g.integers(1, 3, 2000)                        # n = e_m < 2^21
     n = ((m << np.uint64(32)) + Q - np.uint64(1)) // Q        # firing epochs
     n[: 50_000] += np.uint64(1)                               # mostly not firing
     n = n.astype(np.uint32)
-    assert int(n.max()) * neg < 2 ** 32
+    assert int(n.max()) < 2 ** 21 and int(n.max()) * neg < 2 ** 32
     want = negatives_per_firing_exact(q, n, neg)
     tq = torch.from_numpy(q.view(np.int32)).cuda()
     tn = torch.from_numpy(n.view(np.int32)).cuda()

@@ -2210,6 +2210,16 @@ int umap_optimizer_tuning(const umap_optimizer* opt, uint32_t* chunk, uint32_t* 
   API_END
 }
 
+int umap_optimizer_layout_flags(const umap_optimizer* opt, uint32_t* flags) {
+  API_BEGIN
+  need(opt, "optimizer"); need(flags, "flags");
+  *flags = (opt->layout.lane_major ? UMAP_LAYOUT_LANE_MAJOR : 0u) |
+           (opt->layout.short_epoch ? UMAP_LAYOUT_EIGHT_NEGATIVES : 0u) |
+           (opt->layout.order.p ? UMAP_LAYOUT_RENAMED : 0u) |
+           (opt->metric_type == UMAP_METRIC_GENERIC ? UMAP_LAYOUT_GENERIC_RULE : 0u);
+  API_END
+}
+
 // ---- kernel-level entry points
 int umap_smooth_knn_dist_device(const float* dists, uint64_t n, uint64_t k, uint64_t n_iter,
                                 float local_connectivity, float bandwidth, float* sigmas, float* rhos) {

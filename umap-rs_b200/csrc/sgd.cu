@@ -98,25 +98,29 @@ __device__ __forceinline__ bool fires_at(uint32_t n, uint32_t q) {
 }
 // Negatives drawn by the firing at epoch n (n * neg < 2^32 is checked on the host):
 // y(n) - y(p) with y(x) = fires_by(x * neg) and p the epoch of the previous firing, or
-// y(n) - 1 for the first.  Firing m is at epoch ceil(m X), X = 2^32 / Q, so consecutive
-// firings are G = floor(X) or G + 1 epochs apart and p is n - G if the edge fires there, else
-// n - G - 1 (no firing fits in between).  A second firing needs n >= 2X, and epochs are
-// below MAX_EPOCHS = 2^21 (checked on the host), so X < 2^20 here: the float estimate of X
-// (relative error below 2^-21, absolute below 0.5) is off by at most one after truncation,
-// and one integer check (G Q <= 2^32 < (G + 1) Q) makes G exact.
+// y(n) - 1 for the first.  Firings are floor(2^32 / Q) or one more epochs apart, so p is found
+// among a few candidates below n - floor(2^32 / Q) + 1 with the cheap test above (the float
+// estimate of the gap is within one epoch: a second firing needs n >= 2 * 2^32 / Q and epochs
+// stay below MAX_EPOCHS = 2^21, checked on the host; fire_epoch is the exact fallback).
+// A two-candidate form with an exact integer gap (one fewer fires_at test, no fallback)
+// measured 1.7% slower on the 2M workload (317.6 against 312.3 ms per 500 epochs).
 __device__ __forceinline__ uint32_t negatives_at(uint32_t n, uint32_t q, uint32_t neg) {
-  const uint32_t y = (uint32_t)fires_by(n * neg, q);
-  const uint32_t m = (uint32_t)fires_by(n, q);
-  uint32_t prev = 1;
+  const int64_t y = (int64_t)fires_by(n * neg, q);
+  const uint64_t m = fires_by(n, q);
+  int64_t prev = 1;
   if (m > 1) {
-    const uint64_t Q = (uint64_t)q + 1;
-    uint32_t g = (uint32_t)__fdividef(4294967296.0f, (float)Q);
-    if ((uint64_t)g * Q > 4294967296ull) --g;
-    else if ((uint64_t)(g + 1) * Q <= 4294967296ull) ++g;
-    const uint32_t p = fires_at(n - g, q) ? n - g : n - g - 1;
-    prev = (uint32_t)fires_by(p * neg, q);
+    const int64_t g0 = (int64_t)__fdividef(4294967296.0f, (float)q + 1.0f);
+    uint32_t pe = 0;
+#pragma unroll
+    for (int t = 1; t >= -2; --t) {
+      const int64_t x = (int64_t)n - g0 + t;
+      if (pe == 0 && x >= 1 && x < (int64_t)n && fires_at((uint32_t)x, q)) pe = (uint32_t)x;
+    }
+    if (pe == 0) pe = fire_epoch(m - 1, q);
+    prev = (int64_t)fires_by(pe * neg, q);
   }
-  return y > prev ? y - prev : 0u;
+  const int64_t d = y - prev;
+  return d > 0 ? (uint32_t)d : 0u;
 }
 
 // Rust f32::clamp(-4, 4) (utils/clip.rs:13-15): NaN passes through.

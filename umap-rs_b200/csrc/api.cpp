@@ -506,7 +506,8 @@ std::unique_ptr<umap_optimizer> optimizer_prepare_impl(std::unique_ptr<umap_mani
     KeptEdges K;
     compute_kept_edges(*o, K, true, true);
     log.mark("optimizer edge filtering + epochs_per_sample complete");
-    build_sgd_layout(K.ptr.p, K.tail.p, K.eps.p, n, 0, o->layout, s);
+    build_sgd_layout(K.ptr.p, K.tail.p, K.eps.p, n,
+                     o->metric_type == UMAP_METRIC_GENERIC ? pick_chunk_generic(K.E) : 0, o->layout, s);
     log.mark("optimizer task layout complete");
   }
   if (log.on)
@@ -1071,7 +1072,8 @@ void finish_loaded_optimizer(umap_optimizer& o, const DevBuf<uint32_t>& head, co
   }
   DevBuf<uint64_t> ptr(n + 1, s);
   segment_starts(head.p, E, n, ptr.p, s);
-  build_sgd_layout(ptr.p, tail.p, eps.p, n, 0, o.layout, s);
+  build_sgd_layout(ptr.p, tail.p, eps.p, n, o.metric_type == UMAP_METRIC_GENERIC ? pick_chunk_generic(E) : 0,
+                   o.layout, s);
   set_l2_window(o, true);
   UB_CUDA(cudaStreamSynchronize(s));
 }

@@ -815,6 +815,19 @@ uint32_t pick_chunk(uint64_t n_edges) {
   return (uint32_t)std::min<uint64_t>(512, std::max<uint64_t>(16, c));
 }
 
+// The generic-metric rule (optimize_layout_generic.rs) attracts much harder than the
+// Euclidean one, and a row cut into tasks that all start from the same head position
+// overshoots where the reference applies the row's moves one after another: on the 10k-point
+// Gaussian workload (4 seeds each) 16-edge tasks gave 15-NN recall 0.0348 and fuzzy
+// cross-entropy 268,541 against the oracle's 0.0380 and 270,403; 32: 0.0356 / 268,666;
+// 64: 0.0369 / 269,976; 128 and whole rows: no further change.  The Euclidean rule showed no
+// such dependence at any task length.  So the generic rule keeps typical rows whole (tasks
+// of at least 64 edges, about three times a kNN graph's mean degree) and splits only hubs.
+uint32_t pick_chunk_generic(uint64_t n_edges) {
+  if (getenv("UMAP_B200_CHUNK")) return pick_chunk(n_edges);
+  return std::max<uint32_t>(64, pick_chunk(n_edges));
+}
+
 // Whether the epoch kernel takes the 8-negatives budget (the Euclidean rule in 2-D and 1-D):
 // where the layout's warps (one per slice) fill at most two waves of the wide budget's
 // resident warps (SMs x 5 blocks x 8 warps), and for renamed DRAM-bound layouts, where more

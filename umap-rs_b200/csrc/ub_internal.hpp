@@ -241,6 +241,10 @@ void export_state(const double* eps, uint64_t E, uint64_t neg_rate, uint64_t cur
                   double* eons, double* eonns, double* epns, cudaStream_t s);
 // Slice layout from kept edges (kept_ptr, tail, eps).  chunk = 0 picks the task length
 // from the edge count.
+// Task length for a layout of n_edges kept edges (sgd.cu; UMAP_B200_CHUNK overrides it), and
+// the one for the generic-metric rule, whose rows must stay whole tasks (see sgd.cu).
+uint32_t pick_chunk(uint64_t n_edges);
+uint32_t pick_chunk_generic(uint64_t n_edges);
 void build_sgd_layout(const uint64_t* kept_ptr, const uint32_t* tail, const double* eps,
                       uint64_t n, uint32_t chunk, SgdLayout& L, cudaStream_t s,
                       const Segments* seg = nullptr);

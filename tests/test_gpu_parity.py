@@ -497,37 +497,24 @@ def test_update_rules_match_oracle_on_pairs(ub, oracle, generic, dim):
 
 
 def test_generic_metric_quality_matches_oracle(ub, oracle, gauss10k):
-    """10k workload, 200 epochs, MetricType::Generic with the Euclidean output metric, against
-    the oracle's generic rule (mean of 3 seeds): recall within 0.01 per run; fuzzy
-    cross-entropy within 2% per run and on the mean of the GPU runs.  The reference's generic
-    loop is sequential and the GPU runs it in parallel like the Euclidean path: over 12 GPU
-    runs its cross-entropy sat 1.0% +- 0.3% below the sequential oracle's (a slightly tighter
-    fit), against 0.4% run-to-run spread for the oracle.  The result must also be the generic
-    rule's: its recall is nearer the oracle's generic recall than its Euclidean one (0.038
-    against 0.010 here), and so is its mean cross-entropy (270k against 277k)."""
+    """10k workload, 200 epochs, MetricType::Generic with the Euclidean output metric against
+    the oracle's generic rule (the reference's sequential loop): every run's recall within
+    0.01 and cross-entropy within 1% of the oracle's mean, and the runs' mean cross-entropy
+    within 0.5%.  The result must also be the generic rule's: its recall is nearer the
+    oracle's generic recall than its Euclidean one (0.038 against 0.010 here).  The generic
+    rule's layout keeps rows of up to 64 edges whole (pick_chunk_generic): split rows
+    overshoot under its strong attraction.  Over 8 GPU runs the cross-entropy sat 0.04% from
+    the oracle's and the recall 3% below it (0.0368 against 0.0380): the reference applies
+    its generic loop to one row at a time, the GPU to every row at once."""
     from umap_b200 import quality as Q
     idx, dist, init = gauss10k
     cfg = ub.UmapConfig()
     cfg.optimization.n_epochs = 200
-    ocfg = oracle.OracleConfig(n_epochs=200)
-    mo = oracle.learn_manifold(idx, dist, ocfg)
-    a, b = mo.info()["a"], mo.info()["b"]
-    head, tail, _ = oracle.Optimizer(mo, init, 200, ocfg, seed=0).edges()
-    ip, ix, dt = mo.graph()
-    ip = ip.astype(np.int64)
-    w = np.empty(len(head), np.float32)
-    for e in range(len(head)):
-        r = int(head[e])
-        w[e] = dt[ip[r] + int(np.searchsorted(ix[ip[r]:ip[r + 1]], tail[e]))]
-    rec_o, ce_o = [], []
-    for seed in (1, 2, 3):
-        emb, _, _ = oracle.fit(idx, dist, init, ocfg, seed=seed, metric_type=1)
-        rec_o.append(Q.knn_recall(emb, idx))
-        ce_o.append(Q.fuzzy_cross_entropy(emb, head, tail, w, a, b))
-    ro, co = float(np.mean(rec_o)), float(np.mean(ce_o))
+    rec_o, ce_o, (head, tail, w), (a, b) = _oracle_scores(oracle, idx, dist, init, 200, metric_type=1)
     res = []
-    for seed in (1, 2):
+    for seed in (1, 2, 3):
         opt = ub.Optimizer(ub.Umap(cfg).learn_manifold(10_000, idx, dist), init, 200, cfg, ub.MetricType.Generic)
+        assert opt.layout()["generic_rule"] and opt.tuning()[0] >= 64
         opt.set_seed(seed)
         opt.step_epochs(200, ub.GenericEuclideanMetric())
         emb = opt.embedding()
@@ -535,17 +522,17 @@ def test_generic_metric_quality_matches_oracle(ub, oracle, gauss10k):
     f = ub.Umap.with_metrics(cfg, ub.EuclideanMetric(), ub.GenericEuclideanMetric()).fit(10_000, idx, dist, init)
     emb = f.embedding()
     res.append((Q.knn_recall(emb, idx), Q.fuzzy_cross_entropy(emb, head, tail, w, a, b)))
-    emb_e, _, _ = oracle.fit(idx, dist, init, ocfg, seed=1, metric_type=0)
+    emb_e, _, _ = oracle.fit(idx, dist, init, oracle.OracleConfig(n_epochs=200), seed=1, metric_type=0)
     re = Q.knn_recall(emb_e, idx)
-    ce_e = Q.fuzzy_cross_entropy(emb_e, head, tail, w, a, b)
-    print(f"oracle generic recall {rec_o} CE {ce_o}; oracle euclidean recall {re} CE {ce_e}; gpu {res}")
+    ro, co = float(np.mean(rec_o)), float(np.mean(ce_o))
+    print(f"generic rule: oracle recall {np.round(rec_o, 5)} CE {np.round(ce_o, 0)}; "
+          f"gpu {[(round(r, 5), round(c, 0)) for r, c in res]}; oracle euclidean recall {re:.5f}")
     for r, c in res:
         assert abs(r - ro) <= 0.01, (r, ro)
+        assert abs(c - co) <= 0.01 * co, (c, co)
         assert abs(r - ro) < abs(r - re), (r, ro, re)
-        assert abs(c - co) <= 0.02 * co, (c, co)
     cm = float(np.mean([c for _, c in res]))
-    assert abs(cm - co) <= 0.02 * co, (cm, co)
-    assert abs(cm - co) < abs(cm - ce_e), (cm, co, ce_e)
+    assert abs(cm - co) <= 0.005 * co, (cm, co)
 
 
 def test_generic_optimizer_checkpoint_resumes(ub, ring):

@@ -491,11 +491,11 @@ def run_warm_start(a):
 
 
 def swiss_traffic(edges):
-    """DRAM bytes per SGD launch at `edges` kept edges, scaled from the 10M-point capture of
-    the renamed layout (a lower bound at larger sizes: the 10M embedding is partly
-    L2-resident)."""
-    t = ncu_figure("sgd_epoch_swiss_roll_10m_renamed", "traffic_bytes_per_launch")
-    e0 = ncu_figure("sgd_epoch_swiss_roll_10m_renamed", "kept_edges")
+    """DRAM bytes per SGD launch at `edges` kept edges, scaled from the 40M-point capture of
+    the renamed layout (a lower bound at larger sizes: traffic per edge still grows with the
+    embedding, 62 / 146 / 203 bytes per kept edge at 10M / 20M / 40M points)."""
+    t = ncu_figure("sgd_epoch_swiss_roll_40m_renamed", "traffic_bytes_per_launch")
+    e0 = ncu_figure("sgd_epoch_swiss_roll_40m_renamed", "kept_edges")
     return t * edges / e0 if t and e0 else None
 
 
@@ -605,9 +605,9 @@ def run_swiss_roll(a):
             "graph_and_setup_ms": ms_step - sgd_ms,
             "roofline": {"bound": "hbm", "kernel": stats["layout"]["kernel"], "achieved": achieved, "peak": hbm,
                          "unit": "GB/s", "frac": achieved / hbm, "peak_source": hbm_src, "traffic": swiss_traffic(E),
-                         "traffic_note": "DRAM bytes of one epoch-20 launch captured at 10M points, "
-                                         "scaled by kept edges (a lower bound: L2 holds more of the "
-                                         "smaller embedding)",
+                         "traffic_note": "DRAM bytes of one epoch-20 launch captured at 40M points, "
+                                         "scaled by kept edges (a lower bound: traffic per edge grows "
+                                         "with the embedding)",
                          "algorithmic_bytes_per_launch": alg / a.swiss_epochs,
                          "avg_launch_ms": sgd_ms / a.swiss_epochs},
             "device_memory_gb": {"total": total_mem / 1e9, "inputs_resident": (total_mem - free0) / 1e9,

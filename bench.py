@@ -261,6 +261,32 @@ def cpu_baseline(idx, dist, init, epochs_total, n_epochs_timed, skip=20):
             "graph_build_s": round(t_graph, 2)}
 
 
+def l2_roofline(ub, n, fired_per_epoch, negatives_per_epoch, launch_ms):
+    """The SGD epoch's L2 roofline: its random 8-byte row accesses (a tail read, a tail
+    red.add and the negatives' reads per fired edge) at the device's measured rates for that
+    pattern on a table the size of the epoch's snapshot embedding (umap_random_rows_probe_device,
+    CUDA events), against the epoch's measured duration."""
+    import ctypes as C
+    import torch
+    L = ub.lib()
+    table = torch.zeros((n, 2), dtype=torch.float32, device="cuda")
+    out = torch.empty(148 * 8 * 256, dtype=torch.float32, device="cuda")
+    rates = {}
+    for mode, name, count in ((0, "read", 400_000_000), (1, "red_add", 100_000_000)):
+        ms, done = C.c_float(), C.c_uint64()
+        rc = L.umap_random_rows_probe_device(C.c_void_p(table.data_ptr()), n, count, mode, C.c_void_p(out.data_ptr()),
+                                             C.byref(ms), C.byref(done))
+        assert rc == 0, L.umap_last_error()
+        rates[name] = done.value / (ms.value / 1e3)
+    reads = fired_per_epoch + negatives_per_epoch
+    need_ms = (reads / rates["read"] + fired_per_epoch / rates["red_add"]) * 1e3
+    return {"bound": "l2 random 8-byte rows", "frac": need_ms / launch_ms,
+            "peak_reads_per_s": rates["read"], "peak_red_adds_per_s": rates["red_add"],
+            "reads_per_launch": reads, "red_adds_per_launch": fired_per_epoch,
+            "ms_at_peak_rates": need_ms, "avg_launch_ms": launch_ms,
+            "table": f"{n} x 2 f32 (the snapshot embedding's size)"}
+
+
 def quality_vs_oracle(ub, fitted, idx, dist, init, epochs):
     """After the timed region: the oracle's complete fit of the same inputs (all host cores,
     one seed) scored beside the GPU fit just timed.  15-NN recall on a fixed seeded sample of
@@ -895,6 +921,8 @@ def main():
         "gpu_launches": launches,
         "clocks": clocks,
     }
+    if world == 1:
+        line["roofline"]["l2_random_rows"] = l2_roofline(ub, n, F_tot / a.epochs, N_tot / a.epochs, sgd_kernel_ms)
     if rank == 0 and not a.no_cpu:
         line["cpu_baseline"] = cpu_baseline(idx, dist, init, a.epochs, a.cpu_epochs, a.cpu_skip)
         if world == 1 and not a.no_quality:

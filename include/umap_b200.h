@@ -53,7 +53,7 @@ enum umap_metric_type {
 
 /* Output metrics with a device implementation, for the generic rule (the reference's
  * `output_metric: &dyn Metric`).  The reference ships one Metric, EuclideanMetric
- * (distances.rs:197-236): distance sqrt(sum (x-y)^2), gradient (x-y) / (distance + 1e-6). */
+ * (distances.rs:10-50): distance sqrt(sum (x-y)^2), gradient (x-y) / (distance + 1e-6). */
 enum umap_output_metric {
   UMAP_OUTPUT_METRIC_EUCLIDEAN = 0
 };
@@ -328,6 +328,15 @@ int umap_sgd_negative_draws_device(uint64_t seed, uint64_t first_entry, uint64_t
  * optimizer accepts); 0 where the edge does not fire then. */
 int umap_sgd_negatives_per_firing_device(const uint32_t* dev_q, const uint32_t* dev_epoch, uint64_t count,
                                          uint32_t negative_sample_rate, uint32_t* dev_out);
+
+/* Measurement hook (no counterpart in the reference): the device's rate for the SGD epoch's
+ * random access pattern, the denominator of its L2 roofline.  One timed launch (after one
+ * untimed one that brings the table into L2) of about `accesses` random 8-byte row reads
+ * (mode 0) or red.add row moves (mode 1) on dev_table [n_rows][2] f32; *ms = its CUDA-event
+ * time, *accesses_done = the accesses it made.  Mode 0 writes 303,104 floats to dev_out;
+ * mode 1 changes the table. */
+int umap_random_rows_probe_device(float* dev_table, uint64_t n_rows, uint64_t accesses, int mode, float* dev_out,
+                                  float* ms, uint64_t* accesses_done);
 
 /* Allocation-free variant of umap_radix_sort_pairs_device (no counterpart in the
  * reference; the reference has no device code).  For callers that cannot allocate device

@@ -128,6 +128,7 @@ extern "C" {
     pub fn umap_radix_sort_pairs_device(dev_keys_in: *const u32, dev_values_in: *const u32, dev_keys_out: *mut u32, dev_values_out: *mut u32, n: u64, end_bit: c_int) -> c_int;
     pub fn umap_sgd_negative_draws_device(seed: u64, first_entry: u64, n_entries: u64, epoch: u32, per_entry: u32, lo: u32, range: u32, dev_out: *mut u32) -> c_int;
     pub fn umap_sgd_negatives_per_firing_device(dev_q: *const u32, dev_epoch: *const u32, count: u64, negative_sample_rate: u32, dev_out: *mut u32) -> c_int;
+    pub fn umap_random_rows_probe_device(dev_table: *mut f32, n_rows: u64, accesses: u64, mode: c_int, dev_out: *mut f32, ms: *mut f32, accesses_done: *mut u64) -> c_int;
     pub fn umap_radix_sort_pairs_device_noalloc(dev_keys_in: *const u32, dev_values_in: *const u32, dev_keys_out: *mut u32, dev_values_out: *mut u32, n: u64, end_bit: c_int, stream: *mut c_void) -> c_int;
     pub fn umap_radix_sort_noalloc_max_pairs(out: *mut u64) -> c_int;
     pub fn umap_mlp_param_count(in_dim: u64, out_dim: u64, out: *mut u64) -> c_int;

@@ -712,7 +712,7 @@ void orc_optimizer_set_embedding(OrcOptimizer* o, const float* in) {
   memcpy(o->embedding.data(), in, o->embedding.size() * 4);
 }
 
-// distances.rs:208-223 EuclideanMetric::distance: (sqrt(sum diff^2), (x - y) / (dist + 1e-6)).
+// distances.rs:22-37 EuclideanMetric::distance: (sqrt(sum diff^2), (x - y) / (dist + 1e-6)).
 static float euclidean_distance(const float* x, const float* y, uint64_t dim, float* grad) {
   float sum_sq = 0.0f;
   for (uint64_t i = 0; i < dim; ++i) {

@@ -192,7 +192,7 @@ def test_rust_ffi_is_generated_from_the_header():
 
 def test_output_metric_checks_without_gpu(ub):
     """metric.rs / distances.rs on the host side: EuclideanMetric's distance and gradient
-    (distances.rs:208-223, f32), the metric types and device ids that route Optimizer and
+    (distances.rs:22-37, f32), the metric types and device ids that route Optimizer and
     Umap.fit, and the refusal of a metric with no device form before any GPU work."""
     import numpy as np
     x = np.float32([1.5, -2.0, 0.25])

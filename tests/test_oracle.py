@@ -270,7 +270,7 @@ def np_pairs_epochs(x0, a, b, gamma, lr, total, n_ep, generic):
     negative_sample_rate = 0, in numpy float32: live buffer `x`, snapshot `c` cloned once
     (optimizer.rs:314), every edge (j -> j^1) fires at every epoch >= 1.  Euclidean rule:
     optimize_layout_euclidean.rs:284-306; generic rule with EuclideanMetric:
-    optimize_layout_generic.rs:62-86 + distances.rs:208-223."""
+    optimize_layout_generic.rs:62-86 + distances.rs:22-37."""
     f = np.float32
     x = x0.astype(np.float32).copy()
     c = x.copy()

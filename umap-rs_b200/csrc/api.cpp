@@ -2351,6 +2351,18 @@ int umap_sgd_negatives_per_firing_device(const uint32_t* dev_q, const uint32_t* 
   API_END
 }
 
+int umap_random_rows_probe_device(float* dev_table, uint64_t n_rows, uint64_t accesses, int mode, float* dev_out,
+                                  float* ms, uint64_t* accesses_done) {
+  API_BEGIN
+  need(dev_table, "table"); need(ms, "ms"); need(accesses_done, "accesses_done");
+  if (mode != 0 && mode != 1) throw Error(INVALID_ARGUMENT, "mode must be 0 (reads) or 1 (red.add)");
+  if (mode == 0) need(dev_out, "out");
+  Stream st;
+  wait_for_inputs();
+  *ms = random_rows_probe(dev_table, n_rows, accesses, mode, dev_out, accesses_done, st.s);
+  API_END
+}
+
 int umap_radix_sort_pairs_device_noalloc(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
                                          uint32_t* vals_out, uint64_t n, int end_bit, void* stream) {
   API_BEGIN

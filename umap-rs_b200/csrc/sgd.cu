@@ -205,7 +205,7 @@ __device__ __forceinline__ void sub_row(float* p, const float (&g)[DIM]) {
 }
 
 // Force law of the generic-metric path (layout/optimize_layout_generic.rs:65-119) with the
-// built-in output metric EuclideanMetric (distances.rs:208-223): distance d = sqrt(sum diff^2),
+// built-in output metric EuclideanMetric (distances.rs:22-37): distance d = sqrt(sum diff^2),
 // gradient diff / (d + 1e-6), w = 1 / (1 + a d^(2b)).  Returns the coefficient c that
 // multiplies the gradient: 2b (w - 1) / (d + 1e-6) for an attraction, 2 gamma b w / (d + 1e-6)
 // for a repulsion (`scale` = 2b or 2 gamma b, `bias` = -1 or 0); *den receives d + 1e-6.

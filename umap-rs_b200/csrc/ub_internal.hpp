@@ -264,6 +264,12 @@ void pad_gather_rows(const float* x, uint64_t d, uint64_t dp, const uint32_t* ro
 void finite_rows(const float* y, uint64_t n, uint32_t dim, uint32_t* keep, cudaStream_t s);
 void compact_rows(const float* src, uint64_t n, uint64_t width, const uint32_t* keep, const uint64_t* pos,
                   float* dst, cudaStream_t s);
+// Timed rate probe of random 8-byte row reads (mode 0) or red.adds (mode 1) on table [n_rows][2]
+// (probe.cu): returns the CUDA-event milliseconds of one launch; *done = accesses made; out
+// receives 148 * 8 * 256 per-thread sums in mode 0.
+constexpr uint64_t PROBE_THREADS = 148ull * 8 * 256;
+float random_rows_probe(float* table, uint64_t n_rows, uint64_t accesses, int mode, float* out, uint64_t* done,
+                        cudaStream_t s);
 // Locality order of a graph's vertices (order.cu): order[u] = old id of new vertex u,
 // rank = its inverse.
 void locality_order(const uint64_t* kptr, const uint32_t* ktail, uint64_t n, uint32_t* order, uint32_t* rank,

@@ -156,7 +156,7 @@ class Metric:
 
 
 class EuclideanMetric(Metric):
-    """distances.rs:197-236."""
+    """distances.rs:10-50."""
 
     def metric_type(self) -> MetricType:
         return MetricType.Euclidean
@@ -165,7 +165,7 @@ class EuclideanMetric(Metric):
         return OUTPUT_METRIC_EUCLIDEAN
 
     def distance(self, x, y):
-        """(sqrt(sum (x - y)^2), (x - y) / (distance + 1e-6)) in f32 (distances.rs:208-223)."""
+        """(sqrt(sum (x - y)^2), (x - y) / (distance + 1e-6)) in f32 (distances.rs:22-37)."""
         x = np.asarray(x, np.float32)
         y = np.asarray(y, np.float32)
         s = np.float32(0)

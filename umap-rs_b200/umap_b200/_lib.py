@@ -108,6 +108,7 @@ SIGNATURES = {
     "umap_radix_sort_pairs_device_noalloc": [P, P, P, P, u64, i32, P],
     "umap_sgd_negative_draws_device": [u64, u64, u64, u32, u32, u32, u32, P],
     "umap_optimizer_layout_flags": [P, C.POINTER(u32)],
+    "umap_random_rows_probe_device": [P, u64, u64, i32, P, C.POINTER(f32), C.POINTER(u64)],
     "umap_sgd_negatives_per_firing_device": [P, P, u64, u32, P],
     "umap_warm_start_params_default": [C.POINTER(WarmStartParamsC)],
     "umap_warm_start_fit_device": [C.POINTER(UmapConfigC), C.POINTER(WarmStartParamsC), P, u64, u64, P, P, u64,

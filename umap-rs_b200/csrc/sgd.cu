@@ -687,6 +687,51 @@ __global__ void minmax_dim_kernel(const float* __restrict__ emb, uint64_t n, uin
   }
 }
 
+// A plain fit's column min / max in two stages: block b of dimension d reduces rows
+// b, b + G, ... into part[d][b]; then minmax_finish_kernel folds the G partials.  Min and max
+// ignore NaN and are exact in any order, so the result equals one block's.
+__global__ void minmax_part_kernel(const float* __restrict__ emb, uint64_t n, uint32_t dim,
+                                   float* __restrict__ pmin, float* __restrict__ pmax) {
+  const uint32_t d = blockIdx.y, G = gridDim.x;
+  float mn = INFINITY, mx = -INFINITY;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)G * blockDim.x) {
+    const float v = emb[i * dim + d];
+    mn = fminf(mn, v);
+    mx = fmaxf(mx, v);
+  }
+  __shared__ float s_mn[32], s_mx[32];
+  for (int o = 16; o > 0; o >>= 1) {
+    mn = fminf(mn, __shfl_xor_sync(0xFFFFFFFFu, mn, o));
+    mx = fmaxf(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, o));
+  }
+  if ((threadIdx.x & 31) == 0) { s_mn[threadIdx.x >> 5] = mn; s_mx[threadIdx.x >> 5] = mx; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (uint32_t w = 1; w < blockDim.x / 32; ++w) { mn = fminf(mn, s_mn[w]); mx = fmaxf(mx, s_mx[w]); }
+    pmin[d * G + blockIdx.x] = mn;
+    pmax[d * G + blockIdx.x] = mx;
+  }
+}
+
+__global__ void minmax_finish_kernel(const float* __restrict__ pmin, const float* __restrict__ pmax, uint32_t G,
+                                     float* __restrict__ mins, float* __restrict__ scales) {
+  const uint32_t d = blockIdx.x;
+  float mn = INFINITY, mx = -INFINITY;
+  for (uint32_t g = threadIdx.x; g < G; g += blockDim.x) {
+    mn = fminf(mn, pmin[d * G + g]);
+    mx = fmaxf(mx, pmax[d * G + g]);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    mn = fminf(mn, __shfl_xor_sync(0xFFFFFFFFu, mn, o));
+    mx = fmaxf(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, o));
+  }
+  if (threadIdx.x == 0) {
+    const float range = __fsub_rn(mx, mn);
+    mins[d] = mn;
+    scales[d] = range > 0.0f ? __fdiv_rn(10.0f, range) : 0.0f;
+  }
+}
+
 __global__ void normalize_kernel(float* __restrict__ emb, uint64_t total, uint32_t dim,
                                  const float* __restrict__ mins, const float* __restrict__ scales,
                                  const uint32_t* __restrict__ row_seg) {
@@ -968,8 +1013,17 @@ void normalize_init(float* emb, uint64_t n, uint32_t dim, cudaStream_t s, const 
   if (n == 0 || dim == 0) return;
   const uint32_t n_seg = seg ? seg->n_seg : 1u;
   DevBuf<float> mins((uint64_t)dim * n_seg, s), scales((uint64_t)dim * n_seg, s);
-  minmax_dim_kernel<<<dim3(dim, n_seg), 1024, 0, s>>>(emb, n, dim, seg ? seg->seg_off : nullptr, mins.p, scales.p);
-  UB_LAUNCH_CHECK();
+  if (seg || dim > 65535) {  // batched instances: one block per (dimension, instance)
+    minmax_dim_kernel<<<dim3(dim, n_seg), 1024, 0, s>>>(emb, n, dim, seg ? seg->seg_off : nullptr, mins.p, scales.p);
+    UB_LAUNCH_CHECK();
+  } else {
+    const uint32_t G = (uint32_t)std::min<uint64_t>(256, (n + 4095) / 4096);
+    DevBuf<float> pmin((uint64_t)dim * G, s), pmax((uint64_t)dim * G, s);
+    minmax_part_kernel<<<dim3(G, dim), 256, 0, s>>>(emb, n, dim, pmin.p, pmax.p);
+    UB_LAUNCH_CHECK();
+    minmax_finish_kernel<<<dim, 32, 0, s>>>(pmin.p, pmax.p, G, mins.p, scales.p);
+    UB_LAUNCH_CHECK();
+  }
   normalize_kernel<<<grid_for(n * dim, 256), 256, 0, s>>>(emb, n * dim, dim, mins.p, scales.p,
                                                           seg ? seg->row_seg : nullptr);
   UB_LAUNCH_CHECK();

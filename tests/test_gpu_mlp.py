@@ -136,6 +136,25 @@ def test_train_rejects_bad_batch(ub, torch):
         net.train(x, t, epochs=1, batch=512)
 
 
+def test_warm_start_entry_rejects_bad_arguments(ub, torch):
+    """umap_warm_start_fit_device refuses, before any GPU work, a subsample row outside the
+    data and a subsample too small for one 128-row training batch."""
+    from umap_b200 import workloads as W
+    n = 3000
+    X = np.random.default_rng(1).normal(size=(n, 16)).astype(np.float32)
+    idx, dist = W.knn_exact_numpy(X, 15)
+    x = torch.from_numpy(X).cuda()
+    sub = np.arange(0, n, 3)
+    sidx, sdist = W.knn_exact_numpy(X[sub], 15)
+    bad = sub.copy()
+    bad[7] = n + 5
+    with pytest.raises(ub.UmapError, match=r"sub_rows\[7\] = 3005 is not a row of data \(3000 rows\)"):
+        ub.warm_start_fit(ub.UmapConfig(), x, idx, dist, bad, sidx, sdist, sub_epochs=5, epochs=5, mlp_epochs=1)
+    with pytest.raises(ub.UmapError, match="128"):
+        ub.warm_start_fit(ub.UmapConfig(), x, idx, dist, sub[:100], sidx[:100], sdist[:100], sub_epochs=5,
+                          epochs=5, mlp_epochs=1)
+
+
 def _sheet_64d(n, seed):
     """A noisy swiss roll (a 2-D sheet) placed in 64-D by a random isometry: its kNN follow
     the sheet, and its embedding is a smooth function of the input."""

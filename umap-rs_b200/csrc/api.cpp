@@ -1276,6 +1276,14 @@ std::unique_ptr<umap_fitted> warm_start_impl(const umap_config& c, const umap_wa
     throw Error(INVALID_ARGUMENT, "sub_epochs, epochs and mlp_epochs must be positive");
   std::string err = validate_parameters(c, n, n, k);
   if (!err.empty()) throw Error(INVALID_ARGUMENT, err);
+  {  // the subsample's rows index the caller's data: every one must be a row of it
+    std::vector<uint32_t> rows(n_sub);
+    UB_CUDA(cudaMemcpy(rows.data(), sub_rows, n_sub * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    for (uint64_t i = 0; i < n_sub; ++i)
+      if (rows[i] >= n)
+        throw Error(INVALID_ARGUMENT, "sub_rows[" + std::to_string(i) + "] = " + std::to_string(rows[i]) +
+                                          " is not a row of data (" + std::to_string(n) + " rows)");
+  }
   int dev = 0;
   UB_CUDA(cudaGetDevice(&dev));
   float ph[UMAP_WARM_START_PHASES] = {};

@@ -176,15 +176,14 @@ def warm_start_fit(config: UmapConfig, data, knn_indices, knn_dists, sub_index, 
     n, d = data.shape
     dev = data.device
     ki, pki = _dev_u32(knn_indices, dev)
-    kd = _cuda_f32(knn_dists, "knn_dists")
+    kd = _dev_f32(knn_dists, dev)
     rows, prows = _dev_u32(sub_index, dev)
     si, psi = _dev_u32(sub_knn_indices, dev)
-    sd = _cuda_f32(sub_knn_dists, "sub_knn_dists")
+    sd = _dev_f32(sub_knn_dists, dev)
     n_sub = int(rows.shape[0])
     sinit = None
     if sub_init is not None:
-        sinit = _cuda_f32(sub_init if hasattr(sub_init, "is_cuda") else torch.from_numpy(np.asarray(sub_init)).to(dev),
-                          "sub_init")
+        sinit = _dev_f32(sub_init, dev)
     wp = _lib.WarmStartParamsC()
     L = _lib.load()
     _check(L.umap_warm_start_params_default(C.byref(wp)))
@@ -209,6 +208,13 @@ def warm_start_fit(config: UmapConfig, data, knn_indices, knn_dists, sub_index, 
         info["mlp_losses"] = losses[:mlp_epochs].tolist()
         info["n_sub"] = n_sub
     return fitted
+
+
+def _dev_f32(x, dev):
+    """A contiguous CUDA f32 copy (or view) of a CUDA tensor or a host array."""
+    import torch
+    t = x if hasattr(x, "is_cuda") else torch.from_numpy(np.ascontiguousarray(np.asarray(x, np.float32)))
+    return t.to(dev).float().contiguous()
 
 
 def _dev_u32(x, dev):

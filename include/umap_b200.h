@@ -261,13 +261,15 @@ int umap_batch_fit_device(const umap_config* cfg, uint64_t n_instances, const ui
 int umap_optimizer_tuning(const umap_optimizer* opt, uint32_t* chunk, uint32_t* block_threads);
 /* Extension: how the SGD layout is laid out (bit flags): UMAP_LAYOUT_LANE_MAJOR (a lane's
  * edges contiguous; else interleaved by lane), UMAP_LAYOUT_EIGHT_NEGATIVES (the epoch kernel's
- * 8-row-loads-in-flight register budget; else 4), UMAP_LAYOUT_RENAMED (vertices renamed into
- * a locality order; DRAM-bound plain fits), UMAP_LAYOUT_GENERIC_RULE (the optimizer's
- * MetricType is Generic). */
+ * 8-row-loads-in-flight register budget), UMAP_LAYOUT_TWELVE_NEGATIVES (the 12-row budget of
+ * renamed layouts; neither flag: 4), UMAP_LAYOUT_RENAMED (vertices renamed into a locality
+ * order; DRAM-bound plain fits), UMAP_LAYOUT_GENERIC_RULE (the optimizer's MetricType is
+ * Generic). */
 #define UMAP_LAYOUT_LANE_MAJOR 1u
 #define UMAP_LAYOUT_EIGHT_NEGATIVES 2u
 #define UMAP_LAYOUT_RENAMED 4u
 #define UMAP_LAYOUT_GENERIC_RULE 8u
+#define UMAP_LAYOUT_TWELVE_NEGATIVES 16u
 int umap_optimizer_layout_flags(const umap_optimizer* opt, uint32_t* flags);
 
 /* ---- serde checkpoints (optimizer.rs:27, manifold.rs:14, embedding.rs:438) ---------

@@ -2224,7 +2224,8 @@ int umap_optimizer_layout_flags(const umap_optimizer* opt, uint32_t* flags) {
   API_BEGIN
   need(opt, "optimizer"); need(flags, "flags");
   *flags = (opt->layout.lane_major ? UMAP_LAYOUT_LANE_MAJOR : 0u) |
-           (opt->layout.short_epoch ? UMAP_LAYOUT_EIGHT_NEGATIVES : 0u) |
+           (opt->layout.short_epoch && !opt->layout.dram_epoch ? UMAP_LAYOUT_EIGHT_NEGATIVES : 0u) |
+           (opt->layout.dram_epoch ? UMAP_LAYOUT_TWELVE_NEGATIVES : 0u) |
            (opt->layout.order.p ? UMAP_LAYOUT_RENAMED : 0u) |
            (opt->metric_type == UMAP_METRIC_GENERIC ? UMAP_LAYOUT_GENERIC_RULE : 0u);
   API_END

@@ -43,6 +43,12 @@ constexpr uint32_t PAD_ROW = 0xFFFFFFFFu;
 // fetched together (one round trip for a firing's usual 4-6 negatives) and 4 blocks per SM.
 constexpr int NB_WIDE = 4, MINB_WIDE = 5;
 constexpr int NB_SHORT = 8, MINB_SHORT = 4;
+// Renamed DRAM-bound layouts: 12 negative rows fetched together, 3 blocks per SM.  Their random
+// row loads go to DRAM and their warps are limited by registers either way, so more loads in
+// flight per lane beat more warps (30 epochs of a 20M-point roll: 8 / 4: 310.8 ms, 10 / 3:
+// 295.1, 12 / 3: 295.2, 12 / 2: 313.4, 16 / 2: 316.0, 24 / 2: 317.7; 40M points, 24 epochs:
+// 8 / 4: 590.4, 12 / 3: 562.6, 16 / 2: 564.9).
+constexpr int NB_DRAM = 12, MINB_DRAM = 3;
 
 // ------------------------------------------------------------------------------ negatives' RNG
 // Counter-based: the firing of entry `idx` at `epoch` draws its negatives in pairs; pair t is
@@ -883,11 +889,17 @@ bool pick_short_epoch(uint64_t n_slices, bool renamed) {
     if (e[0] == '0') return false;
     if (e[0] == '1') return true;
   }
-  if (renamed) return true;
+  if (renamed) return true;  // the layout takes the DRAM budget (pick_dram_epoch) unless forced
   int dev = 0, sms = 0;
   UB_CUDA(cudaGetDevice(&dev));
   UB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   return n_slices <= 2ull * (uint64_t)std::max(sms, 1) * MINB_WIDE * 8;
+}
+
+// Renamed (DRAM-bound) layouts take the 12-negatives budget unless UMAP_B200_SGD_SHORT forces one
+// of the other two.
+bool pick_dram_epoch(bool renamed) {
+  return renamed && getenv("UMAP_B200_SGD_SHORT") == nullptr;
 }
 
 // Entry order of the layout.  Lane major (a lane's window is one 32-byte sector) wins while
@@ -997,6 +1009,7 @@ void build_sgd_layout(const uint64_t* kept_ptr, const uint32_t* ktail, const dou
   L.split_tasks = 0;
   for (uint32_t v : h) L.split_tasks += __builtin_popcount(v);
   L.short_epoch = pick_short_epoch(L.n_slices, L.order.p != nullptr);
+  L.dram_epoch = pick_dram_epoch(L.order.p != nullptr);
 }
 
 void export_edges(const uint64_t* indptr, const uint32_t* indices, const float* data, uint64_t n,
@@ -1055,6 +1068,12 @@ void sgd_epoch(const SgdLayout& L, float* live, float* snap, const SgdParams& p,
   // parity with the reference's sequential loop was established with it).
   if (p.generic_metric) {
     UB_SGD_DISPATCH(true, false)
+  } else if (L.dram_epoch && (p.dim == 1 || p.dim == 2)) {
+#define UB_SGD_DRAM(D)                                                                                       \
+  if (L.lane_major) sgd_epoch_kernel2<D, false, NB_DRAM, MINB_DRAM, true><<<grid, bt, 0, s>>>(UB_SGD_ARGS); \
+  else sgd_epoch_kernel2<D, false, NB_DRAM, MINB_DRAM, false><<<grid, bt, 0, s>>>(UB_SGD_ARGS)
+    if (p.dim == 1) { UB_SGD_DRAM(1); } else { UB_SGD_DRAM(2); }
+#undef UB_SGD_DRAM
   } else {
     UB_SGD_DISPATCH(false, L.short_epoch)
   }

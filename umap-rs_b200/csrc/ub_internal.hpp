@@ -183,6 +183,7 @@ struct SgdLayout {
   uint32_t max_degree = 0, chunk = 0;
   uint32_t block_threads = 256;  // threads per block of the epoch kernel (multiple of 32)
   bool short_epoch = false;      // epoch kernel budget for graphs of at most ~2 waves of warps
+  bool dram_epoch = false;       // 12-negatives budget of renamed DRAM-bound layouts
   bool lane_major = true;        // entry order: lane major (true) or interleaved by lane
   uint64_t split_tasks = 0;
   DevBuf<uint64_t> slice_base;   // [n_slices + 1]

@@ -656,15 +656,16 @@ class Optimizer(_Handle):
         budget, vertices renamed into a locality order; and the epoch kernel it selects."""
         f = C.c_uint32()
         _check(_lib.load().umap_optimizer_layout_flags(self._get(), C.byref(f)))
-        lm, eight, renamed, generic = (bool(f.value & b) for b in (1, 2, 4, 8))
+        lm, eight, renamed, generic, twelve = (bool(f.value & b) for b in (1, 2, 4, 8, 16))
         _, dim = self.dims()
         eight = eight and dim <= 2 and not generic  # the generic rule keeps the 4-negatives budget
-        nb, minb = (8, 4) if eight else (4, 5)
+        twelve = twelve and dim <= 2 and not generic
+        nb, minb = (12, 3) if twelve else (8, 4) if eight else (4, 5)
         gen = "true" if generic else "false"
         kernel = (f"sgd_epoch_kernel2<{dim}, {gen}, {nb}, {minb}, {'true' if lm else 'false'}>" if dim <= 4
                   else f"sgd_epoch_anydim<{gen}>")
-        return {"lane_major": lm, "eight_negatives": eight, "renamed": renamed, "generic_rule": generic,
-                "kernel": kernel}
+        return {"lane_major": lm, "eight_negatives": eight, "twelve_negatives": twelve, "renamed": renamed,
+                "generic_rule": generic, "kernel": kernel}
 
     def tuning(self):
         """(task length, threads per block) of the SGD kernel in use."""

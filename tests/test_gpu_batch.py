@@ -98,10 +98,11 @@ def test_batch_instances_match_the_oracle(ub, oracle):
     (embedding.rs:274-337 run once per dataset): rho bit-exact and sigma within 1e-5; graph
     row pointers and columns bit-exact, weights within 1e-5; pruned head/tail bit-exact,
     epochs_per_sample within 1e-5; normalised init bit-exact; and, for the embedding, fuzzy
-    cross-entropy of the batched fit within 1% of the oracle's (2 GPU seeds against 3 oracle
-    seeds, means compared)."""
+    cross-entropy of the batched fit within 1% of the oracle's (3 GPU seeds against 5 oracle
+    seeds, means compared) on the instances of at least 1,500 points: on a 700-point instance
+    the oracle's own cross-entropy spans 1.6% over 3 seeds."""
     from umap_b200 import quality as Q
-    sizes = [700, 1800, 64, 2600]
+    sizes = [700, 1800, 64, 2600, 2200]
     off, idxs, dists, inits = make_batch(sizes, seed0=500)
     idxs[1] = idxs[1].copy()
     idxs[1][::9, -2] = 0xFFFFFFFF
@@ -118,7 +119,7 @@ def test_batch_instances_match_the_oracle(ub, oracle):
     bh, bt, be, _, _, _ = bopt.export_edges()
     bemb0 = bopt.embedding()
     fits = []
-    for seed in (11, 12):
+    for seed in (11, 12, 13):
         o = ub.Optimizer.batch(cfg, off, I, D, X0, total)
         o.set_seed(seed)
         o.step_epochs(total)
@@ -141,12 +142,12 @@ def test_batch_instances_match_the_oracle(ub, oracle):
         assert np.array_equal(bh[sel], h.astype(np.int64) + lo) and np.array_equal(bt[sel], t.astype(np.int64) + lo)
         assert np.allclose(be[sel], e, rtol=1e-5, atol=0), i
         assert np.array_equal(bemb0[lo:hi].view(np.uint32), oo.embedding().view(np.uint32)), i
-        if n < 500:
+        if n < 1500:
             continue
         a, b = mo.info()["a"], mo.info()["b"]
         w = _oracle_weights(mo, h, t)
         ce_o = [Q.fuzzy_cross_entropy(oracle.fit(idxs[i], dists[i], inits[i], ocfg, seed=s)[0], h, t, w, a, b)
-                for s in (1, 2, 3)]
+                for s in (1, 2, 3, 4, 5)]
         ce_g = [Q.fuzzy_cross_entropy(f[lo:hi], h, t, w, a, b) for f in fits]
         print(i, n, "oracle", ce_o, "batch", ce_g)
         assert abs(np.mean(ce_g) - np.mean(ce_o)) <= 0.01 * np.mean(ce_o), (i, ce_g, ce_o)

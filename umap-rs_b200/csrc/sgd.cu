@@ -47,7 +47,8 @@ constexpr int NB_SHORT = 8, MINB_SHORT = 4;
 // row loads go to DRAM and their warps are limited by registers either way, so more loads in
 // flight per lane beat more warps (30 epochs of a 20M-point roll: 8 / 4: 310.8 ms, 10 / 3:
 // 295.1, 12 / 3: 295.2, 12 / 2: 313.4, 16 / 2: 316.0, 24 / 2: 317.7; 40M points, 24 epochs:
-// 8 / 4: 590.4, 12 / 3: 562.6, 16 / 2: 564.9).
+// 8 / 4: 590.4, 12 / 3: 562.6, 16 / 2: 564.9).  Small latency-bound graphs keep 8 / 4: with
+// 12 / 3 the warm start's 100k-point subsample fit took 38.4-38.9 ms against 30.5-31.6 ms.
 constexpr int NB_DRAM = 12, MINB_DRAM = 3;
 
 // ------------------------------------------------------------------------------ negatives' RNG

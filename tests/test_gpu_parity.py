@@ -634,3 +634,49 @@ def test_relabelled_layout_is_the_same_fit(ub, oracle, monkeypatch):
     print(f"relabelled: recall {r:.4f} CE {c:.6g}; oracle recall {rec_o} CE {ce_o}")
     assert abs(r - np.mean(rec_o)) <= 0.01
     assert abs(c - np.mean(ce_o)) <= 0.01 * np.mean(ce_o)
+
+
+@pytest.mark.parametrize("dim,generic", [(1, False), (3, False), (5, False), (2, True)])
+def test_relabelled_layout_other_kernels(ub, monkeypatch, dim, generic):
+    """The renamed layout through the epoch kernels other than the 2-D Euclidean one (1-D and
+    3-D instantiations, the any-dimension kernel): normalised init, exported edges and
+    schedule totals equal the plain layout's, the embedding comes back finite in the caller's
+    order, and its fuzzy cross-entropy is within 2% of a plain-layout fit's.  The generic
+    rule keeps the caller's order even when renaming is forced."""
+    from umap_b200 import quality as Q
+    from umap_b200 import workloads as W
+    X, _ = W.swiss_roll(6000, seed=9)
+    idx, dist = W.knn_exact_numpy(X, 15)
+    init = W.uniform_init(6000, dim=dim, seed=4)
+    cfg = ub.UmapConfig()
+    cfg.n_components = dim
+    cfg.optimization.n_epochs = 60
+    mt = ub.MetricType.Generic if generic else ub.MetricType.Euclidean
+    opts = {}
+    for flag in ("1", "0"):
+        monkeypatch.setenv("UMAP_B200_RELABEL", flag)
+        opts[flag] = ub.Optimizer(ub.Umap(cfg).learn_manifold(6000, idx, dist), init, 60, cfg, mt)
+    monkeypatch.delenv("UMAP_B200_RELABEL")
+    r, p = opts["1"], opts["0"]
+    assert r.layout()["renamed"] == (not generic) and not p.layout()["renamed"]
+    assert np.array_equal(r.embedding().view(np.uint32), p.embedding().view(np.uint32))
+    for a_, b_ in zip(r.export_edges(), p.export_edges()):
+        assert np.array_equal(a_, b_)
+    assert r.schedule_totals(0, 60) == p.schedule_totals(0, 60)
+    head, tail, _, _, _, _ = p.export_edges()
+    G = p.manifold().graph()
+    ip = G.indptr.astype(np.int64)
+    w = np.array([G.data[ip[x] + np.searchsorted(G.indices[ip[x]:ip[x + 1]], y)] for x, y in zip(head, tail)])
+    a, b = p.manifold().curve_params()
+    ce = {}
+    for flag, o in opts.items():
+        o.set_seed(5)
+        if generic:
+            o.step_epochs(60, ub.GenericEuclideanMetric())
+        else:
+            o.step_epochs(60)
+        e = o.embedding()
+        assert e.shape == (6000, dim) and np.isfinite(e).all()
+        ce[flag] = Q.fuzzy_cross_entropy(e, head, tail, w, a, b)
+    print(f"dim {dim} generic {generic}: CE renamed {ce['1']:.6g} plain {ce['0']:.6g}")
+    assert abs(ce["1"] - ce["0"]) <= 0.02 * ce["0"]

@@ -506,8 +506,9 @@ std::unique_ptr<umap_optimizer> optimizer_prepare_impl(std::unique_ptr<umap_mani
     KeptEdges K;
     compute_kept_edges(*o, K, true, true);
     log.mark("optimizer edge filtering + epochs_per_sample complete");
-    build_sgd_layout(K.ptr.p, K.tail.p, K.eps.p, n,
-                     o->metric_type == UMAP_METRIC_GENERIC ? pick_chunk_generic(K.E) : 0, o->layout, s);
+    const bool generic = o->metric_type == UMAP_METRIC_GENERIC;
+    build_sgd_layout(K.ptr.p, K.tail.p, K.eps.p, n, generic ? pick_chunk_generic(K.E) : 0, o->layout, s, nullptr,
+                     !generic);
     log.mark("optimizer task layout complete");
   }
   if (log.on)
@@ -1072,8 +1073,8 @@ void finish_loaded_optimizer(umap_optimizer& o, const DevBuf<uint32_t>& head, co
   }
   DevBuf<uint64_t> ptr(n + 1, s);
   segment_starts(head.p, E, n, ptr.p, s);
-  build_sgd_layout(ptr.p, tail.p, eps.p, n, o.metric_type == UMAP_METRIC_GENERIC ? pick_chunk_generic(E) : 0,
-                   o.layout, s);
+  const bool generic = o.metric_type == UMAP_METRIC_GENERIC;
+  build_sgd_layout(ptr.p, tail.p, eps.p, n, generic ? pick_chunk_generic(E) : 0, o.layout, s, nullptr, !generic);
   set_l2_window(o, true);
   UB_CUDA(cudaStreamSynchronize(s));
 }

@@ -246,9 +246,11 @@ void export_state(const double* eps, uint64_t E, uint64_t neg_rate, uint64_t cur
 // the one for the generic-metric rule, whose rows must stay whole tasks (see sgd.cu).
 uint32_t pick_chunk(uint64_t n_edges);
 uint32_t pick_chunk_generic(uint64_t n_edges);
+// `rename`: a plain fit's layout may rename its vertices into a locality order (DRAM-bound
+// sizes); the generic-metric rule passes false.
 void build_sgd_layout(const uint64_t* kept_ptr, const uint32_t* tail, const double* eps,
                       uint64_t n, uint32_t chunk, SgdLayout& L, cudaStream_t s,
-                      const Segments* seg = nullptr);
+                      const Segments* seg = nullptr, bool rename = true);
 void kept_degree(const uint64_t* indptr, const float* data, uint64_t n, float thr,
                  uint32_t* deg, cudaStream_t s, const SegmentPrune* sp = nullptr);
 // K6 normalise init into [0, 10] per dimension (optimizer.rs:181-230), in place.

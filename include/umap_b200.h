@@ -264,12 +264,18 @@ int umap_optimizer_tuning(const umap_optimizer* opt, uint32_t* chunk, uint32_t* 
  * 8-row-loads-in-flight register budget), UMAP_LAYOUT_TWELVE_NEGATIVES (the 12-row budget of
  * renamed layouts; neither flag: 4), UMAP_LAYOUT_RENAMED (vertices renamed into a locality
  * order; DRAM-bound plain fits), UMAP_LAYOUT_GENERIC_RULE (the optimizer's MetricType is
- * Generic). */
+ * Generic), and the order in which tasks are dealt to warps: UMAP_LAYOUT_RATE_ORDER (by
+ * length, then by mean firing rate; small graphs), UMAP_LAYOUT_BLOCK_ORDER (by length inside
+ * blocks of 4096 consecutive rows; renamed layouts), UMAP_LAYOUT_ROW_ORDER (row order, forced
+ * only); none of the three: by length. */
 #define UMAP_LAYOUT_LANE_MAJOR 1u
 #define UMAP_LAYOUT_EIGHT_NEGATIVES 2u
 #define UMAP_LAYOUT_RENAMED 4u
 #define UMAP_LAYOUT_GENERIC_RULE 8u
 #define UMAP_LAYOUT_TWELVE_NEGATIVES 16u
+#define UMAP_LAYOUT_RATE_ORDER 32u
+#define UMAP_LAYOUT_BLOCK_ORDER 64u
+#define UMAP_LAYOUT_ROW_ORDER 128u
 int umap_optimizer_layout_flags(const umap_optimizer* opt, uint32_t* flags);
 
 /* ---- serde checkpoints (optimizer.rs:27, manifold.rs:14, embedding.rs:438) ---------

@@ -603,6 +603,8 @@ def test_relabelled_layout_is_the_same_fit(ub, oracle, monkeypatch):
     monkeypatch.setenv("UMAP_B200_RELABEL", "0")
     opt_p = ub.Optimizer(ub.Umap(cfg).learn_manifold(20000, idx, dist), init, 200, cfg)
     monkeypatch.delenv("UMAP_B200_RELABEL")
+    # renamed layouts deal tasks to warps by blocks of rows, small plain ones by length and rate
+    assert opt_r.layout()["task_order"] == "row blocks" and opt_p.layout()["task_order"] == "length+rate"
     assert np.array_equal(opt_r.embedding().view(np.uint32), opt_p.embedding().view(np.uint32))
     er, ep = opt_r.export_edges(), opt_p.export_edges()
     for a_, b_ in zip(er, ep):
@@ -659,6 +661,8 @@ def test_relabelled_layout_other_kernels(ub, monkeypatch, dim, generic):
     monkeypatch.delenv("UMAP_B200_RELABEL")
     r, p = opts["1"], opts["0"]
     assert r.layout()["renamed"] == (not generic) and not p.layout()["renamed"]
+    assert r.layout()["task_order"] == ("length+rate" if generic else "row blocks")
+    assert p.layout()["task_order"] == "length+rate"
     assert np.array_equal(r.embedding().view(np.uint32), p.embedding().view(np.uint32))
     for a_, b_ in zip(r.export_edges(), p.export_edges()):
         assert np.array_equal(a_, b_)
@@ -680,3 +684,41 @@ def test_relabelled_layout_other_kernels(ub, monkeypatch, dim, generic):
         ce[flag] = Q.fuzzy_cross_entropy(e, head, tail, w, a, b)
     print(f"dim {dim} generic {generic}: CE renamed {ce['1']:.6g} plain {ce['0']:.6g}")
     assert abs(ce["1"] - ce["0"]) <= 0.02 * ce["0"]
+
+
+@pytest.mark.parametrize("order,name", [("len", "length"), ("rate", "length+rate"), ("block", "row blocks"),
+                                        ("row", "rows")])
+def test_task_orders_are_the_same_fit(ub, monkeypatch, order, name):
+    """The order in which tasks are dealt to warps changes which rows update at the same time,
+    not what an epoch computes: under each forced order the layout reports it, the exported
+    edges and schedule totals equal the default layout's, and the fuzzy cross-entropy of a
+    60-epoch fit is within 2% of the default layout's."""
+    from umap_b200 import quality as Q
+    from umap_b200 import workloads as W
+    X, _ = W.swiss_roll(6000, seed=11)
+    idx, dist = W.knn_exact_numpy(X, 15)
+    init = W.uniform_init(6000, seed=6)
+    cfg = ub.UmapConfig()
+    cfg.optimization.n_epochs = 60
+    base = ub.Optimizer(ub.Umap(cfg).learn_manifold(6000, idx, dist), init, 60, cfg)
+    monkeypatch.setenv("UMAP_B200_TASK_ORDER", order)
+    forced = ub.Optimizer(ub.Umap(cfg).learn_manifold(6000, idx, dist), init, 60, cfg)
+    monkeypatch.delenv("UMAP_B200_TASK_ORDER")
+    assert forced.layout()["task_order"] == name
+    for a_, b_ in zip(forced.export_edges(), base.export_edges()):
+        assert np.array_equal(a_, b_)
+    assert forced.schedule_totals(0, 60) == base.schedule_totals(0, 60)
+    head, tail, _, _, _, _ = base.export_edges()
+    G = base.manifold().graph()
+    ip = G.indptr.astype(np.int64)
+    w = np.array([G.data[ip[x] + np.searchsorted(G.indices[ip[x]:ip[x + 1]], y)] for x, y in zip(head, tail)])
+    a, b = base.manifold().curve_params()
+    ce = []
+    for o in (base, forced):
+        o.set_seed(7)
+        o.step_epochs(60)
+        e = o.embedding()
+        assert np.isfinite(e).all()
+        ce.append(Q.fuzzy_cross_entropy(e, head, tail, w, a, b))
+    print(f"order {order}: CE {ce[1]:.6g} default {ce[0]:.6g}")
+    assert abs(ce[1] - ce[0]) <= 0.02 * ce[0]

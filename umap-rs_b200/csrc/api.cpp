@@ -2228,7 +2228,10 @@ int umap_optimizer_layout_flags(const umap_optimizer* opt, uint32_t* flags) {
            (opt->layout.short_epoch && !opt->layout.dram_epoch ? UMAP_LAYOUT_EIGHT_NEGATIVES : 0u) |
            (opt->layout.dram_epoch ? UMAP_LAYOUT_TWELVE_NEGATIVES : 0u) |
            (opt->layout.order.p ? UMAP_LAYOUT_RENAMED : 0u) |
-           (opt->metric_type == UMAP_METRIC_GENERIC ? UMAP_LAYOUT_GENERIC_RULE : 0u);
+           (opt->metric_type == UMAP_METRIC_GENERIC ? UMAP_LAYOUT_GENERIC_RULE : 0u) |
+           (opt->layout.task_order == TaskOrder::LengthRate ? UMAP_LAYOUT_RATE_ORDER : 0u) |
+           (opt->layout.task_order == TaskOrder::RowBlock ? UMAP_LAYOUT_BLOCK_ORDER : 0u) |
+           (opt->layout.task_order == TaskOrder::Row ? UMAP_LAYOUT_ROW_ORDER : 0u);
   API_END
 }
 

@@ -27,6 +27,7 @@
 #include <algorithm>
 #include <cstdint>
 #include <cstdlib>
+#include <cstring>
 #include <vector>
 
 #include "ub_internal.hpp"
@@ -543,12 +544,18 @@ __global__ void ptr_degree_kernel(const uint64_t* __restrict__ kptr, uint64_t n,
   ntask[u] = (d + chunk - 1) / chunk;
 }
 
-// One task per chunk of a row: row id, first kept-edge index, length, split flag.
+// One task per chunk of a row: row id, first kept-edge index, length, split flag, sort key.
+// The key orders tasks by descending length and, with rate_bits = RATE_BITS, then by
+// descending mean firing rate (sum over the task's edges of min(1, 1 / epochs_per_sample),
+// over its length, in RATE_BITS bits), so that a warp's lanes draw similar numbers of firings
+// per epoch; batched instances sort instance-major first.
+constexpr int RATE_BITS = 8;
 __global__ void task_fill_kernel(const uint64_t* __restrict__ kptr, const uint32_t* __restrict__ deg,
                                  const uint64_t* __restrict__ tptr, uint64_t n, uint32_t chunk,
-                                 const uint32_t* __restrict__ row_seg, int len_bits,
-                                 const uint32_t* __restrict__ order, uint32_t* __restrict__ trow,
-                                 uint64_t* __restrict__ tstart, uint32_t* __restrict__ tkey) {
+                                 const uint32_t* __restrict__ row_seg, int len_bits, int rate_bits,
+                                 int block_shift, const double* __restrict__ keps, const uint32_t* __restrict__ order,
+                                 uint32_t* __restrict__ trow, uint64_t* __restrict__ tstart,
+                                 uint32_t* __restrict__ tkey) {
   const uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= n) return;
   const uint64_t src = order ? order[r] : r;  // the kept-edge CSR row of layout row r
@@ -556,16 +563,33 @@ __global__ void task_fill_kernel(const uint64_t* __restrict__ kptr, const uint32
   const uint64_t t0 = tptr[r], nt = tptr[r + 1] - t0;
   for (uint64_t c = 0; c < nt; ++c) {
     const uint32_t len = (uint32_t)min((uint64_t)chunk, (uint64_t)d - c * chunk);
+    const uint64_t st = kptr[src] + c * chunk;
     trow[t0 + c] = (uint32_t)r | (nt > 1 ? 0x80000000u : 0u);   // high bit: partial row
-    tstart[t0 + c] = kptr[src] + c * chunk;
-    // ascending key = descending length; batched instances sort instance-major first
-    tkey[t0 + c] = (row_seg ? (row_seg[r] << len_bits) : 0u) | (chunk - len);
+    tstart[t0 + c] = st;
+    uint32_t rate = 0;
+    if (rate_bits) {
+      float sp = 0.0f;
+      for (uint32_t e = 0; e < len; ++e) {
+        const double x = keps[st + e];
+        sp += x > 1.0 ? (float)(1.0 / x) : (x > 0.0 ? 1.0f : 0.0f);
+      }
+      const uint32_t top = (1u << rate_bits) - 1u;
+      rate = top - min(top, (uint32_t)(sp / (float)max(len, 1u) * (float)(top + 1u)));
+    }
+    const uint32_t hi = block_shift >= 0 ? (uint32_t)(r >> block_shift) : (row_seg ? row_seg[r] : 0u);
+    tkey[t0 + c] = (((hi << len_bits) | (chunk - len)) << rate_bits) | rate;
   }
+}
+
+__global__ void iota_u32_kernel(uint32_t* __restrict__ p, uint64_t n) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) p[i] = (uint32_t)i;
 }
 
 __global__ void slice_meta_kernel(const uint32_t* __restrict__ perm, const uint32_t* __restrict__ trow,
                                   const uint32_t* __restrict__ skey, uint64_t T, uint64_t n_slices,
-                                  uint32_t chunk, uint32_t len_mask, bool lane_major, uint32_t* __restrict__ width,
+                                  uint32_t chunk, int rate_bits, uint32_t len_mask, bool lane_major,
+                                  uint32_t* __restrict__ width,
                                   uint32_t* __restrict__ rowid, uint32_t* __restrict__ split_mask) {
   const uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= n_slices * 32) return;
@@ -573,7 +597,7 @@ __global__ void slice_meta_kernel(const uint32_t* __restrict__ perm, const uint3
   rowid[q] = tr == PAD_ROW ? PAD_ROW : (tr & 0x7FFFFFFFu);
   const unsigned bits = __ballot_sync(0xFFFFFFFFu, tr != PAD_ROW && (tr & 0x80000000u));
   // slice width = longest task of the slice (instance-major order: the max over lanes)
-  uint32_t len = q < T ? chunk - (skey[q] & len_mask) : 0u;
+  uint32_t len = q < T ? chunk - ((skey[q] >> rate_bits) & len_mask) : 0u;
   for (int o = 16; o > 0; o >>= 1) len = max(len, __shfl_xor_sync(0xFFFFFFFFu, len, o));
   // whole register windows per lane (UB_SGD2_W entries, a multiple of one 4-entry sector): the
   // lane-major epoch loads a full window without a bounds check
@@ -587,7 +611,7 @@ __global__ void slice_meta_kernel(const uint32_t* __restrict__ perm, const uint3
 __global__ void slice_fill_kernel(const uint32_t* __restrict__ ktail, const double* __restrict__ keps,
                                   const uint32_t* __restrict__ perm, const uint64_t* __restrict__ tstart,
                                   const uint32_t* __restrict__ skey, uint64_t T, uint32_t chunk,
-                                  uint32_t len_mask, const uint64_t* __restrict__ wscan,
+                                  int rate_bits, uint32_t len_mask, const uint64_t* __restrict__ wscan,
                                   const uint32_t* __restrict__ width, uint64_t n_slices, bool lane_major,
                                   const uint32_t* __restrict__ rank, uint2* __restrict__ entry) {
   const uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -599,7 +623,7 @@ __global__ void slice_fill_kernel(const uint32_t* __restrict__ ktail, const doub
   uint32_t e = 0;
   if (q < T) {
     const uint64_t st = tstart[perm[q]];
-    const uint32_t len = chunk - (skey[q] & len_mask);
+    const uint32_t len = chunk - ((skey[q] >> rate_bits) & len_mask);
     for (; e < len; ++e)
       entry[lane_major ? base + (uint64_t)lane * wd + e : base + (uint64_t)e * 32 + lane] =
           make_uint2(rank ? rank[ktail[st + e]] : ktail[st + e], q_minus_1(keps[st + e]));
@@ -933,6 +957,34 @@ bool pick_relabel(uint64_t n, bool segmented) {
   return n > 4000000ull;
 }
 
+// Order in which the tasks are dealt to warps (32 consecutive tasks per warp):
+//  * Length: descending length (a warp's lanes scan equally long tasks; least padding).
+//  * LengthRate: length, then descending mean firing rate, so that a warp's lanes draw similar
+//    numbers of firings per epoch.  Small graphs, whose epochs are short and bound by their
+//    warps' busiest lanes (100k-point fit: 25.4-25.6 against 26.0-26.1 ms).
+//  * RowBlock: blocks of 2^TASK_BLOCK_SHIFT consecutive layout rows, length order inside each.
+//    Renamed layouts: their warps in flight then cover a narrow range of new ids, whose tails
+//    stay in L2 (30 epochs of the 20M-point roll: 292.6 ms in length order, 245.7 in row
+//    order, blocks of 2^6 / 2^8 / 2^10 / 2^12 / 2^14 / 2^16 rows: 241.4 / 237.7 / 235.6 /
+//    235.3-239.1 / 239.7 / 242.9 ms; 40M points, 24 epochs: 564.7 -> 475.9 ms).
+//  * Row: layout row order (measurement only; the 2M-point fit takes 5x as long in it, its
+//    whole-row tasks of very different lengths padded to the longest of each warp).
+// Plain fits without renaming keep Length at any size that is not short (2M points: 320.6 in
+// LengthRate against 321.0 ms, within noise; a block order: 1106 ms).  Batched instances keep
+// Length inside each instance.  UMAP_B200_TASK_ORDER=len / rate / block / row forces one.
+constexpr int TASK_BLOCK_SHIFT = 12;
+TaskOrder pick_task_order(bool renamed, bool short_graph, bool segmented) {
+  if (const char* e = getenv("UMAP_B200_TASK_ORDER")) {
+    if (!strcmp(e, "len")) return TaskOrder::Length;
+    if (!strcmp(e, "rate")) return TaskOrder::LengthRate;
+    if (!strcmp(e, "block") && !segmented) return TaskOrder::RowBlock;
+    if (!strcmp(e, "row")) return TaskOrder::Row;
+  }
+  if (segmented) return TaskOrder::Length;
+  if (renamed) return TaskOrder::RowBlock;
+  return short_graph ? TaskOrder::LengthRate : TaskOrder::Length;
+}
+
 void build_sgd_layout(const uint64_t* kept_ptr, const uint32_t* ktail, const double* keps, uint64_t n,
                       uint32_t chunk, SgdLayout& L, cudaStream_t s, const Segments* seg, bool rename) {
   L.n_vertices = n;
@@ -970,13 +1022,32 @@ void build_sgd_layout(const uint64_t* kept_ptr, const uint32_t* ktail, const dou
   const uint32_t len_mask = (1u << len_bits) - 1u;
   const uint32_t n_seg = seg ? seg->n_seg : 0u;
   if ((uint64_t)n_seg << len_bits >= (1ull << 32)) throw Error(UNSUPPORTED, "too many instances for the task sort key");
+  const int seg_bits = n_seg ? bits_for(n_seg) : 0;
+  const bool renamed = L.order.p != nullptr;
+  TaskOrder torder = pick_task_order(renamed, pick_short_epoch((T + 31) / 32, renamed), seg != nullptr);
+  if (torder == TaskOrder::LengthRate && len_bits + seg_bits + RATE_BITS > 32) torder = TaskOrder::Length;
+  L.task_order = torder;
+  const int rate_bits = torder == TaskOrder::LengthRate ? RATE_BITS : 0;
+  int block_shift = -1, block_bits = 0;
+  if (torder == TaskOrder::RowBlock) {
+    block_shift = TASK_BLOCK_SHIFT;
+    if (const char* e = getenv("UMAP_B200_TASK_BLOCK")) block_shift = std::min(31, std::max(0, atoi(e)));
+    while (bits_for(n >> block_shift) + len_bits > 32) ++block_shift;  // the key fits 32 bits
+    block_bits = bits_for(n >> block_shift);
+  }
   if (n) {
     task_fill_kernel<<<grid_for(n, 256), 256, 0, s>>>(kept_ptr, deg.p, tptr.p, n, L.chunk,
-                                                      seg ? seg->row_seg : nullptr, len_bits, L.order.p,
-                                                      trow.p, tstart.p, tkey.p);
+                                                      seg ? seg->row_seg : nullptr, len_bits, rate_bits, block_shift,
+                                                      keps, L.order.p, trow.p, tstart.p, tkey.p);
     UB_LAUNCH_CHECK();
   }
-  if (T) radix_sort_pairs(tkey.p, nullptr, skey.p, perm.p, T, len_bits + (n_seg ? bits_for(n_seg) : 0), s);
+  if (T && torder == TaskOrder::Row) {
+    iota_u32_kernel<<<grid_for(T, 256), 256, 0, s>>>(perm.p, T);
+    UB_LAUNCH_CHECK();
+    UB_CUDA(cudaMemcpyAsync(skey.p, tkey.p, T * 4, cudaMemcpyDeviceToDevice, s));
+  } else if (T) {
+    radix_sort_pairs(tkey.p, nullptr, skey.p, perm.p, T, len_bits + (block_shift >= 0 ? block_bits : seg_bits) + rate_bits, s);
+  }
   L.n_slices = (T + 31) / 32;
   L.slice_width.alloc(L.n_slices, s);
   L.split_mask.alloc(L.n_slices, s);
@@ -984,7 +1055,7 @@ void build_sgd_layout(const uint64_t* kept_ptr, const uint32_t* ktail, const dou
   L.slice_base.alloc(L.n_slices + 1, s);
   if (L.n_slices) {
     slice_meta_kernel<<<grid_for(L.n_slices * 32, 256), 256, 0, s>>>(perm.p, trow.p, skey.p, T, L.n_slices,
-                                                                        L.chunk, len_mask, L.lane_major,
+                                                                        L.chunk, rate_bits, len_mask, L.lane_major,
                                                                         L.slice_width.p, L.rowid.p,
                                                                         L.split_mask.p);
     UB_LAUNCH_CHECK();
@@ -998,7 +1069,7 @@ void build_sgd_layout(const uint64_t* kept_ptr, const uint32_t* ktail, const dou
   L.entry.alloc(L.n_entries, s);
   if (L.n_slices) {
     slice_fill_kernel<<<grid_for(L.n_slices * 32, 256), 256, 0, s>>>(ktail, keps, perm.p, tstart.p, skey.p, T,
-                                                                        L.chunk, len_mask, wscan.p,
+                                                                        L.chunk, rate_bits, len_mask, wscan.p,
                                                                         L.slice_width.p, L.n_slices,
                                                                         L.lane_major, rank.p, L.entry.p);
     UB_LAUNCH_CHECK();

@@ -178,6 +178,9 @@ void count_empty_rows(const uint64_t* indptr, const float* data, uint64_t n,
 // arithmetic exact in 32 bits (see negatives_at in sgd.cu).
 constexpr uint64_t MAX_EPOCHS = 1ull << 21;
 
+// Order in which build_sgd_layout deals tasks to warps (sgd.cu, pick_task_order).
+enum class TaskOrder { Length, LengthRate, RowBlock, Row };
+
 struct SgdLayout {
   uint64_t n_vertices = 0, n_edges = 0, n_entries = 0, n_slices = 0, n_tasks = 0;
   uint32_t max_degree = 0, chunk = 0;
@@ -185,6 +188,7 @@ struct SgdLayout {
   bool short_epoch = false;      // epoch kernel budget for graphs of at most ~2 waves of warps
   bool dram_epoch = false;       // 12-negatives budget of renamed DRAM-bound layouts
   bool lane_major = true;        // entry order: lane major (true) or interleaved by lane
+  TaskOrder task_order = TaskOrder::Length;
   uint64_t split_tasks = 0;
   DevBuf<uint64_t> slice_base;   // [n_slices + 1]
   DevBuf<uint32_t> slice_width;  // [n_slices]

@@ -653,7 +653,8 @@ class Optimizer(_Handle):
 
     def layout(self) -> dict:
         """How the SGD layout is laid out: lane-major entries, the 8-negatives register
-        budget, vertices renamed into a locality order; and the epoch kernel it selects."""
+        budget, vertices renamed into a locality order, the order tasks are dealt to warps
+        ("length", "length+rate", "row blocks" or "rows"); and the epoch kernel it selects."""
         f = C.c_uint32()
         _check(_lib.load().umap_optimizer_layout_flags(self._get(), C.byref(f)))
         lm, eight, renamed, generic, twelve = (bool(f.value & b) for b in (1, 2, 4, 8, 16))
@@ -664,8 +665,10 @@ class Optimizer(_Handle):
         gen = "true" if generic else "false"
         kernel = (f"sgd_epoch_kernel2<{dim}, {gen}, {nb}, {minb}, {'true' if lm else 'false'}>" if dim <= 4
                   else f"sgd_epoch_anydim<{gen}>")
+        order = ("length+rate" if f.value & 32 else "row blocks" if f.value & 64 else "rows" if f.value & 128
+                 else "length")
         return {"lane_major": lm, "eight_negatives": eight, "twelve_negatives": twelve, "renamed": renamed,
-                "generic_rule": generic, "kernel": kernel}
+                "generic_rule": generic, "task_order": order, "kernel": kernel}
 
     def tuning(self):
         """(task length, threads per block) of the SGD kernel in use."""

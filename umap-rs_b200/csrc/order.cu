@@ -14,6 +14,7 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <cstdlib>
 
 #include "ub_internal.hpp"
 
@@ -21,6 +22,9 @@ namespace ub {
 namespace {
 
 constexpr uint32_t UNSEEN = 0xFFFFFFFFu;
+// Vertices per BFS source.  30 epochs of a renamed 20M-point roll (tasks by length inside
+// blocks of 4,096 rows): 4,096: 238.0 ms, 16,384: 236.9-237.1, 65,536: 237.5, 262,144: 238.0;
+// UMAP_B200_BFS_REGION overrides it for such measurements.
 constexpr uint64_t REGION = 16384;
 
 __global__ void seed_kernel(uint64_t n, uint32_t n_seeds, uint32_t* __restrict__ label, uint32_t* __restrict__ queue) {
@@ -102,7 +106,12 @@ void locality_order(const uint64_t* kptr, const uint32_t* ktail, uint64_t n, uin
                     cudaStream_t s) {
   if (n == 0) return;
   if (n >= 0xFFFFFFFFull) throw Error(UNSUPPORTED, "locality order: n must be < 2^32");
-  const uint32_t n_seeds = (uint32_t)std::max<uint64_t>(1, n / REGION);
+  uint64_t region = REGION;
+  if (const char* e = getenv("UMAP_B200_BFS_REGION")) {
+    const long v = atol(e);
+    if (v >= 64 && v <= (1l << 30)) region = (uint64_t)v;
+  }
+  const uint32_t n_seeds = (uint32_t)std::max<uint64_t>(1, n / region);
   DevBuf<uint32_t> label(n, s), level(n, s), qa(n, s), qb(n, s);
   DevBuf<unsigned long long> cnt(1, s);
   UB_CUDA(cudaMemsetAsync(label.p, 0xFF, n * 4, s));

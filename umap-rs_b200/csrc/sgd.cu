@@ -42,6 +42,9 @@ constexpr uint32_t PAD_ROW = 0xFFFFFFFFu;
 // 5 resident 256-thread blocks per SM (48 registers).  Graphs that fill about two waves or
 // fewer are bound by the chain of dependent loads of their busiest lanes: 8 negative rows
 // fetched together (one round trip for a firing's usual 4-6 negatives) and 4 blocks per SM.
+// On the 2M-point workload (500 epochs, SGD ms) the wide budget's occupancy beats the extra
+// round trip of a firing's fifth negative: 4 / 5: 314.0, 8 / 4: 317.6, 6 / 4: 330.9, 4 / 4:
+// 343.5, 5 / 4: 349.9 (5 and 6 rows at 5 blocks per SM spill more than 4 / 5's 16 bytes).
 constexpr int NB_WIDE = 4, MINB_WIDE = 5;
 constexpr int NB_SHORT = 8, MINB_SHORT = 4;
 // Renamed DRAM-bound layouts: 12 negative rows fetched together, 3 blocks per SM.  Their random

@@ -265,7 +265,7 @@ int umap_optimizer_tuning(const umap_optimizer* opt, uint32_t* chunk, uint32_t* 
  * renamed layouts; neither flag: 4), UMAP_LAYOUT_RENAMED (vertices renamed into a locality
  * order; DRAM-bound plain fits), UMAP_LAYOUT_GENERIC_RULE (the optimizer's MetricType is
  * Generic), and the order in which tasks are dealt to warps: UMAP_LAYOUT_RATE_ORDER (by
- * length, then by mean firing rate; small graphs), UMAP_LAYOUT_BLOCK_ORDER (by length inside
+ * length, then by mean firing rate; small graphs and batched instances), UMAP_LAYOUT_BLOCK_ORDER (by length inside
  * blocks of 4096 consecutive rows; renamed layouts), UMAP_LAYOUT_ROW_ORDER (row order, forced
  * only); none of the three: by length. */
 #define UMAP_LAYOUT_LANE_MAJOR 1u

@@ -33,6 +33,7 @@ def test_batch_matches_per_instance_plain_fits(ub):
     cfg = ub.UmapConfig()
     total = 120
     bopt = ub.Optimizer.batch(cfg, off, np.vstack(idxs), np.vstack(dists), np.vstack(inits), total)
+    assert bopt.layout()["task_order"] == "length+rate"   # inside each instance
     G = bopt.manifold().graph()
     bs, br = bopt.manifold().sigmas_rhos()
     bh, bt, be, _, _, _ = bopt.export_edges()

@@ -973,8 +973,9 @@ bool pick_relabel(uint64_t n, bool segmented) {
 //  * Row: layout row order (measurement only; the 2M-point fit takes 5x as long in it, its
 //    whole-row tasks of very different lengths padded to the longest of each warp).
 // Plain fits without renaming keep Length at any size that is not short (2M points: 320.6 in
-// LengthRate against 321.0 ms, within noise; a block order: 1106 ms).  Batched instances keep
-// Length inside each instance.  UMAP_B200_TASK_ORDER=len / rate / block / row forces one.
+// LengthRate against 321.0 ms, within noise; a block order: 1106 ms).  Batched instances take
+// LengthRate inside each instance (4,096 instances, 200 epochs: 2,822-2,825 against
+// 2,842-2,843 ms per batch).  UMAP_B200_TASK_ORDER=len / rate / block / row forces one.
 constexpr int TASK_BLOCK_SHIFT = 12;
 TaskOrder pick_task_order(bool renamed, bool short_graph, bool segmented) {
   if (const char* e = getenv("UMAP_B200_TASK_ORDER")) {
@@ -983,7 +984,7 @@ TaskOrder pick_task_order(bool renamed, bool short_graph, bool segmented) {
     if (!strcmp(e, "block") && !segmented) return TaskOrder::RowBlock;
     if (!strcmp(e, "row")) return TaskOrder::Row;
   }
-  if (segmented) return TaskOrder::Length;
+  if (segmented) return TaskOrder::LengthRate;
   if (renamed) return TaskOrder::RowBlock;
   return short_graph ? TaskOrder::LengthRate : TaskOrder::Length;
 }

@@ -557,7 +557,9 @@ def test_persisting_l2_set_aside_released_with_the_last_optimizer(ub):
     """An optimizer puts its embedding in a persisting-L2 window, which reserves a device-wide
     L2 set-aside.  The set-aside stays while any optimizer on the device holds a window and
     returns to 0 when the last one is consumed (into_fitted) or freed, so the host
-    application's own kernels get the whole L2 back."""
+    application's own kernels get the whole L2 back.  An embedding pair larger than the
+    device's persisting maximum gets no window and leaves the set-aside as it found it (a
+    context may start with a nonzero default)."""
     import torch
     from cuda.bindings import runtime as rt
 
@@ -568,6 +570,17 @@ def test_persisting_l2_set_aside_released_with_the_last_optimizer(ub):
         return v
 
     idx, dist, init = small_gauss(3000, 15, seed=5)
+    err, max_persist = rt.cudaDeviceGetAttribute(rt.cudaDeviceAttr.cudaDevAttrMaxPersistingL2CacheSize, 0)
+    assert err == rt.cudaError_t.cudaSuccess
+    wide = max_persist // (2 * 3000 * 4) + 8          # components: live + snapshot > max_persist
+    cfg_w = ub.UmapConfig()
+    cfg_w.n_components = wide
+    cfg_w.optimization.n_epochs = 20
+    init_w = np.random.default_rng(5).uniform(-10, 10, (3000, wide)).astype(np.float32)
+    before = limit()
+    big = ub.Optimizer(ub.Umap(cfg_w).learn_manifold(3000, idx, dist), init_w, 20, cfg_w)
+    assert limit() == before
+    del big
     cfg = ub.UmapConfig()
     cfg.optimization.n_epochs = 20
     u = ub.Umap(cfg)
@@ -643,8 +656,10 @@ def test_relabelled_layout_other_kernels(ub, monkeypatch, dim, generic):
     """The renamed layout through the epoch kernels other than the 2-D Euclidean one (1-D and
     3-D instantiations, the any-dimension kernel): normalised init, exported edges and
     schedule totals equal the plain layout's, the embedding comes back finite in the caller's
-    order, and its fuzzy cross-entropy is within 2% of a plain-layout fit's.  The generic
-    rule keeps the caller's order even when renaming is forced."""
+    order, and the mean fuzzy cross-entropy of 4 seeded fits is within three standard errors
+    (at least 0.5%) of the plain layout's mean.  One 1-D fit of this case spreads by 1-2%
+    from seed to seed, so single runs are not compared.  The generic rule keeps the caller's
+    order even when renaming is forced."""
     from umap_b200 import quality as Q
     from umap_b200 import workloads as W
     X, _ = W.swiss_roll(6000, seed=9)
@@ -672,18 +687,26 @@ def test_relabelled_layout_other_kernels(ub, monkeypatch, dim, generic):
     ip = G.indptr.astype(np.int64)
     w = np.array([G.data[ip[x] + np.searchsorted(G.indices[ip[x]:ip[x + 1]], y)] for x, y in zip(head, tail)])
     a, b = p.manifold().curve_params()
-    ce = {}
-    for flag, o in opts.items():
-        o.set_seed(5)
-        if generic:
-            o.step_epochs(60, ub.GenericEuclideanMetric())
-        else:
-            o.step_epochs(60)
-        e = o.embedding()
-        assert e.shape == (6000, dim) and np.isfinite(e).all()
-        ce[flag] = Q.fuzzy_cross_entropy(e, head, tail, w, a, b)
-    print(f"dim {dim} generic {generic}: CE renamed {ce['1']:.6g} plain {ce['0']:.6g}")
-    assert abs(ce["1"] - ce["0"]) <= 0.02 * ce["0"]
+    ce = {"1": [], "0": []}
+    for seed in range(4):
+        for flag in ("1", "0"):
+            if seed:
+                monkeypatch.setenv("UMAP_B200_RELABEL", flag)
+                opts[flag] = ub.Optimizer(ub.Umap(cfg).learn_manifold(6000, idx, dist), init, 60, cfg, mt)
+                monkeypatch.delenv("UMAP_B200_RELABEL")
+            o = opts[flag]
+            o.set_seed(5 + seed)
+            if generic:
+                o.step_epochs(60, ub.GenericEuclideanMetric())
+            else:
+                o.step_epochs(60)
+            e = o.embedding()
+            assert e.shape == (6000, dim) and np.isfinite(e).all()
+            ce[flag].append(Q.fuzzy_cross_entropy(e, head, tail, w, a, b))
+    mr, mp = np.mean(ce["1"]), np.mean(ce["0"])
+    se = np.sqrt(np.var(ce["1"], ddof=1) / 4 + np.var(ce["0"], ddof=1) / 4)
+    print(f"dim {dim} generic {generic}: CE renamed {mr:.6g} plain {mp:.6g} (standard error {se:.3g})")
+    assert abs(mr - mp) <= max(3.0 * se, 0.005 * mp)
 
 
 @pytest.mark.parametrize("order,name", [("len", "length"), ("rate", "length+rate"), ("block", "row blocks"),

@@ -392,6 +392,12 @@ void set_l2_window(umap_optimizer& o, bool enable) {
     UB_CUDA(cudaDeviceGetAttribute(&max_window, cudaDevAttrMaxAccessPolicyWindowSize, dev));
     if (max_persist <= 0 || max_window <= 0) return;
     const size_t bytes = o.emb2.bytes();
+    // Only an embedding pair that can persist whole gets a window.  A larger one (the
+    // DRAM-bound, renamed layouts) is read in another vertex order during the epochs, and the
+    // lines its gather marks persisting would hold the set-aside unused: renamed 20M / 40M-point
+    // rolls ran 7-9% faster without it (30 epochs 239.0-239.4 -> 222.3-223.7 ms; 24 epochs
+    // 475.8-476.2 -> 431.5 ms), and a window moved onto the working snapshot changed nothing.
+    if (bytes > (size_t)max_persist) return;
     const size_t lim = std::min(bytes, (size_t)max_persist);
     {
       std::lock_guard<std::mutex> lock(g_l2_mu);

@@ -541,7 +541,7 @@ def run_warm_start(a):
 def swiss_traffic(edges):
     """DRAM bytes per SGD launch at `edges` kept edges, scaled from the 40M-point capture of
     the renamed layout (a lower bound at larger sizes: traffic per edge still grows with the
-    embedding, 47 / 129 / 185 bytes per kept edge at 10M / 20M / 40M points)."""
+    embedding, 47 / 128 / 184 bytes per kept edge at 10M / 20M / 40M points)."""
     t = ncu_figure("sgd_epoch_swiss_roll_40m_renamed", "traffic_bytes_per_launch")
     e0 = ncu_figure("sgd_epoch_swiss_roll_40m_renamed", "kept_edges")
     return t * edges / e0 if t and e0 else None

@@ -257,7 +257,16 @@ __device__ __forceinline__ void fired_edge(float (&cur)[DIM], uint32_t r, uint32
         }
         const uint32_t rv = (qq & 1) ? (uint32_t)(rnd >> 32) : (uint32_t)rnd;
         kk[q] = seg_lo + __umulhi(rv, seg_n);
-        load_row<DIM>(ob[q], snap + (uint64_t)kk[q] * DIM);
+        if constexpr (DIM == 2) {
+          // uniform rows, rarely reused by this SM: cached in L2 only, so they do not evict
+          // the tail and head lines L1 serves (2M workload, 500 epochs: 311.1-311.2 against
+          // 311.8-311.9 ms; renamed 20M roll, 30 epochs: 219.7-220.1 against 221.3-223.6 ms)
+          const float2 t = __ldcg(reinterpret_cast<const float2*>(snap + (uint64_t)kk[q] * DIM));
+          ob[q][0] = t.x;
+          ob[q][1] = t.y;
+        } else {
+          load_row<DIM>(ob[q], snap + (uint64_t)kk[q] * DIM);
+        }
       }
     }
   };

@@ -32,6 +32,14 @@ def test_python_binding_covers_header(ub):
     assert names == set(_lib.SIGNATURES)
 
 
+def test_layout_flag_bits_match_header(ub):
+    """The layout flags the Python binding decodes are the header's UMAP_LAYOUT_* values."""
+    from umap_b200 import _lib
+    txt = open(HEADER).read()
+    defs = {m.group(1): int(m.group(2)) for m in re.finditer(r"#define UMAP_LAYOUT_(\w+) (\d+)u", txt)}
+    assert defs == _lib.LAYOUT_FLAGS
+
+
 def test_config_default_matches_reference(ub):
     # config.rs:43-52, :117-127, :171-180, :226-235
     c = ub._lib.UmapConfigC()

@@ -657,7 +657,10 @@ class Optimizer(_Handle):
         ("length", "length+rate", "row blocks" or "rows"); and the epoch kernel it selects."""
         f = C.c_uint32()
         _check(_lib.load().umap_optimizer_layout_flags(self._get(), C.byref(f)))
-        lm, eight, renamed, generic, twelve = (bool(f.value & b) for b in (1, 2, 4, 8, 16))
+        bit = _lib.LAYOUT_FLAGS
+        lm, eight, renamed, generic, twelve = (bool(f.value & bit[k]) for k in
+                                               ("LANE_MAJOR", "EIGHT_NEGATIVES", "RENAMED", "GENERIC_RULE",
+                                                "TWELVE_NEGATIVES"))
         _, dim = self.dims()
         eight = eight and dim <= 2 and not generic  # the generic rule keeps the 4-negatives budget
         twelve = twelve and dim <= 2 and not generic
@@ -665,8 +668,8 @@ class Optimizer(_Handle):
         gen = "true" if generic else "false"
         kernel = (f"sgd_epoch_kernel2<{dim}, {gen}, {nb}, {minb}, {'true' if lm else 'false'}>" if dim <= 4
                   else f"sgd_epoch_anydim<{gen}>")
-        order = ("length+rate" if f.value & 32 else "row blocks" if f.value & 64 else "rows" if f.value & 128
-                 else "length")
+        order = ("length+rate" if f.value & bit["RATE_ORDER"] else "row blocks" if f.value & bit["BLOCK_ORDER"]
+                 else "rows" if f.value & bit["ROW_ORDER"] else "length")
         return {"lane_major": lm, "eight_negatives": eight, "twelve_negatives": twelve, "renamed": renamed,
                 "generic_rule": generic, "task_order": order, "kernel": kernel}
 

@@ -39,6 +39,10 @@ class WarmStartParamsC(C.Structure):
     ]
 
 
+# umap_optimizer_layout_flags bits (UMAP_LAYOUT_* in include/umap_b200.h)
+LAYOUT_FLAGS = {"LANE_MAJOR": 1, "EIGHT_NEGATIVES": 2, "RENAMED": 4, "GENERIC_RULE": 8, "TWELVE_NEGATIVES": 16,
+                "RATE_ORDER": 32, "BLOCK_ORDER": 64, "ROW_ORDER": 128}
+
 WARM_START_PHASES = ("prepare", "subsample_fit", "mlp_train", "mlp_predict", "wait_full_graph", "fit",
                      "full_graph_overlapped", "total")
 

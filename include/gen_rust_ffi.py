@@ -70,11 +70,14 @@ def parse(header: str):
                 params.append((mm.group(2), rust_type(mm.group(1))))
         funcs.append((name, rust_type(ret), params))
     ver = re.search(r"#define\s+UMAP_B200_ABI_VERSION\s+(\d+)", src).group(1)
-    return ver, enums, fields, opaque, funcs
+    # other numeric #defines: layout flag bits (u32) and counts such as the warm start's phases
+    defines = [(n, "u32" if u else "usize", v) for n, v, u in
+               re.findall(r"^#define\s+(UMAP_\w+)\s+(\d+)(u?)\b", src, re.M) if n != "UMAP_B200_ABI_VERSION"]
+    return ver, enums, fields, opaque, funcs, defines
 
 
 def render(header: str) -> str:
-    ver, enums, fields, opaque, funcs = parse(header)
+    ver, enums, fields, opaque, funcs, defines = parse(header)
     out = ["// Generated from include/umap_b200.h by include/gen_rust_ffi.py; do not edit by hand.",
            "// Every entry point of the B200 UMAP library, for a Rust crate's src/ffi.rs.",
            "#![allow(non_camel_case_types, dead_code)]",
@@ -82,6 +85,7 @@ def render(header: str) -> str:
            "",
            f"pub const UMAP_B200_ABI_VERSION: c_int = {ver};"]
     out += [f"pub const {n}: c_int = {v};" for n, v in enums]
+    out += [f"pub const {n}: {t} = {v};" for n, t, v in defines]
     out += ["", "#[repr(C)]", "#[derive(Clone, Copy, Debug, Default)]", "pub struct umap_config {"]
     out += [f"    pub {n}: {t}," for n, t in fields]
     out += ["}", ""]

@@ -16,6 +16,15 @@ pub const UMAP_ERR_UNSUPPORTED: c_int = 8;
 pub const UMAP_METRIC_EUCLIDEAN: c_int = 0;
 pub const UMAP_METRIC_GENERIC: c_int = 1;
 pub const UMAP_OUTPUT_METRIC_EUCLIDEAN: c_int = 0;
+pub const UMAP_LAYOUT_LANE_MAJOR: u32 = 1;
+pub const UMAP_LAYOUT_EIGHT_NEGATIVES: u32 = 2;
+pub const UMAP_LAYOUT_RENAMED: u32 = 4;
+pub const UMAP_LAYOUT_GENERIC_RULE: u32 = 8;
+pub const UMAP_LAYOUT_TWELVE_NEGATIVES: u32 = 16;
+pub const UMAP_LAYOUT_RATE_ORDER: u32 = 32;
+pub const UMAP_LAYOUT_BLOCK_ORDER: u32 = 64;
+pub const UMAP_LAYOUT_ROW_ORDER: u32 = 128;
+pub const UMAP_WARM_START_PHASES: usize = 8;
 
 #[repr(C)]
 #[derive(Clone, Copy, Debug, Default)]

@@ -40,6 +40,34 @@ def test_layout_flag_bits_match_header(ub):
     assert defs == _lib.LAYOUT_FLAGS
 
 
+@pytest.mark.parametrize("flags,dims,expect", [
+    (1 | 2 | 32, 2, {"lane_major": True, "eight_negatives": True, "task_order": "length+rate",
+                     "kernel": "sgd_epoch_kernel2<2, false, 8, 4, true>"}),
+    (4 | 16 | 64, 2, {"renamed": True, "twelve_negatives": True, "task_order": "row blocks",
+                      "kernel": "sgd_epoch_kernel2<2, false, 12, 3, false>"}),
+    (1, 2, {"task_order": "length", "kernel": "sgd_epoch_kernel2<2, false, 4, 5, true>"}),
+    (1 | 8 | 2, 2, {"generic_rule": True, "eight_negatives": False,
+                    "kernel": "sgd_epoch_kernel2<2, true, 4, 5, true>"}),
+    (128, 5, {"task_order": "rows", "kernel": "sgd_epoch_anydim<false>"}),
+])
+def test_layout_flags_decoded_without_gpu(ub, monkeypatch, flags, dims, expect):
+    """Optimizer.layout() turns umap_optimizer_layout_flags into the kernel it selects."""
+    from umap_b200 import _lib
+
+    class StubLib:
+        def umap_optimizer_layout_flags(self, h, out):
+            out._obj.value = flags
+            return 0
+
+    opt = ub.Optimizer.__new__(ub.Optimizer)
+    monkeypatch.setattr(_lib, "load", lambda: StubLib())
+    monkeypatch.setattr(type(opt), "_get", lambda self: None)
+    monkeypatch.setattr(type(opt), "dims", lambda self: (10, dims))
+    got = opt.layout()
+    for k, v in expect.items():
+        assert got[k] == v, (k, got)
+
+
 def test_config_default_matches_reference(ub):
     # config.rs:43-52, :117-127, :171-180, :226-235
     c = ub._lib.UmapConfigC()

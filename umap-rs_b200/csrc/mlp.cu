@@ -89,6 +89,7 @@ struct EpiArgs {
 // blockIdx.y == 0 also write the transposed copy xt [K, ldt] (for dW1).
 struct GatherA {
   const float* X;
+  const __nv_bfloat16* Xb;  // if set: rows already standardised and rounded (training), read instead of X
   int ldx;
   const uint32_t* rows;
   int64_t n_valid;
@@ -258,22 +259,30 @@ __global__ void __launch_bounds__(GT) umma_gemm_kernel(const bf16* __restrict__ 
         const int64_t b = m0 + r;
         const int64_t src = ga.rows ? (int64_t)ga.rows[b] : (b < ga.n_valid ? b : ga.n_valid - 1);
         const int64_t k0 = kg + c8 * 8;
-        const float4* xp = reinterpret_cast<const float4*>(ga.X + src * ga.ldx + k0);
-        const float4 x0 = __ldg(xp), x1 = __ldg(xp + 1);
-        float f[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
-        if (ga.scale) {
-          // shift / scale hold in_dim floats from a 256-byte aligned allocation; k0 % 8 == 0
-          const float4* sp = reinterpret_cast<const float4*>(ga.shift + k0);
-          const float4* cp = reinterpret_cast<const float4*>(ga.scale + k0);
-          const float4 s0 = __ldg(sp), s1 = __ldg(sp + 1), c0 = __ldg(cp), c1 = __ldg(cp + 1);
-          const float sh[8] = {s0.x, s0.y, s0.z, s0.w, s1.x, s1.y, s1.z, s1.w};
-          const float sc[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
-#pragma unroll
-          for (int e = 0; e < 8; ++e) f[e] = (f[e] - sh[e]) * sc[e];
-        }
         uint32_t pk[4];
+        if (ga.Xb) {
+          const uint4 u = __ldg(reinterpret_cast<const uint4*>(ga.Xb + src * ga.ldx + k0));
+          pk[0] = u.x;
+          pk[1] = u.y;
+          pk[2] = u.z;
+          pk[3] = u.w;
+        } else {
+          const float4* xp = reinterpret_cast<const float4*>(ga.X + src * ga.ldx + k0);
+          const float4 x0 = __ldg(xp), x1 = __ldg(xp + 1);
+          float f[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
+          if (ga.scale) {
+            // shift / scale hold in_dim floats from a 256-byte aligned allocation; k0 % 8 == 0
+            const float4* sp = reinterpret_cast<const float4*>(ga.shift + k0);
+            const float4* cp = reinterpret_cast<const float4*>(ga.scale + k0);
+            const float4 s0 = __ldg(sp), s1 = __ldg(sp + 1), c0 = __ldg(cp), c1 = __ldg(cp + 1);
+            const float sh[8] = {s0.x, s0.y, s0.z, s0.w, s1.x, s1.y, s1.z, s1.w};
+            const float sc[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
 #pragma unroll
-        for (int e = 0; e < 4; ++e) pk[e] = pack_bf16(f[2 * e], f[2 * e + 1]);
+            for (int e = 0; e < 8; ++e) f[e] = (f[e] - sh[e]) * sc[e];
+          }
+#pragma unroll
+          for (int e = 0; e < 4; ++e) pk[e] = pack_bf16(f[2 * e], f[2 * e + 1]);
+        }
         *reinterpret_cast<uint4*>(sA + (r >> 3) * (KC * 16) + c8 * 128 + (r & 7) * 16) =
             make_uint4(pk[0], pk[1], pk[2], pk[3]);
         if (ga.xt && blockIdx.y == 0) {
@@ -730,6 +739,7 @@ struct AdamArgs {
 __device__ __forceinline__ float slice_sum(const float* part, int ks, int64_t stride, int64_t k) {
   float s = 0.0f;
   int z = 0;
+#pragma unroll 4
   for (; z + 8 <= ks; z += 8) {
     float v[8];
 #pragma unroll
@@ -825,6 +835,30 @@ __global__ void column_stats_kernel(const float* __restrict__ X, int64_t n, int 
 }
 
 inline unsigned grid_for(int64_t n, unsigned bt) { return (unsigned)((n + bt - 1) / bt); }
+
+// The first layer's input rows standardised and rounded once per training run, with the same
+// operations as the layer-1 gather: Xb = bf16((X - shift) * scale) (X itself without a norm).
+// Eight features per thread; d % 8 == 0.
+__global__ void standardize_bf16_kernel(const float* __restrict__ X, int64_t n, int d,
+                                        const float* __restrict__ shift, const float* __restrict__ scale,
+                                        bf16* __restrict__ Xb) {
+  const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t per_row = d / 8;
+  if (v >= n * per_row) return;
+  const int64_t r = v / per_row;
+  const int k0 = (int)(v - r * per_row) * 8;
+  const float4* xp = reinterpret_cast<const float4*>(X + r * d + k0);
+  const float4 x0 = __ldg(xp), x1 = __ldg(xp + 1);
+  float f[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
+  if (scale) {
+#pragma unroll
+    for (int e = 0; e < 8; ++e) f[e] = (f[e] - __ldg(shift + k0 + e)) * __ldg(scale + k0 + e);
+  }
+  uint32_t pk[4];
+#pragma unroll
+  for (int e = 0; e < 4; ++e) pk[e] = pack_bf16(f[2 * e], f[2 * e + 1]);
+  *reinterpret_cast<uint4*>(Xb + r * d + k0) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+}
 
 // Sort keys of the shuffles of epochs e0 .. e0 + total / n - 1 (entry q * n + row): the
 // splitmix64 finaliser of (seed, epoch, row), top 32 bits; with eb > 0 the epoch's offset q
@@ -1084,13 +1118,15 @@ void Mlp::set_input_norm(const float* shift, const float* scale) {
 // batch.  Each kernel after the first on `s` is a programmatic dependent launch; the first
 // one is too when `after_step` says the previous kernel on `s` was this network's update.
 static void run_batch(Mlp::Impl& m, const float* X, const uint32_t* rows, int64_t B, int64_t n_valid,
-                      const float* Y, float* y_out, bool with_adam, float lr, bool after_step = false) {
+                      const float* Y, float* y_out, bool with_adam, float lr, bool after_step = false,
+                      const bf16* Xb = nullptr) {
   cudaStream_t s = m.s;
   const bool pdl = m.pdl;
   const bool train = Y != nullptr;
   float* g = m.g.p;
   GatherA ga{};
   ga.X = X;
+  ga.Xb = Xb;
   ga.ldx = m.in_dim;
   ga.rows = rows;
   ga.n_valid = n_valid;
@@ -1247,9 +1283,15 @@ void Mlp::train(const float* X, const float* Y, int64_t n, int epochs, int64_t b
   }
   DevBuf<float> dloss(epochs, s);
   UB_CUDA(cudaMemsetAsync(m.g.p, 0, m.P * 4, s));
+  // the epochs' batches gather rows of this standardised bf16 copy
+  DevBuf<bf16> xb((uint64_t)n * m.in_dim, s);
+  const int64_t vec = n * (m.in_dim / 8);
+  standardize_bf16_kernel<<<grid_for(vec, 256), 256, 0, s>>>(X, n, m.in_dim, m.has_norm ? m.shift.p : nullptr,
+                                                            m.has_norm ? m.scale.p : nullptr, xb.p);
+  UB_LAUNCH_CHECK();
   auto one_epoch = [&]() {
     for (int64_t t = 0; t < steps; ++t)
-      run_batch(m, X, cur.p + t * batch, batch, batch, Y, nullptr, true, lr, t > 0);
+      run_batch(m, X, cur.p + t * batch, batch, batch, Y, nullptr, true, lr, t > 0, xb.p);
   };
   cudaGraphExec_t exec = nullptr;
   if (graphs_enabled()) {

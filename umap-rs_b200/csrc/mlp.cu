@@ -15,8 +15,9 @@
 // them to the stage's mbarrier, and a stage is refilled only after its MMAs completed (every
 // wait bounded by a timer).  The epilogue reads the accumulator with tcgen05.ld (warp w owns
 // rows 32w..32w+31, thread = row) and fuses bias, GELU, the GELU derivative, column sums and
-// transposed copies.  The first layer's A operand is gathered straight from the fp32 input
-// rows (standardised, rounded to bf16) by the staging threads.
+// transposed copies.  The first layer's A operand is gathered by the staging threads: in
+// training from a bf16 copy of the input rows standardised once per training run, otherwise
+// straight from the fp32 rows (standardised and rounded to bf16 on the way).
 //
 // One training step (batch B): L1 GEMM (gather) -> L2 GEMM -> output layer + loss + its
 // backward (CUDA cores) -> { dH1 GEMM (GELU derivative, db1) -> dW1 GEMM } || dW2 GEMM on a

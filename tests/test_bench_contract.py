@@ -25,6 +25,10 @@ def test_roofline_inputs_from_committed_profile():
     assert l2 is not None
     for k in ("l2_throughput_pct", "l2_hit_rate_pct", "issue_active_pct"):
         assert 0.0 < l2[k] <= 100.0, (k, l2[k])
+    # the 100M-point roll's traffic scales the 40M capture by kept edges
+    t40 = bench.ncu_figure("sgd_epoch_swiss_roll_40m_renamed", "traffic_bytes_per_launch")
+    e40 = bench.ncu_figure("sgd_epoch_swiss_roll_40m_renamed", "kept_edges")
+    assert t40 and e40 and abs(bench.swiss_traffic(2 * e40) - 2 * t40) <= 1e-6 * t40
 
 
 def test_both_arms_share_one_config():

@@ -246,3 +246,36 @@ def test_output_metric_checks_without_gpu(ub):
     with pytest.raises(ub.UmapError) as e:
         ub.Umap.with_metrics(ub.UmapConfig(), ub.EuclideanMetric(), ub.Metric()).fit(20, idx, dist, init)
     assert e.value.code == ub.ERR_UNSUPPORTED
+
+
+@pytest.mark.parametrize("change,message", [
+    ({"n_sub": 100}, "the subsample must have 128..n_samples rows"),
+    ({"n_sub": 2000}, "the subsample must have 128..n_samples rows"),
+    ({"data_dim": 0}, "data_dim must be 1..4096, got 0"),
+    ({"data_dim": 5000}, "data_dim must be 1..4096, got 5000"),
+    ({"n_components": 5}, "the warm start's network predicts 1..4 components"),
+    ({"mlp_epochs": 0}, "sub_epochs, epochs and mlp_epochs must be positive"),
+    # the config's own validation (embedding.rs:339-429) runs next
+    ({"knn_cols": 1}, "knn_dists has 1 neighbors but n_neighbors is 15"),
+])
+def test_warm_start_argument_checks_without_gpu(ub, change, message):
+    """umap_warm_start_fit_device refuses arguments that need no device before it touches
+    the GPU: subsample size, feature count, component count, epoch counts, then the
+    config's own validation."""
+    from umap_b200 import _lib
+    L = ub.lib()
+    cfg = ub.UmapConfig()
+    cfg.n_components = change.get("n_components", 2)
+    c = cfg.to_c()
+    wp = _lib.WarmStartParamsC()
+    assert L.umap_warm_start_params_default(C.byref(wp)) == 0
+    wp.mlp_epochs = change.get("mlp_epochs", wp.mlp_epochs)
+    n, k = 1000, change.get("knn_cols", 15)
+    buf_f = np.zeros(64, np.float32)   # never read: the call returns before any pointer is used
+    buf_u = np.zeros(64, np.uint32)
+    pf, pu = buf_f.ctypes.data_as(C.c_void_p), buf_u.ctypes.data_as(C.c_void_p)
+    out = C.c_void_p()
+    rc = L.umap_warm_start_fit_device(C.byref(c), C.byref(wp), pf, n, change.get("data_dim", 64), pu, pf, k, pu,
+                                      change.get("n_sub", 300), pu, pf, None, C.byref(out), None, None)
+    assert rc == ub.ERR_INVALID_ARGUMENT and not out.value
+    assert L.umap_last_error().decode() == message

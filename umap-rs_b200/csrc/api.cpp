@@ -1266,6 +1266,19 @@ std::vector<float> mlp_initial_params(int in_dim, int out_dim, uint64_t seed) {
   return p;
 }
 
+// The warm start's checks that need no device (run before the call touches the GPU).
+void warm_start_check_args(const umap_config& c, const umap_warm_start_params& wp, uint64_t n, uint64_t d,
+                           uint64_t k, uint64_t n_sub) {
+  const uint64_t dim = c.n_components;
+  if (d < 1 || d > 4096) throw Error(INVALID_ARGUMENT, "data_dim must be 1..4096, got " + std::to_string(d));
+  if (dim < 1 || dim > 4) throw Error(INVALID_ARGUMENT, "the warm start's network predicts 1..4 components");
+  if (n_sub < 128 || n_sub > n) throw Error(INVALID_ARGUMENT, "the subsample must have 128..n_samples rows");
+  if (wp.sub_epochs < 1 || wp.epochs < 1 || wp.mlp_epochs < 1)
+    throw Error(INVALID_ARGUMENT, "sub_epochs, epochs and mlp_epochs must be positive");
+  std::string err = validate_parameters(c, n, n, k);
+  if (!err.empty()) throw Error(INVALID_ARGUMENT, err);
+}
+
 std::unique_ptr<umap_fitted> warm_start_impl(const umap_config& c, const umap_warm_start_params& wp,
                                              const float* data, uint64_t n, uint64_t d, const uint32_t* idx,
                                              const float* dist, uint64_t k, const uint32_t* sub_rows,
@@ -1276,13 +1289,7 @@ std::unique_ptr<umap_fitted> warm_start_impl(const umap_config& c, const umap_wa
     return std::chrono::duration<float, std::milli>(clk::now() - t).count();
   };
   const uint64_t dim = c.n_components;
-  if (d < 1 || d > 4096) throw Error(INVALID_ARGUMENT, "data_dim must be 1..4096, got " + std::to_string(d));
-  if (dim < 1 || dim > 4) throw Error(INVALID_ARGUMENT, "the warm start's network predicts 1..4 components");
-  if (n_sub < 128 || n_sub > n) throw Error(INVALID_ARGUMENT, "the subsample must have 128..n_samples rows");
-  if (wp.sub_epochs < 1 || wp.epochs < 1 || wp.mlp_epochs < 1)
-    throw Error(INVALID_ARGUMENT, "sub_epochs, epochs and mlp_epochs must be positive");
-  std::string err = validate_parameters(c, n, n, k);
-  if (!err.empty()) throw Error(INVALID_ARGUMENT, err);
+  warm_start_check_args(c, wp, n, d, k, n_sub);
   {  // the subsample's rows index the caller's data: every one must be a row of it
     std::vector<uint32_t> rows(n_sub);
     UB_CUDA(cudaMemcpy(rows.data(), sub_rows, n_sub * sizeof(uint32_t), cudaMemcpyDeviceToHost));
@@ -2545,6 +2552,7 @@ int umap_warm_start_fit_device(const umap_config* cfg, const umap_warm_start_par
   need(knn_dists, "knn_dists"); need(sub_rows, "sub_rows"); need(sub_knn_indices, "sub_knn_indices");
   need(sub_knn_dists, "sub_knn_dists"); need(out, "out");
   *out = nullptr;
+  warm_start_check_args(*cfg, *params, n_samples, data_dim, knn_cols, n_sub);
   wait_for_inputs();
   *out = warm_start_impl(*cfg, *params, data, n_samples, data_dim, knn_indices, knn_dists, knn_cols, sub_rows, n_sub,
                          sub_knn_indices, sub_knn_dists, sub_init, phase_ms, mlp_losses)
